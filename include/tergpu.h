@@ -1,0 +1,175 @@
+/*
+ * tergpu.h -- C ABI of the B200 root backend for the exact depth-3 TER attempt.
+ *
+ * Plain pointers and sizes only.  Every entry point is synchronous from the
+ * caller's view: inputs are host buffers (read only), the call uploads them,
+ * runs the device kernels on one CUDA stream of its own and copies the results
+ * back before it returns.  The library holds a per-device workspace between
+ * calls; tergpu_release() frees it.
+ *
+ * Status values 0..11 are the numeric values of ter::Status
+ * (reference include/ter/types.hpp:10-23).  Values from 64 up are this ABI's
+ * own and never collide with ter::Status.
+ */
+#ifndef TERGPU_H
+#define TERGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TERGPU_ABI_VERSION 1
+
+enum tergpu_status {
+  TERGPU_COMPLETED = 0,
+  TERGPU_FOUND = 1,
+  TERGPU_NO_WITNESS_THIS_ATTEMPT = 2,
+  TERGPU_ATTEMPT_LIMIT_REACHED = 3,
+  TERGPU_INVALID_CONFIGURATION = 4,
+  TERGPU_INVALID_SHAPE = 5,
+  TERGPU_GENERATION_INCOMPLETE = 6,
+  TERGPU_RESOURCE_LIMIT = 7,
+  TERGPU_CANCELLED = 8,
+  TERGPU_INVARIANT_VIOLATION = 9,
+  TERGPU_NOT_APPLICABLE = 10,
+  TERGPU_UNSUPPORTED_WIDTH = 11,
+  /* ABI-specific */
+  TERGPU_OUTPUT_OVERFLOW = 64, /* more triples than capacity: nothing was emitted,
+                                  out->triples_count holds the exact count */
+  TERGPU_DEVICE_ERROR = 65,    /* no CUDA device, or a CUDA call failed */
+  TERGPU_INVALID_INPUT = 66    /* malformed arguments (null pointers, widths) */
+};
+
+/* Largest root quotient width the backend accepts: bits [64, Q) travel in one
+ * byte per entry, like the reference's FamilyKeys::hi. */
+#define TERGPU_MAX_QUOTIENT_BITS 72u
+
+/* tergpu_root_in.flags */
+#define TERGPU_ROOT_COUNT_ONLY 1u /* count triples, write none */
+
+/*
+ * One L1 -> L0 root on full quotient keys.
+ *
+ * Replaces the body of a frozen root backend: the C ABI a run_gpu_root adapter
+ * with the signature of run_hash_join
+ * (reference ter2_root/campaign/ter_hash_join_root.hpp:38-40) calls after
+ * flattening mr8::Dataset + a64::FamilyKeys
+ * (ter2_root/frozen/ter_microreport8_dataset.hpp:60-64,
+ *  ter2_root/frozen/ter_a64_chqr.hpp:55-63).
+ *
+ * List 0 holds q_A, list 1 q_B and list 2 d = tau - q_C, all mod 2^Q, so a
+ * full-Q triple is (a, b, c) with key_a + key_b == key_c (mod 2^Q).  key_lo
+ * holds bits [0, min(Q, 64)), key_hi bits [64, Q) (may be NULL when Q <= 64).
+ * id maps an entry to the EntryId reported in triples (NULL: the index).
+ * cells (4096 bytes, index s * 64 + t with s, t the low 6 key bits of the A
+ * and B entries) restricts the pairs exactly like RootIndex::selected
+ * (ter2_root/frozen/ter_root_queue_kernels.hpp:63-67); NULL selects all.
+ */
+typedef struct {
+  uint32_t quotient_bits;      /* Q, 1..TERGPU_MAX_QUOTIENT_BITS */
+  uint32_t flags;              /* TERGPU_ROOT_* */
+  uint64_t count[3];
+  const uint64_t *key_lo[3];
+  const uint8_t *key_hi[3];
+  const uint32_t *id[3];
+  const uint8_t *cells;
+  uint32_t projected_bits;     /* > 0: also count triples equal on key bits [0, k), k <= 64 */
+  int32_t device;              /* CUDA device ordinal */
+  uint64_t memory_limit_bytes; /* device bytes the call may hold; 0: no ceiling */
+  uint32_t family_bits;        /* 0: autotuned; else the device partition radix (6..16) */
+  uint32_t filter_bits;        /* 0: autotuned; else log2 of the filter bitmap bits (10..20) */
+} tergpu_root_in;
+
+typedef struct {
+  uint32_t *triples;        /* capacity * 3 EntryIds: (a, b, c) per full-Q triple */
+  uint64_t capacity;
+  uint64_t triples_count;   /* full-Q triples, with multiplicity */
+  uint64_t logical_pairs;   /* sum over selected cells of |A_s| * |B_t| */
+  uint64_t filter_survivors;/* pairs that passed the on-chip filter */
+  uint64_t fast_hits;       /* triples equal on the low min(Q, 64) bits */
+  uint64_t projected_hits;  /* triples equal on the low projected_bits bits */
+  uint64_t device_bytes;    /* device workspace held by the call */
+  double join_ms;           /* device time of the partition + join kernels */
+  double total_ms;          /* wall time of the call */
+  uint32_t family_bits;     /* tuning the call ran with */
+  uint32_t filter_bits;
+} tergpu_root_out;
+
+/* Replaces: run_hash_join / run_arwlf / run_k2_wide bodies
+ * (ter2_root/campaign/ter_hash_join_root.cpp:73-215,
+ *  ter2_root/frozen/ter_arwlf.cpp:256-418, ter2_root/frozen/ter_a64_chqr.cpp:329-416). */
+int tergpu_root_run(const tergpu_root_in *in, tergpu_root_out *out);
+
+/*
+ * One L1 -> L0 root straight from the three captured L1 lists, with the final
+ * decision on the original residue words on the device.
+ *
+ * Records use the layout of the reference's FullTerRootStream / .snap record
+ * (include/ter/full_ter.hpp:297-303, ter2_root/frozen/ter_root_snapshot.hpp:9-11):
+ *   uint64 pos[W64] | uint64 neg[W64] | uint32 residue[W32]
+ * with W64 = ceil(n/64), W32 = ceil(n/32).  EntryId = record index.
+ * The device derives q_L = ((R - c_L) mod 2^n) >> r1 over Q = n - r1 bits and
+ * d = tau - q_C with tau = ((T - c_0 - c_1 - c_2) mod 2^n) >> r1, exactly as
+ * load_snapshot_workload (ter2_root/frozen/ter_root_generalization_workload.cpp:630-702)
+ * and ternary_tiled_l1_to_l0 (src/full_ter.cpp:1747-1763) do.
+ *
+ * For every full-Q triple the device then applies the authority chain of
+ * RootSink::emit_triple (ter2_root/frozen/ter_root_queue_kernels.cpp:165-195):
+ * residue sum == T (mod 2^n) over all residue words, the FiniteSanity
+ * structural count, and the root rule of solve_attempt
+ * (ter2_root/campaign/ter_arwlf_solve.cpp:100-114): the parent digit sum is
+ * binary with weight n/2 (the design-B root's valid roots, src/full_ter.cpp:1576-1598).
+ */
+typedef struct {
+  uint32_t n;                  /* 36 | n, n <= 128 */
+  uint32_t r1;
+  uint32_t flags;
+  uint32_t record_bytes;       /* 16 * W64 + 4 * W32 */
+  uint64_t count[3];
+  const uint8_t *records[3];
+  const uint32_t *child_target[3]; /* W32 words each, little endian */
+  const uint32_t *root_target;     /* W32 words */
+  const uint8_t *cells;
+  uint32_t projected_bits;
+  int32_t device;
+  uint64_t memory_limit_bytes;
+  uint32_t family_bits;
+  uint32_t filter_bits;
+} tergpu_root_records_in;
+
+typedef struct {
+  tergpu_root_out root;        /* triples, counts and timing of the join */
+  uint8_t *triple_flags;       /* capacity bytes (may be NULL): bit0 residue-exact,
+                                  bit1 FiniteSanity structural, bit2 root rule */
+  uint64_t residue_exact;      /* triples whose residues sum to T */
+  uint64_t structural;         /* ... that also pass the FiniteSanity structural count */
+  uint64_t valid_roots;        /* ... residue-exact with a binary weight-n/2 parent */
+  uint64_t tau_lo;             /* the root quotient target */
+  uint64_t tau_hi;
+} tergpu_root_records_out;
+
+/* Replaces: ternary_tiled_l1_to_l0 + full_ter_root_tiled_visitor
+ * (src/full_ter.cpp:1537-1925) and the root pass of solve_attempt
+ * (ter2_root/campaign/ter_arwlf_solve.cpp:41-178). */
+int tergpu_root_run_records(const tergpu_root_records_in *in, tergpu_root_records_out *out);
+
+/* Number of CUDA devices visible to the library (0 when none). */
+int tergpu_device_count(void);
+
+/* ABI version compiled into the library. */
+int tergpu_abi_version(void);
+
+/* Frees every per-device workspace the library holds. */
+void tergpu_release(void);
+
+/* Last error text of the calling thread ("" when none). */
+const char *tergpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TERGPU_H */

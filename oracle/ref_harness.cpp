@@ -1,0 +1,362 @@
+// Reference harness -- test infrastructure, never part of the product.
+//
+// Drives the reference's own compiled code (built from its sources by
+// oracle/Makefile) so tests can pin the oracle restatement and the GPU backend
+// against it, and so bench.py can time the reference's CPU backends on the same
+// host.  Every line of output is one JSON object.
+//
+//   terref solve N SEED ATTEMPTS KIND POLICY AUDIT
+//       solve_full_ter (src/full_ter.cpp:3867) on authentic_instance (KIND=auth)
+//       or build_instance(n, 10, seed) (KIND=build); per-attempt level sizes,
+//       root accounting and the witness.
+//   terref capture N SEED ATTEMPT KIND OUT
+//       root_snapshot::capture_to_file (ter2_root/frozen/ter_root_snapshot.cpp:124).
+//   terref snaproot SNAP BACKEND CELLS PROJ
+//       load_snapshot_workload + build_family_keys + build_root_index, optional
+//       select_microproblems(CELLS), then one backend into an authority sink.
+//   terref synth BITS SEED SIZE POOL OUT
+//       ter2_root/tests/ter_synthetic_root.hpp make_root; writes the three key
+//       lists to OUT and prints the brute-force oracle digest.
+//   terref keysroot KEYS BACKEND CELLS REPS PROJ
+//       one backend over key lists read from KEYS (list 2 holds d), sink without
+//       authority; REPS timed repetitions.
+// BACKEND: arwlf | k2wide | k2 | hash | gpu | brute
+
+#include "ter_a64_chqr.hpp"
+#include "ter_arwlf.hpp"
+#include "ter_gpu_root.hpp"
+#include "ter_hash_join_root.hpp"
+#include "ter_root_generalization_workload.hpp"
+#include "ter_root_queue_kernels.hpp"
+#include "ter_root_snapshot.hpp"
+#include "ter_synthetic_root.hpp"
+
+#include "ter/full_ter.hpp"
+#include "ter/instance.hpp"
+#include "ter/limitations.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+namespace rg = ter::root_generalization;
+namespace mr8 = ter::microreport8;
+namespace a64 = ter::a64;
+namespace aw = ter::arwlf;
+namespace rs = ter::root_snapshot;
+namespace sr = ter::synthetic_root;
+namespace hj = ter::hash_join_root;
+namespace gr = ter::gpu_root;
+
+using Clock = std::chrono::steady_clock;
+
+std::string hex64(std::uint64_t v) {
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "\"0x%016llx\"", static_cast<unsigned long long>(v));
+  return buf;
+}
+
+ter::Instance make_instance(std::uint32_t n, std::uint64_t seed, const std::string& kind) {
+  if (kind == "auth") { return rg::authentic_instance(n, seed); }
+  auto built = ter::build_instance(n, ter::limits::benchmark::kFullTerFixtureModulusBits, seed);
+  return built.status == ter::Status::Completed ? built.value : ter::Instance{};
+}
+
+std::string digest_json(const rg::OutputDigest& d) {
+  std::ostringstream o;
+  o << "\"triples\":" << d.triples << ",\"triple_sum\":" << hex64(d.triple_sum)
+    << ",\"triple_xor\":" << hex64(d.triple_xor) << ",\"triple_sum2\":" << hex64(d.triple_sum2)
+    << ",\"full_q\":" << d.full_q << ",\"residue\":" << d.residue
+    << ",\"residue_sum\":" << hex64(d.residue_sum) << ",\"structural\":" << d.structural;
+  return o.str();
+}
+
+std::string witnesses_json(std::vector<std::array<ter::EntryId, 3>> w) {
+  std::sort(w.begin(), w.end());
+  std::ostringstream o;
+  o << "[";
+  for (std::size_t i = 0; i < w.size(); ++i) {
+    o << (i ? "," : "") << "[" << w[i][0] << "," << w[i][1] << "," << w[i][2] << "]";
+  }
+  o << "]";
+  return o.str();
+}
+
+int cmd_solve(int argc, char** argv) {
+  if (argc < 8) { return 2; }
+  const auto n = static_cast<std::uint32_t>(std::strtoul(argv[2], nullptr, 0));
+  const std::uint64_t seed = std::strtoull(argv[3], nullptr, 0);
+  const auto attempts = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
+  const std::string kind = argv[5];
+  const std::string policy = argv[6];
+  const bool audit = std::string(argv[7]) == "1";
+  const ter::Instance instance = make_instance(n, seed, kind);
+  ter::FullTerConfig config = rg::authentic_config(seed);
+  config.attempt_limit = attempts;
+  config.audit = audit;
+  config.root_output_policy = policy == "canon" ? ter::RootOutputPolicy::FullCanonicalOutput
+                                                : ter::RootOutputPolicy::FirstWitness;
+  const auto start = Clock::now();
+  const ter::FullTerResult result = ter::solve_full_ter(instance, config);
+  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+  const auto& t = result.telemetry;
+  for (const auto& a : t.attempts) {
+    std::cout << "{\"attempt\":" << a.attempt << ",\"seed\":" << a.seed
+              << ",\"status\":" << static_cast<int>(a.status) << ",\"level2\":[";
+    for (std::size_t i = 0; i < 9; ++i) { std::cout << (i ? "," : "") << a.level2_sizes[i]; }
+    std::cout << "],\"level1\":[" << a.level1_sizes[0] << "," << a.level1_sizes[1] << ","
+              << a.level1_sizes[2] << "],\"level0\":" << a.level0_size
+              << ",\"l3_modular\":" << a.level3_to_level2.modular_candidates
+              << ",\"l2_modular\":" << a.level2_to_level1.modular_candidates
+              << ",\"root_prefilter\":" << a.level1_to_level0.low_prefilter_candidates
+              << ",\"root_quotient_rejects\":" << a.level1_to_level0.full_quotient_rejects
+              << ",\"root_modular\":" << a.level1_to_level0.modular_candidates
+              << ",\"valid_roots\":" << a.level1_to_level0.valid_root_count
+              << ",\"prefilter_bits\":" << a.level1_to_level0.prefilter_bits
+              << ",\"root_ns\":" << a.level1_to_level0.elapsed_ns
+              << ",\"total_ns\":" << a.total_ns << "}\n";
+  }
+  std::cout << "{\"status\":" << static_cast<int>(result.status) << ",\"r1\":" << t.parameters.r1
+            << ",\"r2\":" << t.parameters.r2 << ",\"l3\":[" << t.physical_level3_sizes[0] << ","
+            << t.physical_level3_sizes[1] << "],\"fingerprint\":" << hex64(t.fingerprint)
+            << ",\"ms\":" << ms << ",\"witness\":\"";
+  for (const auto d : result.witness) { std::cout << static_cast<int>(d); }
+  std::cout << "\",\"message\":\"" << result.message << "\"}\n";
+  return 0;
+}
+
+int cmd_capture(int argc, char** argv) {
+  if (argc < 7) { return 2; }
+  const auto n = static_cast<std::uint32_t>(std::strtoul(argv[2], nullptr, 0));
+  const std::uint64_t seed = std::strtoull(argv[3], nullptr, 0);
+  const auto attempt = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
+  const ter::Instance instance = make_instance(n, seed, argv[5]);
+  ter::FullTerConfig config = rg::authentic_config(seed);
+  const auto start = Clock::now();
+  const rs::CaptureOutcome outcome = rs::capture_to_file(instance, config, attempt, argv[6],
+                                                         std::uint64_t{4} << 20, "reference");
+  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+  std::cout << "{\"written\":" << (outcome.written ? "true" : "false")
+            << ",\"status\":" << static_cast<int>(outcome.stream.status)
+            << ",\"level1\":[" << outcome.stream.level1_sizes[0] << ","
+            << outcome.stream.level1_sizes[1] << "," << outcome.stream.level1_sizes[2]
+            << "],\"level2\":[";
+  for (std::size_t i = 0; i < 9; ++i) { std::cout << (i ? "," : "") << outcome.stream.level2_sizes[i]; }
+  std::cout << "],\"file_bytes\":" << outcome.file_bytes << ",\"ms\":" << ms << "}\n";
+  return outcome.written ? 0 : 1;
+}
+
+// One backend pass into `sink`; returns backend telemetry as JSON fields.
+std::string run_backend(const std::string& backend, const mr8::Dataset& data, rg::RootIndex& index,
+                        const a64::FamilyKeys& keys, rg::RootSink& sink, std::uint32_t proj,
+                        double* ms) {
+  std::ostringstream o;
+  const auto start = Clock::now();
+  if (backend == "arwlf") {
+    aw::Config config;
+    if (proj != 0U) { config.check_bits = proj - 19U; }
+    aw::Telemetry t;
+    const aw::Status st = aw::run_arwlf(data, index, keys, config, sink, &t);
+    *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+    o << "\"backend_status\":\"" << aw::status_label(st) << "\",\"logical_pairs\":" << t.logical_pairs
+      << ",\"filter_survivors\":" << t.filter_survivors << ",\"projected_hits\":" << t.projected_hits
+      << ",\"projected_bits\":" << 19U + t.check_bits << ",\"fast_hits\":" << t.fast_hits
+      << ",\"full_hits\":" << t.full_hits;
+  } else if (backend == "k2wide") {
+    a64::Telemetry t;
+    a64::run_k2_wide(data, index, keys, sink, &t, false);
+    *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+    o << "\"backend_status\":\"Completed\",\"logical_pairs\":" << t.logical_pairs
+      << ",\"projected_hits\":" << t.projected_hits << ",\"fast_hits\":" << t.fast_hits
+      << ",\"full_hits\":" << t.full_hits;
+  } else if (backend == "k2") {
+    rg::run_k2(data, sink);
+    *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+    o << "\"backend_status\":\"Completed\"";
+  } else if (backend == "hash") {
+    hj::Telemetry t;
+    const hj::Status st = hj::run_hash_join(data, index, keys, hj::Config{}, sink, &t);
+    *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+    o << "\"backend_status\":\"" << hj::status_label(st) << "\",\"logical_pairs\":" << t.logical_pairs
+      << ",\"full_hits\":" << t.full_hits;
+  } else if (backend == "gpu") {
+    gr::Config config;
+    config.projected_bits = proj;
+    gr::Telemetry t;
+    const gr::Status st = gr::run_gpu_root(data, index, keys, config, sink, &t);
+    *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+    o << "\"backend_status\":\"" << gr::status_label(st) << "\",\"logical_pairs\":" << t.logical_pairs
+      << ",\"filter_survivors\":" << t.filter_survivors << ",\"projected_hits\":" << t.projected_hits
+      << ",\"projected_bits\":" << proj << ",\"fast_hits\":" << t.fast_hits
+      << ",\"full_hits\":" << t.full_hits << ",\"join_ms\":" << t.join_ms
+      << ",\"family_bits\":" << t.family_bits << ",\"filter_bits\":" << t.filter_bits;
+  } else {
+    *ms = 0.0;
+    o << "\"backend_status\":\"unknown backend\"";
+  }
+  return o.str();
+}
+
+int cmd_snaproot(int argc, char** argv) {
+  if (argc < 6) { return 2; }
+  const std::string path = argv[2];
+  const std::string backend = argv[3];
+  const auto cells = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
+  const auto proj = static_cast<std::uint32_t>(std::strtoul(argv[5], nullptr, 0));
+  const auto workload = rg::load_snapshot_workload(path, true);
+  if (workload->status != rg::WorkloadStatus::Completed) {
+    std::cout << "{\"error\":\"" << rg::status_label(workload->status) << ": "
+              << workload->status_detail << "\"}\n";
+    return 1;
+  }
+  const a64::FamilyKeys keys = a64::build_family_keys(*workload);
+  const mr8::Dataset& data = *workload->data;
+  rg::RootIndex index;
+  rg::build_root_index(data, index);
+  if (cells < 4096U) { rg::select_microproblems(index, cells); }
+  std::vector<std::array<ter::EntryId, 3>> witnesses;
+  rg::RootSink sink;
+  sink.data = &data;
+  sink.index = &index;
+  sink.authority = &workload->authority;
+  sink.witnesses = &witnesses;
+  sink.reset();
+  double ms = 0.0;
+  const std::string extra = run_backend(backend, data, index, keys, sink, proj, &ms);
+  std::uint64_t pairs = 0U;
+  for (std::uint32_t s = 0; s < 64U; ++s)
+    for (std::uint32_t t = 0; t < 64U; ++t)
+      if (index.active(s, t)) pairs += data.q_family[s].size() * data.x_family[t].size();
+  std::cout << "{\"backend\":\"" << backend << "\",\"n\":" << workload->n
+            << ",\"sizes\":[" << workload->a_size << "," << workload->b_size << "," << workload->c_size
+            << "],\"quotient_bits\":" << workload->quotient_bits << ",\"cells\":" << index.selected_count
+            << ",\"pairs\":" << pairs << ",\"ms\":" << ms << "," << digest_json(sink.digest) << ","
+            << extra << ",\"witnesses\":" << witnesses_json(witnesses) << "}\n";
+  return 0;
+}
+
+bool write_keys(const std::string& path, const sr::Synthetic& root) {
+  std::ofstream f(path, std::ios::binary);
+  const char magic[8] = {'T', 'E', 'R', 'K', 'E', 'Y', 'S', '1'};
+  f.write(magic, 8);
+  const std::uint32_t head[2] = {root.bits, 0U};
+  f.write(reinterpret_cast<const char*>(head), sizeof head);
+  for (std::size_t l = 0; l < 3; ++l) {
+    const std::uint64_t count = root.lists[l].size();
+    f.write(reinterpret_cast<const char*>(&count), 8);
+  }
+  for (std::size_t l = 0; l < 3; ++l) {
+    for (const auto& v : root.lists[l]) { f.write(reinterpret_cast<const char*>(&v.lo), 8); }
+    for (const auto& v : root.lists[l]) {
+      const auto h = static_cast<std::uint8_t>(v.hi);
+      f.write(reinterpret_cast<const char*>(&h), 1);
+    }
+    const std::size_t pad = (8U - root.lists[l].size() % 8U) % 8U;
+    const char zeros[8] = {};
+    f.write(zeros, static_cast<std::streamsize>(pad));
+  }
+  return static_cast<bool>(f);
+}
+
+bool read_keys(const std::string& path, sr::Synthetic& root) {
+  std::ifstream f(path, std::ios::binary);
+  char magic[8];
+  f.read(magic, 8);
+  if (!f || std::memcmp(magic, "TERKEYS1", 8) != 0) { return false; }
+  std::uint32_t head[2];
+  f.read(reinterpret_cast<char*>(head), sizeof head);
+  root.bits = head[0];
+  std::uint64_t counts[3];
+  f.read(reinterpret_cast<char*>(counts), sizeof counts);
+  for (std::size_t l = 0; l < 3; ++l) {
+    std::vector<std::uint64_t> lo(counts[l]);
+    std::vector<std::uint8_t> hi(counts[l]);
+    f.read(reinterpret_cast<char*>(lo.data()), static_cast<std::streamsize>(8U * counts[l]));
+    f.read(reinterpret_cast<char*>(hi.data()), static_cast<std::streamsize>(counts[l]));
+    f.ignore(static_cast<std::streamsize>((8U - counts[l] % 8U) % 8U));
+    root.lists[l].resize(counts[l]);
+    for (std::size_t i = 0; i < counts[l]; ++i) { root.lists[l][i] = sr::Value{lo[i], hi[i]}; }
+  }
+  return static_cast<bool>(f);
+}
+
+int cmd_synth(int argc, char** argv) {
+  if (argc < 7) { return 2; }
+  const auto bits = static_cast<std::uint32_t>(std::strtoul(argv[2], nullptr, 0));
+  const std::uint64_t seed = std::strtoull(argv[3], nullptr, 0);
+  const auto size = static_cast<std::size_t>(std::strtoull(argv[4], nullptr, 0));
+  const auto pool = static_cast<std::uint32_t>(std::strtoul(argv[5], nullptr, 0));
+  sr::Synthetic root = sr::make_root(bits, seed, size, pool);
+  const rg::OutputDigest expected = sr::oracle(root);
+  if (!write_keys(argv[6], root)) { return 1; }
+  std::cout << "{\"bits\":" << bits << ",\"sizes\":[" << root.lists[0].size() << ","
+            << root.lists[1].size() << "," << root.lists[2].size() << "]," << digest_json(expected)
+            << "}\n";
+  return 0;
+}
+
+int cmd_keysroot(int argc, char** argv) {
+  if (argc < 7) { return 2; }
+  sr::Synthetic root;
+  if (!read_keys(argv[2], root)) {
+    std::cout << "{\"error\":\"cannot read keys\"}\n";
+    return 1;
+  }
+  const std::string backend = argv[3];
+  const auto cells = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
+  const int reps = std::max(1, std::atoi(argv[5]));
+  const auto proj = static_cast<std::uint32_t>(std::strtoul(argv[6], nullptr, 0));
+  const auto build_start = Clock::now();
+  sr::finish(root);
+  const double build_ms = std::chrono::duration<double, std::milli>(Clock::now() - build_start).count();
+  if (cells < 4096U) { rg::select_microproblems(root.index, cells); }
+  std::uint64_t pairs = 0U;
+  for (std::uint32_t s = 0; s < 64U; ++s)
+    for (std::uint32_t t = 0; t < 64U; ++t)
+      if (root.index.active(s, t)) pairs += root.data->q_family[s].size() * root.data->x_family[t].size();
+  for (int rep = 0; rep < reps; ++rep) {
+    rg::RootSink sink = sr::make_sink(root);
+    double ms = 0.0;
+    std::string extra;
+    if (backend == "brute") {
+      const auto start = Clock::now();
+      sink.digest = sr::oracle(root);
+      ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+      extra = "\"backend_status\":\"Completed\"";
+    } else {
+      extra = run_backend(backend, *root.data, root.index, root.keys, sink, proj, &ms);
+    }
+    std::cout << "{\"backend\":\"" << backend << "\",\"rep\":" << rep << ",\"bits\":" << root.bits
+              << ",\"cells\":" << root.index.selected_count << ",\"pairs\":" << pairs
+              << ",\"build_ms\":" << build_ms << ",\"ms\":" << ms << "," << digest_json(sink.digest)
+              << "," << extra << "}\n" << std::flush;
+  }
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) {
+    std::cerr << "usage: terref solve|capture|snaproot|synth|keysroot ...\n";
+    return 2;
+  }
+  const std::string cmd = argv[1];
+  int rc = 2;
+  if (cmd == "solve") { rc = cmd_solve(argc, argv); }
+  else if (cmd == "capture") { rc = cmd_capture(argc, argv); }
+  else if (cmd == "snaproot") { rc = cmd_snaproot(argc, argv); }
+  else if (cmd == "synth") { rc = cmd_synth(argc, argv); }
+  else if (cmd == "keysroot") { rc = cmd_keysroot(argc, argv); }
+  if (rc == 2) { std::cerr << "bad arguments for " << cmd << "\n"; }
+  return rc;
+}
