@@ -48,7 +48,9 @@ enum tergpu_status {
 #define TERGPU_MAX_QUOTIENT_BITS 72u
 
 /* tergpu_root_in.flags */
-#define TERGPU_ROOT_COUNT_ONLY 1u /* count triples, write none */
+#define TERGPU_ROOT_COUNT_ONLY 1u    /* count triples, write none */
+#define TERGPU_ROOT_DEVICE_INPUTS 2u /* key_lo / key_hi / id / cells are device pointers of
+                                        `device`, already resident: nothing is uploaded */
 
 /*
  * One L1 -> L0 root on full quotient keys.
@@ -81,6 +83,7 @@ typedef struct {
   uint64_t memory_limit_bytes; /* device bytes the call may hold; 0: no ceiling */
   uint32_t family_bits;        /* 0: autotuned; else the device partition radix (6..16) */
   uint32_t filter_bits;        /* 0: autotuned; else log2 of the filter bitmap bits (10..20) */
+  void *stream;                /* cudaStream_t to launch on; NULL: the library's own */
 } tergpu_root_in;
 
 typedef struct {
@@ -93,9 +96,12 @@ typedef struct {
   uint64_t projected_hits;  /* triples equal on the low projected_bits bits */
   uint64_t device_bytes;    /* device workspace held by the call */
   double join_ms;           /* device time of the partition + join kernels */
+  double partition_ms;      /* device time of the partition kernels alone */
+  double sweep_ms;          /* device time of the sweep kernel(s) alone */
   double total_ms;          /* wall time of the call */
   uint32_t family_bits;     /* tuning the call ran with */
   uint32_t filter_bits;
+  uint32_t kernel_launches; /* device kernels this call launched */
 } tergpu_root_out;
 
 /* Replaces: run_hash_join / run_arwlf / run_k2_wide bodies
@@ -155,6 +161,11 @@ typedef struct {
  * (src/full_ter.cpp:1537-1925) and the root pass of solve_attempt
  * (ter2_root/campaign/ter_arwlf_solve.cpp:41-178). */
 int tergpu_root_run_records(const tergpu_root_records_in *in, tergpu_root_records_out *out);
+
+/* FNV-1a-64 over size bytes starting from state (0xcbf29ce484222325 for a fresh
+ * hash): the list and header checksums of the .snap format
+ * (reference ter2_root/frozen/ter_root_snapshot.cpp:94-101).  Host code only. */
+uint64_t tergpu_fnv1a(const void *bytes, uint64_t size, uint64_t state);
 
 /* Number of CUDA devices visible to the library (0 when none). */
 int tergpu_device_count(void);

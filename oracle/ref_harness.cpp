@@ -141,6 +141,7 @@ int cmd_capture(int argc, char** argv) {
   const auto attempt = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
   const ter::Instance instance = make_instance(n, seed, argv[5]);
   ter::FullTerConfig config = rg::authentic_config(seed);
+  config.attempt_limit = attempt + 1U;  // the stream refuses attempts outside the budget
   const auto start = Clock::now();
   const rs::CaptureOutcome outcome = rs::capture_to_file(instance, config, attempt, argv[6],
                                                          std::uint64_t{4} << 20, "reference");
@@ -312,13 +313,29 @@ int cmd_keysroot(int argc, char** argv) {
     return 1;
   }
   const std::string backend = argv[3];
+  // CELLS: a count (the reference's declared subsample) or "mod:P:I:M" -- the
+  // first M cells c (index s * 64 + t) with c % P == I, for disjoint slices.
+  const std::string cells_arg = argv[4];
   const auto cells = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
   const int reps = std::max(1, std::atoi(argv[5]));
   const auto proj = static_cast<std::uint32_t>(std::strtoul(argv[6], nullptr, 0));
   const auto build_start = Clock::now();
   sr::finish(root);
   const double build_ms = std::chrono::duration<double, std::milli>(Clock::now() - build_start).count();
-  if (cells < 4096U) { rg::select_microproblems(root.index, cells); }
+  if (cells_arg.rfind("mod:", 0) == 0) {
+    unsigned p = 1, i = 0, m = 4096;
+    std::sscanf(cells_arg.c_str(), "mod:%u:%u:%u", &p, &i, &m);
+    root.index.selected.fill(0U);
+    root.index.selected_count = 0U;
+    for (std::uint32_t c = 0; c < 4096U && root.index.selected_count < m; ++c) {
+      if (p != 0U && c % p == i) {
+        root.index.selected[c] = 1U;
+        ++root.index.selected_count;
+      }
+    }
+  } else if (cells < 4096U) {
+    rg::select_microproblems(root.index, cells);
+  }
   std::uint64_t pairs = 0U;
   for (std::uint32_t s = 0; s < 64U; ++s)
     for (std::uint32_t t = 0; t < 64U; ++t)

@@ -803,9 +803,12 @@ uint64_t orc_synthetic_root(uint32_t bits, uint64_t seed, uint64_t size, uint32_
     }
   }
 #define PLANT(a, b) do { val_t pa = (a), pb = (b); PUT(0, pa); PUT(1, pb); val_t pd = vadd(pa, pb, bits); PUT(2, pd); } while (0)
+  /* The reference writes plant(random_value(), random_value()); C++ leaves the
+   * order of the two calls unspecified and the GCC build of the reference (the
+   * one that pins this oracle) evaluates the second argument first. */
   for (int i = 0; i < 40; ++i) {
-    val_t a = srng_value(&r);
     val_t b = srng_value(&r);
+    val_t a = srng_value(&r);
     PLANT(a, b);
   }
   PLANT(all_ones, ((val_t){1, 0}));

@@ -1,0 +1,419 @@
+// B200 kernels of the TER root join.  See root_kernels.cuh for the layout.
+//
+// Partition (HBM-bound):  histogram -> exclusive scan -> scatter, one pass per
+//   list, radix fb bits of the low key.  Reads 13 B and writes 13 B per entry.
+// Sweep (issue-bound):  one CTA per (target family u, slice of s).  The CTA
+//   builds, in shared memory, a filter bitmap and an exact-lookup hash of the
+//   D family u.  Each warp owns 128 A-entries of family s as 32-bit windows in
+//   registers and streams B family t = u - s: per logical pair one IADD, one
+//   SHF, one LDS, two funnel shifts.  Filter survivors are compacted into a
+//   per-warp shared queue (ballot/popc) and resolved exactly against the full
+//   residual and the high key byte.  No floating point anywhere.
+
+#include "root_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+namespace tergpu {
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t yhash_of(uint32_t w) { return (w * 0x9E3779B1u) >> (32 - kYHashBits); }
+
+template <bool ALIGNED>
+__device__ __forceinline__ uint32_t window_of(uint64_t r, uint32_t mrb) {
+  // ALIGNED (fewer than 32 residual bits compared): left-align so the 32-bit
+  // add wraps exactly mod 2^mrb.  Otherwise the low 32 residual bits.
+  if (ALIGNED) return static_cast<uint32_t>(r << (32 - mrb));
+  return static_cast<uint32_t>(r);
+}
+
+__global__ void k_hist(const uint64_t* __restrict__ key, uint64_t n, uint32_t fmask,
+                       uint32_t* __restrict__ cnt) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    atomicAdd(&cnt[static_cast<uint32_t>(key[i]) & fmask], 1u);
+  }
+}
+
+// One CTA of 1024 threads: padded exclusive scan of up to 65536 family counts.
+__global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t nfam, uint32_t* __restrict__ off,
+                       uint32_t* __restrict__ cursor) {
+  __shared__ uint32_t warp_sums[32];
+  const uint32_t per = (nfam + blockDim.x - 1) / blockDim.x;
+  const uint32_t begin = threadIdx.x * per;
+  const uint32_t end = min(nfam, begin + per);
+  uint32_t local = 0;
+  for (uint32_t f = begin; f < end; ++f) local += (cnt[f] + 1u) & ~1u;
+  // inclusive scan of `local` across the block
+  uint32_t v = local;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  if (lane == 31) warp_sums[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t o = __shfl_up_sync(kFull, w, d);
+      if (lane >= (uint32_t)d) w += o;
+    }
+    warp_sums[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = v - local + (warp > 0 ? warp_sums[warp - 1] : 0);
+  for (uint32_t f = begin; f < end; ++f) {
+    off[f] = run;
+    cursor[f] = run;
+    run += (cnt[f] + 1u) & ~1u;
+  }
+  if (threadIdx.x == blockDim.x - 1) off[nfam] = run;
+}
+
+__global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __restrict__ key_hi,
+                          const uint32_t* __restrict__ id, uint64_t n, uint32_t fb,
+                          uint64_t fast_mask, uint32_t hi_mask, uint32_t* __restrict__ cursor,
+                          uint64_t* __restrict__ res, uint8_t* __restrict__ hi,
+                          uint32_t* __restrict__ out_id) {
+  const uint32_t fmask = (1u << fb) - 1u;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = key_lo[i] & fast_mask;
+    const uint32_t pos = atomicAdd(&cursor[static_cast<uint32_t>(k) & fmask], 1u);
+    res[pos] = k >> fb;
+    hi[pos] = key_hi != nullptr ? static_cast<uint8_t>(key_hi[i] & hi_mask) : 0;
+    out_id[pos] = id != nullptr ? id[i] : static_cast<uint32_t>(i);
+  }
+}
+
+template <bool ALIGNED>
+__global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t item_counter;
+  const uint32_t nfam = 1u << a.fb;
+  const uint32_t fmask = nfam - 1u;
+  const uint32_t wb = a.wb;
+  uint32_t* bm = smem;
+  uint32_t* ywin = bm + (1u << wb);
+  uint32_t* yhash = ywin + kYCap;
+  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
+
+  const uint32_t u = blockIdx.x % nfam;
+  const uint32_t part = blockIdx.x / nfam;
+  const uint32_t s_per = (nfam + a.s_split - 1u) / a.s_split;
+  const uint32_t s0 = part * s_per;
+  const uint32_t s1 = min(nfam, s0 + s_per);
+  const uint32_t ny = a.y.cnt[u];
+  if (s0 >= s1 || ny == 0u) return;  // uniform across the block
+  const uint32_t yoff = a.y.off[u];
+  const uint64_t mmask = a.mrb >= 64 ? ~0ull : ((1ull << a.mrb) - 1ull);
+  const uint32_t tid = threadIdx.x;
+
+  for (uint32_t i = tid; i < (1u << wb); i += kSweepThreads) bm[i] = 0u;
+  for (uint32_t i = tid; i < (1u << kYHashBits); i += kSweepThreads) yhash[i] = 0u;
+  if (tid == 0) item_counter = 0u;
+  __syncthreads();
+  const bool yshared = ny <= kYCap;
+  for (uint32_t i = tid; i < ny; i += kSweepThreads) {
+    const uint32_t w = window_of<ALIGNED>(a.y.res[yoff + i] & mmask, a.mrb);
+    const uint32_t word = (~w) >> (32u - wb);
+    const uint32_t bit = ALIGNED ? ((w >> (27u - wb)) & 31u) : (w & 31u);
+    atomicOr(&bm[word], 1u << bit);
+    if (yshared) {
+      ywin[i] = w;
+      uint32_t h = yhash_of(w);
+      // at most kYCap entries in 2 * kYCap slots: an empty slot always exists
+      while (atomicCAS(&yhash[h], 0u, i + 1u) != 0u) h = (h + 1u) & ((1u << kYHashBits) - 1u);
+    }
+  }
+  __syncthreads();
+
+  const uint32_t warp = tid >> 5, lane = tid & 31u;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  uint2* wq = queues + warp * kQueueCap;
+  const uint32_t qc_max = static_cast<uint32_t>((a.counters[kMaxQ] + 127ull) / 128ull);
+  const uint32_t total_items = (s1 - s0) * qc_max;
+  unsigned long long c_surv = 0, c_fast = 0, c_proj = 0, c_fall = 0;
+  const uint32_t kap_shift = ALIGNED ? (32u - a.mrb) : 0u;
+  const uint32_t rot_shift = ALIGNED ? (27u - wb) : 0u;
+  const uint32_t word_shift = 32u - wb;
+  const uint32_t hi_mask = (1u << a.hi_bits) - 1u;
+
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total_items) break;
+    const uint32_t s = s0 + item / qc_max;
+    const uint32_t qc = item % qc_max;
+    const uint32_t t = (u - s) & fmask;
+    const uint32_t kap = s > u ? 1u : 0u;
+    if (a.cells != nullptr && a.cells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
+    const uint32_t nq = a.q.cnt[s];
+    const uint32_t nx = a.x.cnt[t];
+    const uint32_t qbase = qc * 128u;
+    if (qbase >= nq || nx == 0u) continue;
+    const uint32_t qoff = a.q.off[s];
+    const uint32_t xoff = a.x.off[t];
+
+    uint32_t nqv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t qi = qbase + r * 32u + lane;
+      const uint64_t rq = qi < nq ? (a.q.res[qoff + qi] & mmask) : 0ull;
+      nqv[r] = ~(window_of<ALIGNED>(rq, a.mrb) + (kap << kap_shift));
+    }
+
+    uint32_t qlen = 0;
+    // Exact resolution of every queued (q, x) survivor; all lanes take part.
+    auto drain = [&]() {
+      __syncwarp();
+      for (uint32_t e = lane; e < qlen; e += 32u) {
+        const uint2 ent = wq[e];
+        const uint32_t qi = ent.x, xi = ent.y;
+        const uint64_t rq = a.q.res[qoff + qi];
+        const uint64_t rx = a.x.res[xoff + xi];
+        const uint64_t sum = rq + rx + kap;  // residuals < 2^58: no overflow
+        const uint64_t ms = sum & mmask;
+        const uint32_t w = window_of<ALIGNED>(ms, a.mrb);
+        ++c_surv;
+        auto check = [&](uint32_t idx) {
+          if ((a.y.res[yoff + idx] & mmask) != ms) return;
+          if (a.project) {
+            ++c_proj;
+            return;
+          }
+          ++c_fast;
+          if (a.hi_bits != 0u) {
+            const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                   static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+            if (high != a.y.hi[yoff + idx]) return;
+          }
+          const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+          if (slot < a.cap) {
+            a.triples[3 * slot] = a.q.id[qoff + qi];
+            a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+            a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+          }
+        };
+        if (yshared) {
+          uint32_t h = yhash_of(w);
+          for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+            if (ywin[v - 1u] == w) check(v - 1u);
+            h = (h + 1u) & ((1u << kYHashBits) - 1u);
+          }
+        } else {
+          ++c_fall;
+          for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
+        }
+      }
+      __syncwarp();
+      qlen = 0;
+    };
+
+    const uint64_t* xr = a.x.res + xoff;
+    for (uint32_t j = 0; j < nx; j += 8u) {
+      uint32_t m = 0;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        // uniform address: one broadcast load of two residuals (the array
+        // carries 8 slack entries, so j + 7 stays inside it)
+        const ulonglong2 xx = *reinterpret_cast<const ulonglong2*>(xr + j + 2 * p);
+        const uint32_t xw0 = window_of<ALIGNED>(xx.x & mmask, a.mrb);
+        const uint32_t xw1 = window_of<ALIGNED>(xx.y & mmask, a.mrb);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const uint32_t t0 = nqv[r] - xw0;
+          const uint32_t w0 = bm[t0 >> word_shift];
+          m = __funnelshift_l(__funnelshift_l(w0, w0, t0 >> rot_shift), m, 1);
+          const uint32_t t1 = nqv[r] - xw1;
+          const uint32_t w1 = bm[t1 >> word_shift];
+          m = __funnelshift_l(__funnelshift_l(w1, w1, t1 >> rot_shift), m, 1);
+        }
+      }
+      if (__any_sync(kFull, m != 0u)) {
+        // test k = p*8 + r*2 + e sits at bit 31 - k
+        for (;;) {
+          const bool has = m != 0u;
+          uint32_t qi = 0, xi = 0;
+          bool valid = false;
+          if (has) {
+            const uint32_t b = __ffs(m) - 1u;
+            m &= m - 1u;
+            const uint32_t k = 31u - b;
+            qi = qbase + ((k >> 1) & 3u) * 32u + lane;
+            xi = j + 2u * (k >> 3) + (k & 1u);
+            valid = qi < nq && xi < nx;
+          }
+          if (__ballot_sync(kFull, has) == 0u) break;
+          const uint32_t ball = __ballot_sync(kFull, valid);
+          if (qlen + __popc(ball) > kQueueCap) drain();
+          if (valid) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2(qi, xi);
+          qlen += __popc(ball);
+        }
+      }
+    }
+    drain();
+  }
+
+  // per-lane counters -> global
+  for (int d = 16; d > 0; d >>= 1) {
+    c_surv += __shfl_down_sync(kFull, c_surv, d);
+    c_fast += __shfl_down_sync(kFull, c_fast, d);
+    c_proj += __shfl_down_sync(kFull, c_proj, d);
+    c_fall += __shfl_down_sync(kFull, c_fall, d);
+  }
+  if (lane == 0) {
+    if (c_surv) atomicAdd(&a.counters[kSurvivors], c_surv);
+    if (c_fast) atomicAdd(&a.counters[kFast], c_fast);
+    if (c_proj) atomicAdd(&a.counters[kProjected], c_proj);
+    if (c_fall) atomicAdd(&a.counters[kFallback], c_fall);
+  }
+}
+
+__global__ void k_max_family(const uint32_t* __restrict__ cnt, uint32_t nfam,
+                             unsigned long long* __restrict__ counters) {
+  uint32_t m = 0;
+  for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < nfam; f += gridDim.x * blockDim.x) {
+    m = max(m, cnt[f]);
+  }
+  for (int d = 16; d > 0; d >>= 1) m = max(m, __shfl_down_sync(kFull, m, d));
+  if ((threadIdx.x & 31u) == 0u && m != 0u) atomicMax(&counters[kMaxQ], (unsigned long long)m);
+}
+
+__global__ void k_record_keys(const RecordKeyArgs a) {
+  typedef unsigned __int128 u128;
+  const u128 nmask = a.n >= 128 ? ~(u128)0 : ((((u128)1) << a.n) - 1);
+  const u128 qmask = a.qbits >= 128 ? ~(u128)0 : ((((u128)1) << a.qbits) - 1);
+  const u128 child = ((u128)a.child_hi << 64) | a.child_lo;
+  const u128 tau = ((u128)a.tau_hi << 64) | a.tau_lo;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.count;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a.records + i * a.record_bytes + a.res_offset);
+    u128 r = 0;
+    for (uint32_t k = 0; k < a.words32 && k < 4u; ++k) r |= ((u128)w[k]) << (32 * k);
+    u128 q = (((r - child) & nmask) >> a.r1) & qmask;
+    if (a.negate) q = (tau - q) & qmask;
+    a.key_lo[i] = static_cast<uint64_t>(q);
+    a.key_hi[i] = static_cast<uint8_t>(q >> 64);
+  }
+}
+
+__global__ void k_authority(const AuthorityArgs a) {
+  typedef unsigned __int128 u128;
+  const u128 nmask = a.n >= 128 ? ~(u128)0 : ((((u128)1) << a.n) - 1);
+  const u128 root = ((u128)a.root_hi << 64) | a.root_lo;
+  unsigned long long c_res = 0, c_struct = 0, c_rule = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.count;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    u128 sum = 0;
+    uint64_t pos[3][2] = {{0, 0}, {0, 0}, {0, 0}}, neg[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int l = 0; l < 3; ++l) {
+      const uint8_t* rec = a.records[l] + static_cast<uint64_t>(a.triples[3 * i + l]) * a.record_bytes;
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(rec + a.res_offset);
+      u128 r = 0;
+      for (uint32_t k = 0; k < a.words32 && k < 4u; ++k) r |= ((u128)w[k]) << (32 * k);
+      sum += r;
+      const uint32_t* pw = reinterpret_cast<const uint32_t*>(rec);
+      for (uint32_t k = 0; k < a.words64 && k < 2u; ++k) {
+        pos[l][k] = (uint64_t)pw[2 * k] | ((uint64_t)pw[2 * k + 1] << 32);
+        neg[l][k] = (uint64_t)pw[2 * (a.words64 + k)] | ((uint64_t)pw[2 * (a.words64 + k) + 1] << 32);
+      }
+    }
+    uint8_t flags = 0;
+    if ((sum & nmask) == root) {
+      flags |= 1;
+      // three-way ternary add of the masks (reference src/packed.cpp:15-38)
+      bool ok = true;
+      uint32_t npos = 0, nneg = 0;
+      for (uint32_t k = 0; k < a.words64 && k < 2u; ++k) {
+        const uint64_t ap = pos[0][k], an = neg[0][k], bp = pos[1][k], bn = neg[1][k];
+        const uint64_t cp = pos[2][k], cn = neg[2][k];
+        const uint64_t pany = ap | bp | cp, nany = an | bn | cn;
+        const uint64_t ptwo = (ap & bp) | (ap & cp) | (bp & cp);
+        const uint64_t ntwo = (an & bn) | (an & cn) | (bn & cn);
+        const uint64_t invalid = (ptwo & ~nany) | (ntwo & ~pany);
+        const uint64_t pp = ((pany & ~ptwo) & ~nany) | (ptwo & nany);
+        const uint64_t pn = ((nany & ~ntwo) & ~pany) | (ntwo & pany);
+        uint64_t valid = ~0ull;
+        if (k + 1 == a.words64 && (a.n % 64u) != 0u) valid = (1ull << (a.n % 64u)) - 1ull;
+        if ((invalid & valid) != 0 || ((pp | pn) & ~valid) != 0) ok = false;
+        npos += __popcll(pp & valid);
+        nneg += __popcll(pn & valid);
+      }
+      if (ok && nneg == 2u && npos == 2u + a.n / 6u) flags |= 2;
+      if (ok && nneg == 0u && npos == a.n / 2u) flags |= 4;
+    }
+    if (a.flags != nullptr) a.flags[i] = flags;
+    c_res += flags & 1;
+    c_struct += (flags >> 1) & 1;
+    c_rule += (flags >> 2) & 1;
+  }
+  if (c_res) atomicAdd(&a.counters[0], c_res);
+  if (c_struct) atomicAdd(&a.counters[1], c_struct);
+  if (c_rule) atomicAdd(&a.counters[2], c_rule);
+}
+
+int grid_for(uint64_t n, int threads) {
+  uint64_t blocks = (n + threads - 1) / threads;
+  if (blocks > 148ull * 16ull) blocks = 148ull * 16ull;
+  return blocks == 0 ? 1 : static_cast<int>(blocks);
+}
+
+}  // namespace
+
+void launch_hist(const uint64_t* key, uint64_t n, uint32_t fmask, uint32_t* cnt, cudaStream_t st) {
+  if (n == 0) return;
+  k_hist<<<grid_for(n, 256), 256, 0, st>>>(key, n, fmask, cnt);
+}
+
+void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor,
+                 cudaStream_t st) {
+  k_scan<<<1, 1024, 0, st>>>(cnt, nfam, off, cursor);
+}
+
+void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, uint64_t n,
+                    uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
+                    uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st) {
+  if (n == 0) return;
+  k_scatter<<<grid_for(n, 256), 256, 0, st>>>(key_lo, key_hi, id, n, fb, fast_mask, hi_mask, cursor,
+                                             res, hi, out_id);
+}
+
+void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters,
+                       cudaStream_t st) {
+  k_max_family<<<(nfam + 255) / 256, 256, 0, st>>>(cnt, nfam, counters);
+}
+
+size_t sweep_smem_bytes(uint32_t wb) {
+  return (static_cast<size_t>(1) << wb) * 4 + kYCap * 4 + (static_cast<size_t>(1) << kYHashBits) * 4 +
+         static_cast<size_t>(kSweepWarps) * kQueueCap * sizeof(uint2);
+}
+
+void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st) {
+  const size_t smem = sweep_smem_bytes(a.wb);
+  const unsigned grid = (1u << a.fb) * a.s_split;
+  if (aligned) {
+    cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sweep<true><<<grid, kSweepThreads, smem, st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sweep<false><<<grid, kSweepThreads, smem, st>>>(a);
+  }
+}
+
+void launch_record_keys(const RecordKeyArgs& a, cudaStream_t st) {
+  if (a.count == 0) return;
+  k_record_keys<<<grid_for(a.count, 256), 256, 0, st>>>(a);
+}
+
+void launch_authority(const AuthorityArgs& a, cudaStream_t st) {
+  if (a.count == 0) return;
+  k_authority<<<grid_for(a.count, 128), 128, 0, st>>>(a);
+}
+
+}  // namespace tergpu

@@ -1,0 +1,98 @@
+// Device side of the B200 root join (L1 -> L0 of the depth-3 TER attempt).
+//
+// Problem: lists A (q), B (x), D (d = tau - q_C) of Q-bit keys; report every
+// (a, b, c) with key_a + key_b == key_c (mod 2^Q), with multiplicity.
+//
+// Layout in HBM after the partition (per list, structure of arrays):
+//   res[i]  uint64  residual key = (key_lo mod 2^F) >> fb      F = min(Q, 64)
+//   hi[i]   uint8   key bits [64, Q)
+//   id[i]   uint32  EntryId reported in triples
+// entries grouped by family f = key_lo mod 2^fb; family f occupies
+// [off[f], off[f] + cnt[f]), off[f] even so two residuals load as one 16-byte word.
+//
+// A cell (s, t) pairs A family s with B family t; its sums land in D family
+// u = (s + t) mod 2^fb with carry kappa = (s + t) >> fb into the residual.
+#pragma once
+
+#include <cstdint>
+
+namespace tergpu {
+
+constexpr int kSweepThreads = 256;
+constexpr int kSweepWarps = kSweepThreads / 32;
+constexpr int kQueueCap = 128;         // survivor slots per warp
+constexpr uint32_t kYHashBits = 12;    // shared exact-lookup table: 4096 slots
+constexpr uint32_t kYCap = 2048;       // D-family entries the shared table takes
+
+struct ListView {
+  const uint64_t* res;
+  const uint8_t* hi;
+  const uint32_t* id;
+  const uint32_t* off;
+  const uint32_t* cnt;
+};
+
+struct SweepArgs {
+  ListView q, x, y;
+  const uint8_t* cells;     // 4096 bytes over the low 6 key bits, or null
+  uint32_t fb;              // family bits
+  uint32_t s_split;         // CTAs per target family
+  uint32_t wb;              // log2 of filter words (filter bits = wb + 5)
+  uint32_t mrb;             // residual bits compared exactly
+  uint32_t rb;              // full residual width (carry into the high byte)
+  uint32_t hi_bits;         // key bits above 64 (0 when Q <= 64)
+  uint32_t project;         // 1: count triples on mrb residual bits only
+  uint32_t* triples;        // 3 * cap
+  unsigned long long cap;
+  unsigned long long* counters;  // [0] triples [1] survivors [2] fast [3] projected [4] fallback
+};
+
+// counters[kMaxQ] holds the largest A family (set by launch_max_family before
+// the sweep reads it), so no host round trip separates partition and sweep.
+enum Counter {
+  kTriples = 0, kSurvivors = 1, kFast = 2, kProjected = 3, kFallback = 4, kMaxQ = 5, kCounters = 8
+};
+
+// Host-callable launchers (root_kernels.cu).
+void launch_hist(const uint64_t* key, uint64_t n, uint32_t fmask, uint32_t* cnt, cudaStream_t st);
+void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor,
+                 cudaStream_t st);
+void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, uint64_t n,
+                    uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
+                    uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st);
+void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters,
+                       cudaStream_t st);
+size_t sweep_smem_bytes(uint32_t wb);
+void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st);
+
+// Keys from captured L1 records: q = ((R - c) mod 2^n) >> r1 over Q bits,
+// list 2 turned into d = tau - q_C.
+struct RecordKeyArgs {
+  const uint8_t* records;
+  uint64_t count;
+  uint32_t record_bytes;
+  uint32_t res_offset;     // 16 * W64
+  uint32_t words32;
+  uint32_t n, r1, qbits;
+  uint64_t child_lo, child_hi;
+  uint64_t tau_lo, tau_hi;
+  int negate;              // list 2
+  uint64_t* key_lo;
+  uint8_t* key_hi;
+};
+void launch_record_keys(const RecordKeyArgs& a, cudaStream_t st);
+
+// Authority chain for the emitted triples: residue sum == T, FiniteSanity
+// structural count, root rule (binary parent of weight n/2).
+struct AuthorityArgs {
+  const uint8_t* records[3];
+  uint32_t record_bytes, res_offset, words32, words64, n;
+  uint64_t root_lo, root_hi;
+  const uint32_t* triples;
+  uint64_t count;
+  uint8_t* flags;
+  unsigned long long* counters;  // [0] residue [1] structural [2] root rule
+};
+void launch_authority(const AuthorityArgs& a, cudaStream_t st);
+
+}  // namespace tergpu

@@ -1,0 +1,628 @@
+// C ABI of the B200 root backend (include/tergpu.h).
+//
+// One workspace per device, grown on demand and reused across calls; calls on
+// the same device are serialized by that workspace's mutex.  Every call checks
+// its predicted device bytes against the caller's ceiling before it allocates
+// anything, so a refused call returns TERGPU_RESOURCE_LIMIT with no partial
+// result (the reference's ResourceLimit contract, src/full_ter.cpp:3174-3185).
+
+#include "tergpu.h"
+#include "root_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace tergpu {
+namespace {
+
+thread_local std::string t_error;
+
+enum Slot {
+  kSlotKeyLo = 0, kSlotKeyHi = 3, kSlotInId = 6, kSlotRes = 9, kSlotHi = 12, kSlotId = 15,
+  kSlotCnt = 18, kSlotOff = 21, kSlotCur = 24, kSlotCells = 27, kSlotTriples = 28,
+  kSlotCounters = 29, kSlotRecords = 30, kSlotFlags = 33, kSlots = 34
+};
+
+struct Buffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct Workspace {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t start = nullptr, mid = nullptr, stop = nullptr;
+  Buffer buf[kSlots];
+  std::mutex mu;
+};
+
+std::mutex g_mu;
+std::vector<std::unique_ptr<Workspace>> g_ws;
+
+struct Failure {
+  int status;
+};
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    t_error = std::string(what) + ": " + cudaGetErrorString(e);
+    throw Failure{e == cudaErrorMemoryAllocation ? TERGPU_RESOURCE_LIMIT : TERGPU_DEVICE_ERROR};
+  }
+}
+
+Workspace& workspace(int device) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  for (auto& w : g_ws) {
+    if (w->device == device) return *w;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    t_error = "no CUDA device " + std::to_string(device);
+    throw Failure{TERGPU_DEVICE_ERROR};
+  }
+  auto w = std::make_unique<Workspace>();
+  w->device = device;
+  check(cudaSetDevice(device), "cudaSetDevice");
+  check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreate(&w->start), "cudaEventCreate");
+  check(cudaEventCreate(&w->mid), "cudaEventCreate");
+  check(cudaEventCreate(&w->stop), "cudaEventCreate");
+  g_ws.push_back(std::move(w));
+  return *g_ws.back();
+}
+
+template <typename T>
+T* ensure(Workspace& w, int slot, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 256);
+  Buffer& b = w.buf[slot];
+  if (b.bytes < bytes) {
+    if (b.ptr != nullptr) check(cudaFree(b.ptr), "cudaFree");
+    b.ptr = nullptr;
+    b.bytes = 0;
+    check(cudaMalloc(&b.ptr, bytes), "cudaMalloc");
+    b.bytes = bytes;
+  }
+  return static_cast<T*>(b.ptr);
+}
+
+uint32_t ceil_log2(uint64_t v) {
+  uint32_t b = 0;
+  while ((1ull << b) < v) ++b;
+  return b;
+}
+
+struct Tuning {
+  uint32_t fb = 6, wb = 12, s_split = 1;
+};
+
+// Family radix: about 1024 D entries per family; the filter: about 256 bits
+// per D entry of the largest-average family (false-pass rate near 1/256).
+Tuning choose_tuning(uint64_t n_d, uint32_t fast_bits, uint32_t projected, uint32_t fb_req,
+                     uint32_t filter_req) {
+  Tuning t;
+  uint32_t fb_max = std::min<uint32_t>(14, fast_bits - 2);
+  if (projected != 0) fb_max = std::min<uint32_t>(fb_max, projected - 6);
+  if (fb_req != 0) {
+    t.fb = fb_req;
+  } else {
+    const double ideal = std::log2(std::max<double>(1.0, static_cast<double>(n_d) / 1024.0));
+    t.fb = static_cast<uint32_t>(std::max(6.0, std::floor(ideal + 0.5)));
+    t.fb = std::min(t.fb, fb_max);
+    t.fb = std::max<uint32_t>(t.fb, 6);
+  }
+  const uint64_t avg = std::max<uint64_t>(1, n_d >> t.fb);
+  if (filter_req != 0) {
+    t.wb = filter_req - 5;
+  } else {
+    t.wb = std::clamp<uint32_t>(ceil_log2(avg * 256) - 5, 10, 14);
+  }
+  const uint32_t nfam = 1u << t.fb;
+  const uint32_t target_ctas = 148 * 2 * 8;
+  t.s_split = std::clamp<uint32_t>((target_ctas + nfam - 1) / nfam, 1, nfam);
+  return t;
+}
+
+// Device-resident inputs of one join: keys per list.
+struct JoinInput {
+  uint32_t quotient_bits;
+  uint64_t count[3];
+  const uint64_t* key_lo[3];  // device
+  const uint8_t* key_hi[3];   // device or null
+  const uint32_t* id[3];      // device or null
+  const uint8_t* cells;       // host or null
+  const uint8_t* cells_device;  // device or null (takes precedence)
+  uint32_t projected_bits;
+  uint32_t family_bits, filter_bits;
+  uint64_t memory_limit_bytes;
+  uint64_t capacity;
+  bool count_only;
+  cudaStream_t stream;
+};
+
+struct JoinResult {
+  uint64_t triples = 0, pairs = 0, survivors = 0, fast = 0, projected = 0;
+  uint64_t device_bytes = 0;
+  float join_ms = 0, partition_ms = 0, sweep_ms = 0;
+  uint32_t launches = 0;
+  Tuning tuning;
+  uint32_t* d_triples = nullptr;
+};
+
+uint64_t partition_bytes(const uint64_t count[3], uint32_t fb) {
+  uint64_t b = 0;
+  for (int l = 0; l < 3; ++l) {
+    const uint64_t slots = count[l] + (1ull << fb) + 16;
+    b += slots * (8 + 1 + 4);
+    b += 3ull * ((1ull << fb) + 1) * 4;
+  }
+  return b;
+}
+
+// Partition + sweep(s) on keys already on the device.  The only host
+// synchronization is the final download of counters and family sizes.
+JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
+  JoinResult r;
+  const uint32_t Q = in.quotient_bits;
+  const uint32_t F = std::min<uint32_t>(Q, 64);
+  const uint32_t hi_bits = Q - F;
+  r.tuning = choose_tuning(in.count[2], F, in.projected_bits, in.family_bits, in.filter_bits);
+  const Tuning& tu = r.tuning;
+  if (tu.fb < 6 || tu.fb > 16 || tu.fb + 2 > F || tu.wb < 5 || tu.wb > 15 ||
+      (in.projected_bits != 0 && (in.projected_bits > F || in.projected_bits < tu.fb + 1))) {
+    t_error = "family/filter bits outside the supported range for this quotient width";
+    throw Failure{TERGPU_INVALID_INPUT};
+  }
+  const uint32_t nfam = 1u << tu.fb;
+  const uint64_t fast_mask = F >= 64 ? ~0ull : ((1ull << F) - 1ull);
+  const uint64_t need = input_bytes + partition_bytes(in.count, tu.fb) +
+                        (in.count_only ? 0 : in.capacity * 12) + 4096 + 64;
+  r.device_bytes = need;
+  if (in.memory_limit_bytes != 0 && need > in.memory_limit_bytes) {
+    t_error = "predicted device bytes " + std::to_string(need) + " exceed the ceiling " +
+              std::to_string(in.memory_limit_bytes);
+    throw Failure{TERGPU_RESOURCE_LIMIT};
+  }
+  cudaStream_t st = in.stream;
+  ListView views[3];
+  uint64_t* res[3];
+  uint8_t* hi[3];
+  uint32_t* ids[3];
+  uint32_t *cnt[3], *off[3], *cur[3];
+  for (int l = 0; l < 3; ++l) {
+    const uint64_t slots = in.count[l] + nfam + 16;
+    res[l] = ensure<uint64_t>(w, kSlotRes + l, slots * 8);
+    hi[l] = ensure<uint8_t>(w, kSlotHi + l, slots);
+    ids[l] = ensure<uint32_t>(w, kSlotId + l, slots * 4);
+    cnt[l] = ensure<uint32_t>(w, kSlotCnt + l, (nfam + 1) * 4ull);
+    off[l] = ensure<uint32_t>(w, kSlotOff + l, (nfam + 1) * 4ull);
+    cur[l] = ensure<uint32_t>(w, kSlotCur + l, (nfam + 1) * 4ull);
+  }
+  unsigned long long* counters = ensure<unsigned long long>(w, kSlotCounters, kCounters * 8);
+  uint32_t* d_triples = ensure<uint32_t>(w, kSlotTriples, std::max<uint64_t>(in.capacity, 1) * 12);
+  const uint8_t* d_cells = in.cells_device;
+  if (d_cells == nullptr && in.cells != nullptr) {
+    uint8_t* c = ensure<uint8_t>(w, kSlotCells, 4096);
+    check(cudaMemcpyAsync(c, in.cells, 4096, cudaMemcpyHostToDevice, st), "cells upload");
+    d_cells = c;
+  }
+  check(cudaEventRecord(w.start, st), "event");
+  check(cudaMemsetAsync(counters, 0, kCounters * 8, st), "memset");
+  for (int l = 0; l < 3; ++l) {
+    check(cudaMemsetAsync(cnt[l], 0, nfam * 4ull, st), "memset");
+    launch_hist(in.key_lo[l], in.count[l], nfam - 1, cnt[l], st);
+    launch_scan(cnt[l], nfam, off[l], cur[l], st);
+    launch_scatter(in.key_lo[l], in.key_hi[l], in.id[l], in.count[l], tu.fb, fast_mask,
+                   hi_bits ? ((1u << hi_bits) - 1u) : 0u, cur[l], res[l], hi[l], ids[l], st);
+    views[l] = ListView{res[l], hi[l], ids[l], off[l], cnt[l]};
+    r.launches += (in.count[l] != 0 ? 2 : 0) + 1;
+  }
+  launch_max_family(cnt[0], nfam, counters, st);
+  r.launches += 1;
+  check(cudaGetLastError(), "partition launch");
+  check(cudaEventRecord(w.mid, st), "event");
+  SweepArgs a{};
+  a.q = views[0];
+  a.x = views[1];
+  a.y = views[2];
+  a.cells = d_cells;
+  a.fb = tu.fb;
+  a.s_split = tu.s_split;
+  a.wb = tu.wb;
+  a.rb = F - tu.fb;
+  a.hi_bits = hi_bits;
+  a.triples = d_triples;
+  a.cap = in.count_only ? 0 : in.capacity;
+  a.counters = counters;
+  if (!in.count_only || in.projected_bits == 0) {
+    a.project = 0;
+    a.mrb = F - tu.fb;
+    launch_sweep(a, a.mrb < 32, st);
+    r.launches += 1;
+  }
+  if (in.projected_bits != 0) {
+    a.project = 1;
+    a.mrb = in.projected_bits - tu.fb;
+    launch_sweep(a, a.mrb < 32, st);
+    r.launches += 1;
+  }
+  check(cudaGetLastError(), "sweep launch");
+  check(cudaEventRecord(w.stop, st), "event");
+  unsigned long long hc[kCounters];
+  std::vector<uint32_t> hcnt[2];
+  check(cudaMemcpyAsync(hc, counters, sizeof hc, cudaMemcpyDeviceToHost, st), "counters");
+  for (int l = 0; l < 2; ++l) {
+    hcnt[l].resize(nfam);
+    check(cudaMemcpyAsync(hcnt[l].data(), cnt[l], nfam * 4ull, cudaMemcpyDeviceToHost, st),
+          "count download");
+  }
+  check(cudaStreamSynchronize(st), "join");
+  check(cudaEventElapsedTime(&r.join_ms, w.start, w.stop), "elapsed");
+  check(cudaEventElapsedTime(&r.partition_ms, w.start, w.mid), "elapsed");
+  check(cudaEventElapsedTime(&r.sweep_ms, w.mid, w.stop), "elapsed");
+  std::vector<uint8_t> hcells;
+  if (d_cells != nullptr) {
+    hcells.resize(4096);
+    if (in.cells != nullptr) {
+      std::memcpy(hcells.data(), in.cells, 4096);
+    } else {
+      check(cudaMemcpy(hcells.data(), d_cells, 4096, cudaMemcpyDeviceToHost), "cells download");
+    }
+  }
+  for (uint32_t s = 0; s < nfam; ++s) {
+    for (uint32_t t = 0; t < nfam; ++t) {
+      if (!hcells.empty() && hcells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
+      r.pairs += static_cast<uint64_t>(hcnt[0][s]) * hcnt[1][t];
+    }
+  }
+  r.triples = hc[kTriples];
+  r.survivors = hc[kSurvivors];
+  r.fast = hc[kFast];
+  r.projected = hc[kProjected];
+  r.d_triples = d_triples;
+  return r;
+}
+
+void fill_out(const JoinResult& j, tergpu_root_out* out) {
+  out->triples_count = j.triples;
+  out->logical_pairs = j.pairs;
+  out->filter_survivors = j.survivors;
+  out->fast_hits = j.fast;
+  out->projected_hits = j.projected;
+  out->device_bytes = j.device_bytes;
+  out->join_ms = j.join_ms;
+  out->partition_ms = j.partition_ms;
+  out->sweep_ms = j.sweep_ms;
+  out->family_bits = j.tuning.fb;
+  out->filter_bits = j.tuning.wb + 5;
+  out->kernel_launches = j.launches;
+}
+
+int guarded(const char* what, int (*body)(const void*, void*), const void* in, void* out) {
+  (void)what;
+  t_error.clear();
+  try {
+    return body(in, out);
+  } catch (const Failure& f) {
+    return f.status;
+  } catch (const std::bad_alloc&) {
+    t_error = "host allocation failed";
+    return TERGPU_RESOURCE_LIMIT;
+  } catch (...) {
+    t_error = "unexpected exception";
+    return TERGPU_DEVICE_ERROR;
+  }
+}
+
+int root_run_body(const void* vin, void* vout) {
+  const auto* in = static_cast<const tergpu_root_in*>(vin);
+  auto* out = static_cast<tergpu_root_out*>(vout);
+  const auto t0 = std::chrono::steady_clock::now();
+  if (in == nullptr || out == nullptr) {
+    t_error = "null argument";
+    return TERGPU_INVALID_INPUT;
+  }
+  const uint32_t Q = in->quotient_bits;
+  if (Q < 8 || Q > TERGPU_MAX_QUOTIENT_BITS) {
+    t_error = "quotient width outside [8, 72]";
+    return TERGPU_UNSUPPORTED_WIDTH;
+  }
+  const bool count_only = (in->flags & TERGPU_ROOT_COUNT_ONLY) != 0;
+  const bool resident = (in->flags & TERGPU_ROOT_DEVICE_INPUTS) != 0;
+  for (int l = 0; l < 3; ++l) {
+    if (in->count[l] >= 0x80000000ull || (in->count[l] != 0 && in->key_lo[l] == nullptr) ||
+        (Q > 64 && in->count[l] != 0 && in->key_hi[l] == nullptr)) {
+      t_error = "list pointers or sizes invalid";
+      return TERGPU_INVALID_INPUT;
+    }
+  }
+  if (!count_only && out->capacity != 0 && out->triples == nullptr) {
+    t_error = "triples buffer missing";
+    return TERGPU_INVALID_INPUT;
+  }
+  Workspace& w = workspace(in->device);
+  std::lock_guard<std::mutex> lock(w.mu);
+  check(cudaSetDevice(w.device), "cudaSetDevice");
+  cudaStream_t st = in->stream != nullptr ? static_cast<cudaStream_t>(in->stream) : w.stream;
+  uint64_t input_bytes = 0;
+  if (!resident) {
+    for (int l = 0; l < 3; ++l) input_bytes += in->count[l] * 13 + 64;
+  }
+  if (in->memory_limit_bytes != 0 && input_bytes > in->memory_limit_bytes) {
+    t_error = "input keys alone exceed the device ceiling";
+    return TERGPU_RESOURCE_LIMIT;
+  }
+  JoinInput j{};
+  j.quotient_bits = Q;
+  j.stream = st;
+  for (int l = 0; l < 3; ++l) {
+    j.count[l] = in->count[l];
+    if (resident) {
+      j.key_lo[l] = in->key_lo[l];
+      j.key_hi[l] = Q > 64 ? in->key_hi[l] : nullptr;
+      j.id[l] = in->id[l];
+      continue;
+    }
+    uint64_t* dlo = ensure<uint64_t>(w, kSlotKeyLo + l, in->count[l] * 8 + 8);
+    if (in->count[l]) {
+      check(cudaMemcpyAsync(dlo, in->key_lo[l], in->count[l] * 8, cudaMemcpyHostToDevice, st),
+            "key upload");
+    }
+    j.key_lo[l] = dlo;
+    j.key_hi[l] = nullptr;
+    if (Q > 64) {
+      uint8_t* dhi = ensure<uint8_t>(w, kSlotKeyHi + l, in->count[l] + 8);
+      if (in->count[l]) {
+        check(cudaMemcpyAsync(dhi, in->key_hi[l], in->count[l], cudaMemcpyHostToDevice, st),
+              "key upload");
+      }
+      j.key_hi[l] = dhi;
+    }
+    j.id[l] = nullptr;
+    if (in->id[l] != nullptr) {
+      uint32_t* did = ensure<uint32_t>(w, kSlotInId + l, in->count[l] * 4 + 8);
+      if (in->count[l]) {
+        check(cudaMemcpyAsync(did, in->id[l], in->count[l] * 4, cudaMemcpyHostToDevice, st),
+              "id upload");
+      }
+      j.id[l] = did;
+    }
+  }
+  j.cells = resident ? nullptr : in->cells;
+  j.cells_device = resident ? in->cells : nullptr;
+  j.projected_bits = in->projected_bits;
+  j.family_bits = in->family_bits;
+  j.filter_bits = in->filter_bits;
+  j.memory_limit_bytes = in->memory_limit_bytes;
+  j.capacity = count_only ? 0 : out->capacity;
+  j.count_only = count_only;
+  const JoinResult res = run_join(w, j, input_bytes);
+  fill_out(res, out);
+  int status = TERGPU_COMPLETED;
+  if (!count_only) {
+    if (res.triples > out->capacity) {
+      status = TERGPU_OUTPUT_OVERFLOW;
+    } else if (res.triples != 0) {
+      check(cudaMemcpyAsync(out->triples, res.d_triples, res.triples * 12, cudaMemcpyDeviceToHost,
+                            st), "triples download");
+      check(cudaStreamSynchronize(st), "triples download");
+    }
+  }
+  out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return status;
+}
+
+typedef unsigned __int128 u128;
+
+u128 words_to_u128(const uint32_t* w, uint32_t words) {
+  u128 v = 0;
+  for (uint32_t k = 0; k < words && k < 4; ++k) v |= ((u128)w[k]) << (32 * k);
+  return v;
+}
+
+int root_records_body(const void* vin, void* vout) {
+  const auto* in = static_cast<const tergpu_root_records_in*>(vin);
+  auto* out = static_cast<tergpu_root_records_out*>(vout);
+  const auto t0 = std::chrono::steady_clock::now();
+  if (in == nullptr || out == nullptr) {
+    t_error = "null argument";
+    return TERGPU_INVALID_INPUT;
+  }
+  const uint32_t n = in->n;
+  if (n == 0 || n % 36 != 0 || n > 128 || in->r1 == 0 || in->r1 >= n) {
+    t_error = "records root requires 36 | n <= 128 and 0 < r1 < n";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
+  const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
+  if (in->record_bytes != 16 * w64 + 4 * w32) {
+    t_error = "record_bytes does not match n";
+    return TERGPU_INVALID_INPUT;
+  }
+  const uint32_t Q = n - in->r1;
+  if (Q < 8 || Q > TERGPU_MAX_QUOTIENT_BITS) {
+    t_error = "root quotient width outside [8, 72]";
+    return TERGPU_UNSUPPORTED_WIDTH;
+  }
+  for (int l = 0; l < 3; ++l) {
+    if (in->count[l] >= 0x80000000ull || (in->count[l] && in->records[l] == nullptr) ||
+        in->child_target[l] == nullptr) {
+      t_error = "record lists invalid";
+      return TERGPU_INVALID_INPUT;
+    }
+  }
+  if (in->root_target == nullptr) {
+    t_error = "root target missing";
+    return TERGPU_INVALID_INPUT;
+  }
+  const bool count_only = (in->flags & TERGPU_ROOT_COUNT_ONLY) != 0;
+  if (!count_only && out->root.capacity != 0 && out->root.triples == nullptr) {
+    t_error = "triples buffer missing";
+    return TERGPU_INVALID_INPUT;
+  }
+  const u128 nmask = n >= 128 ? ~(u128)0 : ((((u128)1) << n) - 1);
+  const u128 T = words_to_u128(in->root_target, w32) & nmask;
+  u128 c[3];
+  u128 tau_res = T;
+  for (int l = 0; l < 3; ++l) {
+    c[l] = words_to_u128(in->child_target[l], w32) & nmask;
+    tau_res = (tau_res - c[l]) & nmask;
+  }
+  const u128 qmask = Q >= 128 ? ~(u128)0 : ((((u128)1) << Q) - 1);
+  const u128 tau = (tau_res >> in->r1) & qmask;
+  out->tau_lo = static_cast<uint64_t>(tau);
+  out->tau_hi = static_cast<uint64_t>(tau >> 64);
+
+  Workspace& w = workspace(in->device);
+  std::lock_guard<std::mutex> lock(w.mu);
+  check(cudaSetDevice(w.device), "cudaSetDevice");
+  uint64_t input_bytes = 0;
+  for (int l = 0; l < 3; ++l) input_bytes += in->count[l] * (in->record_bytes + 9) + 64;
+  if (in->memory_limit_bytes != 0 && input_bytes > in->memory_limit_bytes) {
+    t_error = "input records alone exceed the device ceiling";
+    return TERGPU_RESOURCE_LIMIT;
+  }
+  JoinInput j{};
+  j.quotient_bits = Q;
+  j.stream = w.stream;
+  uint8_t* drec[3];
+  for (int l = 0; l < 3; ++l) {
+    j.count[l] = in->count[l];
+    drec[l] = ensure<uint8_t>(w, kSlotRecords + l, in->count[l] * in->record_bytes + 16);
+    if (in->count[l]) {
+      check(cudaMemcpyAsync(drec[l], in->records[l], in->count[l] * in->record_bytes,
+                            cudaMemcpyHostToDevice, w.stream), "records upload");
+    }
+    uint64_t* dlo = ensure<uint64_t>(w, kSlotKeyLo + l, in->count[l] * 8 + 8);
+    uint8_t* dhi = ensure<uint8_t>(w, kSlotKeyHi + l, in->count[l] + 8);
+    RecordKeyArgs k{};
+    k.records = drec[l];
+    k.count = in->count[l];
+    k.record_bytes = in->record_bytes;
+    k.res_offset = 16 * w64;
+    k.words32 = w32;
+    k.n = n;
+    k.r1 = in->r1;
+    k.qbits = Q;
+    k.child_lo = static_cast<uint64_t>(c[l]);
+    k.child_hi = static_cast<uint64_t>(c[l] >> 64);
+    k.tau_lo = out->tau_lo;
+    k.tau_hi = out->tau_hi;
+    k.negate = l == 2;
+    k.key_lo = dlo;
+    k.key_hi = dhi;
+    launch_record_keys(k, w.stream);
+    j.key_lo[l] = dlo;
+    j.key_hi[l] = dhi;
+    j.id[l] = nullptr;
+  }
+  check(cudaGetLastError(), "key derivation");
+  j.cells = in->cells;
+  j.projected_bits = in->projected_bits;
+  j.family_bits = in->family_bits;
+  j.filter_bits = in->filter_bits;
+  j.memory_limit_bytes = in->memory_limit_bytes;
+  j.capacity = count_only ? 0 : out->root.capacity;
+  j.count_only = count_only;
+  const JoinResult res = run_join(w, j, input_bytes);
+  fill_out(res, &out->root);
+  out->residue_exact = out->structural = out->valid_roots = 0;
+  int status = TERGPU_COMPLETED;
+  if (!count_only) {
+    if (res.triples > out->root.capacity) {
+      status = TERGPU_OUTPUT_OVERFLOW;
+    } else if (res.triples != 0) {
+      uint8_t* dflags = ensure<uint8_t>(w, kSlotFlags, res.triples + 16);
+      unsigned long long* counters = ensure<unsigned long long>(w, kSlotCounters, kCounters * 8);
+      check(cudaMemsetAsync(counters, 0, kCounters * 8, w.stream), "memset");
+      AuthorityArgs au{};
+      for (int l = 0; l < 3; ++l) au.records[l] = drec[l];
+      au.record_bytes = in->record_bytes;
+      au.res_offset = 16 * w64;
+      au.words32 = w32;
+      au.words64 = w64;
+      au.n = n;
+      au.root_lo = static_cast<uint64_t>(T);
+      au.root_hi = static_cast<uint64_t>(T >> 64);
+      au.triples = res.d_triples;
+      au.count = res.triples;
+      au.flags = dflags;
+      au.counters = counters;
+      launch_authority(au, w.stream);
+      check(cudaGetLastError(), "authority launch");
+      unsigned long long hc[3];
+      check(cudaMemcpyAsync(hc, counters, sizeof hc, cudaMemcpyDeviceToHost, w.stream), "counters");
+      check(cudaMemcpyAsync(out->root.triples, res.d_triples, res.triples * 12,
+                            cudaMemcpyDeviceToHost, w.stream), "triples download");
+      if (out->triple_flags != nullptr) {
+        check(cudaMemcpyAsync(out->triple_flags, dflags, res.triples, cudaMemcpyDeviceToHost,
+                              w.stream), "flags download");
+      }
+      check(cudaStreamSynchronize(w.stream), "authority");
+      out->residue_exact = hc[0];
+      out->structural = hc[1];
+      out->valid_roots = hc[2];
+    }
+  }
+  out->root.total_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return status;
+}
+
+}  // namespace
+}  // namespace tergpu
+
+extern "C" {
+
+int tergpu_root_run(const tergpu_root_in* in, tergpu_root_out* out) {
+  return tergpu::guarded("tergpu_root_run", tergpu::root_run_body, in, out);
+}
+
+int tergpu_root_run_records(const tergpu_root_records_in* in, tergpu_root_records_out* out) {
+  return tergpu::guarded("tergpu_root_run_records", tergpu::root_records_body, in, out);
+}
+
+int tergpu_device_count(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) return 0;
+  return count;
+}
+
+int tergpu_abi_version(void) { return TERGPU_ABI_VERSION; }
+
+uint64_t tergpu_fnv1a(const void* bytes, uint64_t size, uint64_t state) {
+  const auto* p = static_cast<const uint8_t*>(bytes);
+  for (uint64_t i = 0; i < size; ++i) {
+    state ^= p[i];
+    state *= 0x100000001b3ULL;
+  }
+  return state;
+}
+
+void tergpu_release(void) {
+  std::lock_guard<std::mutex> lock(tergpu::g_mu);
+  for (auto& w : tergpu::g_ws) {
+    std::lock_guard<std::mutex> inner(w->mu);
+    cudaSetDevice(w->device);
+    for (auto& b : w->buf) {
+      if (b.ptr != nullptr) cudaFree(b.ptr);
+      b.ptr = nullptr;
+      b.bytes = 0;
+    }
+    if (w->start) cudaEventDestroy(w->start);
+    if (w->mid) cudaEventDestroy(w->mid);
+    if (w->stop) cudaEventDestroy(w->stop);
+    if (w->stream) cudaStreamDestroy(w->stream);
+  }
+  tergpu::g_ws.clear();
+}
+
+const char* tergpu_last_error(void) { return tergpu::t_error.c_str(); }
+
+}  // extern "C"

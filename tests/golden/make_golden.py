@@ -1,0 +1,98 @@
+"""Regenerates tests/golden/ from the reference's own compiled code.
+
+Run on a machine where oracle/_ref/terref was built from the reference sources
+(python __graft_entry__.py, then python tests/golden/make_golden.py).  Every
+number written here is printed by the reference itself (solve_full_ter,
+capture_to_file, the frozen K2 / K2_WIDE / ARWLF backends, the synthetic-root
+brute-force oracle of ter2_root/tests/ter_synthetic_root.hpp); nothing is typed
+in by hand.
+"""
+from __future__ import annotations
+
+import json
+import sys
+import tempfile
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent / "oracle"))
+import oracle as O  # noqa: E402
+
+ANCHOR_SEED = 19797034556212562  # the reference's authentic n=72 anchor seed
+
+
+def n36_attempts():
+    out = []
+    for kind in ("auth", "build"):
+        for seed in (ANCHOR_SEED, 0x1001, 0x2A):
+            rows = O.ref_run("solve", 36, seed, 8, kind, "canon", 0)
+            out.append({"kind": kind, "seed": seed, "attempts": rows[:-1], "final": rows[-1]})
+    return out
+
+
+def synthetic_roots(tmp: Path):
+    out = []
+    # the configurations of ter2_root/tests/ter_arwlf_tests.cpp:302-307
+    for bits, seed, size, pool in ((69, 0x1234, 2000, 0), (47, 0x5555, 2000, 0),
+                                   (69, 0x9876, 600, 16), (47, 0x4242, 600, 16),
+                                   (69, 0x3131, 600, 1), (47, 0x2727, 600, 1)):
+        path = tmp / f"s{bits}_{seed:x}.keys"
+        brute = O.ref_run("synth", bits, seed, size, pool, path)[0]
+        arwlf = O.ref_run("keysroot", path, "arwlf", 4096, 1, 0)[0]
+        sub = O.ref_run("keysroot", path, "arwlf", 700, 1, 0)[0]
+        out.append({"bits": bits, "seed": seed, "size": size, "pool": pool, "sizes": brute["sizes"],
+                    "brute": {k: brute[k] for k in ("triples", "triple_sum", "triple_xor", "triple_sum2")},
+                    "arwlf": {k: arwlf[k] for k in ("triples", "triple_sum", "triple_xor", "triple_sum2",
+                                                    "projected_hits", "projected_bits",
+                                                    "logical_pairs")},
+                    "subsample700": {k: sub[k] for k in ("triples", "triple_sum", "triple_xor",
+                                                         "triple_sum2", "logical_pairs")}})
+    return out
+
+
+def n72_roots(tmp: Path):
+    out = []
+    for seed, attempt in ((ANCHOR_SEED, 0), (0x7201, 0), (0x7201, 21)):
+        snap = tmp / f"n72_{seed:x}_{attempt}.snap"
+        cap = O.ref_run("capture", 72, seed, attempt, "auth", snap)[0]
+        row = {"seed": seed, "attempt": attempt, "level1": cap["level1"], "level2": cap["level2"],
+               "file_bytes": cap["file_bytes"]}
+        k2 = O.ref_run("snaproot", snap, "k2", 4096, 0)[0]
+        wide = O.ref_run("snaproot", snap, "k2wide", 4096, 0)[0]
+        a32 = O.ref_run("snaproot", snap, "arwlf", 4096, 32)[0]
+        keep = ("triples", "triple_sum", "triple_xor", "triple_sum2", "full_q", "residue",
+                "residue_sum", "structural", "witnesses", "pairs")
+        row["k2"] = {k: k2[k] for k in keep}
+        row["k2wide"] = {k: wide[k] for k in keep}
+        row["k2wide"]["projected_hits_25"] = wide["projected_hits"]
+        row["arwlf_k32_projected_hits"] = a32["projected_hits"]
+        sub = O.ref_run("snaproot", snap, "k2wide", 512, 0)[0]
+        row["k2wide_subsample512"] = {k: sub[k] for k in keep}
+        out.append(row)
+    return out
+
+
+def n36_snapshot(tmp: Path):
+    path = HERE / "n36_anchor_a0.snap"
+    cap = O.ref_run("capture", 36, ANCHOR_SEED, 0, "auth", path)[0]
+    return {"path": path.name, "level1": cap["level1"], "level2": cap["level2"],
+            "file_bytes": cap["file_bytes"]}
+
+
+def main():
+    if not O.ref_available():
+        raise SystemExit("oracle/_ref/terref missing: build it where the reference sources exist")
+    with tempfile.TemporaryDirectory() as d:
+        tmp = Path(d)
+        golden = {
+            "n36_attempts": n36_attempts(),
+            "n36_snapshot": n36_snapshot(tmp),
+            "synthetic_roots": synthetic_roots(tmp),
+            "n72_roots": n72_roots(tmp),
+        }
+    (HERE / "reference_golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True) + "\n")
+    print("wrote", HERE / "reference_golden.json")
+
+
+if __name__ == "__main__":
+    main()

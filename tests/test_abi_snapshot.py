@@ -1,0 +1,108 @@
+"""C-ABI library loading and the .snap reader/writer (CPU only, no device compute)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, ROOT
+
+
+def test_library_exports_every_declared_symbol():
+    from tergpu import _abi
+
+    lib = _abi.load()
+    header = (ROOT / "include" / "tergpu.h").read_text()
+    declared = set(re.findall(r"^\w[\w \*]*?\b(tergpu_\w+)\s*\(", header, flags=re.M))
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(_abi.EXPORTED) <= declared
+    assert lib.tergpu_abi_version() == 1
+
+
+def test_fnv1a_known_answers():
+    from tergpu import snapshot
+
+    assert snapshot.fnv1a(b"") == 0xcbf29ce484222325
+    assert snapshot.fnv1a(b"a") == 0xaf63dc4c8601ec8c
+    assert snapshot.fnv1a(b"foobar") == 0x85944171f73967e8
+
+
+def test_adapter_header_declares_hash_join_signature():
+    text = (ROOT / "subset-sum-ter-fft_b200" / "adapter" / "ter_gpu_root.hpp").read_text()
+    assert re.search(r"Status run_gpu_root\(const mr8::Dataset& data, const rg::RootIndex& index,\s*"
+                     r"const a64::FamilyKeys& keys, const Config& config,\s*"
+                     r"rg::RootSink& sink, Telemetry\* telemetry", text)
+
+
+def test_snapshot_load_matches_reference_capture(golden):
+    from tergpu import snapshot
+
+    g = golden["n36_snapshot"]
+    snap = snapshot.load(GOLDEN_DIR / g["path"])
+    assert snap.entries == g["level1"]
+    assert snap.level2_sizes == g["level2"]
+    assert snap.n == 36 and snap.r1 == 12 and snap.r2 == 3
+    assert (GOLDEN_DIR / g["path"]).stat().st_size == g["file_bytes"]
+    pos, neg = snap.masks(0)
+    assert not np.any(neg) and all(bin(int(p)).count("1") == 6 for p in pos[:, 0])
+
+
+def test_snapshot_roundtrip_is_byte_identical(tmp_path, golden):
+    from tergpu import snapshot
+
+    src = GOLDEN_DIR / golden["n36_snapshot"]["path"]
+    snap = snapshot.load(src)
+    out = tmp_path / "copy.snap"
+    snapshot.save(snap, out, git_commit="reference")
+    a, b = src.read_bytes(), out.read_bytes()
+    # identical lists, targets and checksums; the writer does not carry the
+    # capture-only telemetry fields (peak bytes, elapsed ns, memory limit)
+    assert a[424:] == b[424:]
+    ha = np.frombuffer(a[:424], dtype=snapshot.HEADER_DTYPE)[0]
+    hb = np.frombuffer(b[:424], dtype=snapshot.HEADER_DTYPE)[0]
+    for f in ("n", "r1", "r2", "entries", "offset", "checksum", "child_target", "root_target",
+              "level2_sizes", "seed", "attempt_seed", "attempt"):
+        assert np.array_equal(ha[f], hb[f]), f
+    assert snapshot.load(out).entries == snap.entries
+
+
+def test_snapshot_damage_is_rejected(tmp_path, golden):
+    from tergpu import snapshot
+
+    src = GOLDEN_DIR / golden["n36_snapshot"]["path"]
+    raw = bytearray(src.read_bytes())
+    for where in (10, 500, len(raw) - 3):
+        bad = bytearray(raw)
+        bad[where] ^= 0x40
+        p = tmp_path / f"bad{where}.snap"
+        p.write_bytes(bytes(bad))
+        with pytest.raises(snapshot.SnapshotError):
+            snapshot.load(p)
+    p = tmp_path / "trunc.snap"
+    p.write_bytes(bytes(raw[:-5]))
+    with pytest.raises(snapshot.SnapshotError):
+        snapshot.load(p)
+
+
+def test_host_key_derivation_matches_oracle_attempt(oracle_mod, golden):
+    """Keys from the reference's n=36 capture equal the oracle's quotients."""
+    from tergpu import snapshot
+
+    snap = snapshot.load(GOLDEN_DIR / golden["n36_snapshot"]["path"])
+    Q, lo, hi, tau = snapshot.root_keys(snap)
+    assert Q == 24
+    att = oracle_mod.attempt(36, 19797034556212562, 0, export_l1=True)
+    r1 = att["r1"]
+    for l in range(3):
+        res = att["l1"]["res_lo"][l].astype(object) | (att["l1"]["res_hi"][l].astype(object) << 64)
+        q = [(((int(r) - att["t1"][l]) % (1 << 36)) >> r1) for r in res]
+        if l == 2:
+            q = [(tau - v) % (1 << Q) for v in q]
+        assert [int(v) for v in lo[l]] == q
+    # the oracle's full-Q join over these keys reproduces the reference's root stage
+    d, _ = oracle_mod.root_join(Q, lo, [h.astype(np.uint64) for h in hi])
+    row = golden["n36_attempts"][0]["attempts"][0]
+    assert d["triples"] == row["root_modular"]

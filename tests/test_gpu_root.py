@@ -1,0 +1,212 @@
+"""GPU root parity: libtergpu.so through its C ABI against the oracle and the
+reference's own outputs (golden fixtures, and the reference harness when it
+was built)."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, hexint
+
+pytestmark = pytest.mark.gpu
+
+ANCHOR_SEED = 19797034556212562
+DIGEST_KEYS = ("triples", "triple_sum", "triple_xor", "triple_sum2")
+
+
+@pytest.fixture(scope="module")
+def tg():
+    import tergpu
+
+    if tergpu.device_count() < 1:
+        raise RuntimeError("the GPU tests need a CUDA device and libtergpu.so")
+    return tergpu
+
+
+def keys_of(oracle_mod, bits, seed, size, pool):
+    import tergpu
+
+    lo, hi = oracle_mod.synthetic_root(bits, seed, size, pool)
+    return lo, hi, tergpu.RootKeys(quotient_bits=bits, lo=lo, hi=[h.astype(np.uint8) for h in hi])
+
+
+def assert_digest(got, expected):
+    for k in DIGEST_KEYS:
+        assert got[k] == hexint(expected[k]), (k, got[k], expected[k])
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case):
+    from tergpu import workload
+
+    g = golden["synthetic_roots"][case]
+    lo, hi, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
+    res = tg.run_gpu_root(keys, tg.Config(projected_bits=g["arwlf"]["projected_bits"]))
+    assert_digest(workload.digest(res.triples), g["brute"])
+    assert res.telemetry.logical_pairs == g["arwlf"]["logical_pairs"]
+    assert res.telemetry.projected_hits == g["arwlf"]["projected_hits"]
+    assert res.telemetry.full_hits == g["brute"]["triples"]
+    # the reference's declared 700-cell subsample
+    sub = tg.run_gpu_root(keys, tg.Config(), cells=oracle_mod.select_cells(700))
+    assert_digest(workload.digest(sub.triples), g["subsample700"])
+    assert sub.telemetry.logical_pairs == g["subsample700"]["logical_pairs"]
+
+
+@pytest.mark.parametrize("fb,filt", [(6, 10), (6, 19), (7, 12), (8, 15), (9, 20), (10, 11)])
+def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt):
+    from tergpu import workload
+
+    g = golden["synthetic_roots"][0]
+    _, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
+    res = tg.run_gpu_root(keys, tg.Config(family_bits=fb, filter_bits=filt))
+    assert res.telemetry.family_bits == fb and res.telemetry.filter_bits == filt
+    assert_digest(workload.digest(res.triples), g["brute"])
+
+
+@pytest.mark.parametrize("bits", [24, 33, 40, 47, 58, 64, 65, 69, 72])
+def test_widths_against_oracle(tg, oracle_mod, bits):
+    """Every key width from the n=36 root (24) to the one-byte high limit (72),
+    with the carry, multiplicity and high-bit plants; projected counts at two k."""
+    from tergpu import workload
+
+    lo, hi, keys = keys_of(oracle_mod, bits, 0xABC0 + bits, 3000, 0)
+    expected, _ = oracle_mod.root_join(bits, lo, hi)
+    k = min(bits, 64) - 3
+    res = tg.run_gpu_root(keys, tg.Config(projected_bits=k))
+    got = workload.digest(res.triples)
+    for key in DIGEST_KEYS:
+        assert got[key] == expected[key], key
+    assert res.telemetry.projected_hits == oracle_mod.projected_count(k, lo)
+
+
+def test_dense_skewed_families_against_oracle(tg, oracle_mod):
+    """pool=1: every key shares its low 19 bits, so one family holds everything."""
+    from tergpu import workload
+
+    lo, hi, keys = keys_of(oracle_mod, 69, 0x3131, 3000, 1)
+    expected, _ = oracle_mod.root_join(69, lo, hi)
+    res = tg.run_gpu_root(keys, tg.Config())
+    assert workload.digest(res.triples)["triple_sum"] == expected["triple_sum"]
+    assert res.telemetry.full_hits == expected["triples"]
+
+
+def test_output_capacity_retry_and_count_only(tg, oracle_mod, golden):
+    from tergpu import workload
+
+    g = golden["synthetic_roots"][1]
+    _, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
+    res = tg.run_gpu_root(keys, tg.Config(capacity=1))
+    assert_digest(workload.digest(res.triples), g["brute"])
+    cnt = tg.run_gpu_root(keys, tg.Config(count_only=True))
+    assert cnt.telemetry.full_hits == g["brute"]["triples"] and len(cnt.triples) == 0
+
+
+def test_resource_limit_and_invalid_width(tg, oracle_mod):
+    _, _, keys = keys_of(oracle_mod, 69, 1, 500, 0)
+    with pytest.raises(tg.TergpuError) as e:
+        tg.run_gpu_root(keys, tg.Config(memory_limit_bytes=4096))
+    assert e.value.status == 7  # ResourceLimit, refused before any allocation
+    bad = tg.RootKeys(quotient_bits=100, lo=keys.lo, hi=keys.hi)
+    with pytest.raises(tg.TergpuError) as e:
+        tg.run_gpu_root(bad)
+    assert e.value.status == 11  # UnsupportedWidth
+
+
+def test_empty_and_ragged_lists(tg):
+    from tergpu import workload
+
+    Q = 47
+    rng = np.random.default_rng(5)
+    a = rng.integers(0, 1 << Q, 1000, dtype=np.uint64)
+    b = rng.integers(0, 1 << Q, 7, dtype=np.uint64)
+    d = np.array([(int(a[3]) + int(b[5])) % (1 << Q)], dtype=np.uint64)
+    z = np.zeros
+    keys = tg.RootKeys(Q, [a, b, d], [z(1000, np.uint8), z(7, np.uint8), z(1, np.uint8)])
+    res = tg.run_gpu_root(keys)
+    assert [tuple(t) for t in res.triples] == [(3, 5, 0)]
+    empty = tg.RootKeys(Q, [a, b[:0], d], [z(1000, np.uint8), z(0, np.uint8), z(1, np.uint8)])
+    assert len(tg.run_gpu_root(empty).triples) == 0
+
+
+def test_n36_records_root_matches_reference(tg, oracle_mod, golden):
+    """The reference's n=36 capture through the records entry: device key
+    derivation, join and authority, against the reference's root stage and the
+    oracle's projected counts on host-derived keys."""
+    from tergpu import snapshot
+
+    snap = snapshot.load(GOLDEN_DIR / golden["n36_snapshot"]["path"])
+    Q, lo, hi, tau = snapshot.root_keys(snap)
+    row = golden["n36_attempts"][0]["attempts"][0]
+    for k in (12, 16, 20, 24):
+        res = tg.run_gpu_root_records(snap, tg.Config(projected_bits=k))
+        assert res.tau == tau
+        assert res.telemetry.projected_hits == oracle_mod.projected_count(k, lo), k
+        assert res.telemetry.full_hits == row["root_modular"]
+        assert res.valid_roots == row["valid_roots"]
+
+
+def _n72_snapshot(oracle_mod, tmp_path, seed, attempt):
+    from tergpu import snapshot
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference harness not built on this host")
+    path = tmp_path / f"n72_{seed:x}_{attempt}.snap"
+    oracle_mod.ref_run("capture", 72, seed, attempt, "auth", path)
+    return snapshot.load(path)
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_n72_authentic_roots_match_frozen_backends(tg, oracle_mod, golden, tmp_path, case):
+    from tergpu import workload
+
+    g = golden["n72_roots"][case]
+    snap = _n72_snapshot(oracle_mod, tmp_path, g["seed"], g["attempt"])
+    assert snap.entries == g["level1"]
+    res = tg.run_gpu_root_records(snap, tg.Config(projected_bits=32))
+    assert_digest(workload.digest(res.triples), g["k2wide"])
+    assert res.telemetry.logical_pairs == g["k2wide"]["pairs"]
+    assert res.telemetry.projected_hits == g["arwlf_k32_projected_hits"] == g["k2"]["full_q"]
+    assert res.residue_exact == g["k2wide"]["residue"]
+    assert sorted(map(list, res.triples[res.flags & 1 == 1].tolist())) == g["k2wide"]["witnesses"]
+    p25 = tg.run_gpu_root_records(snap, tg.Config(projected_bits=25, count_only=True))
+    assert p25.telemetry.projected_hits == g["k2wide"]["projected_hits_25"]
+    sub = tg.run_gpu_root_records(snap, tg.Config(), cells=oracle_mod.select_cells(512))
+    assert_digest(workload.digest(sub.triples), g["k2wide_subsample512"])
+    if g["attempt"] == 21:
+        # the reference's positive attempt: one residue-exact triple, a valid root
+        assert res.valid_roots == 1 and res.residue_exact == 1
+
+
+def test_n72_adapter_through_reference_sink(tg, oracle_mod, golden, tmp_path):
+    """run_gpu_root as a fifth backend of the reference harness, through the
+    reference's own Dataset / FamilyKeys / RootSink (authority chain on)."""
+    g = golden["n72_roots"][2]
+    _n72_snapshot(oracle_mod, tmp_path, g["seed"], g["attempt"])
+    path = tmp_path / f"n72_{g['seed']:x}_{g['attempt']}.snap"
+    row = oracle_mod.ref_run("snaproot", path, "gpu", 4096, 32)[0]
+    assert row["backend_status"] == "Completed"
+    for k in ("triples", "triple_sum", "triple_xor", "triple_sum2", "residue", "residue_sum",
+              "structural", "witnesses"):
+        assert row[k] == g["k2wide"][k], k
+    assert row["projected_hits"] == g["arwlf_k32_projected_hits"]
+
+
+def test_large_planted_root_is_exact_and_deterministic(tg):
+    """2e10 logical pairs at Q=69: every planted triple is reported, every
+    reported triple satisfies the root equation exactly, two runs and two
+    tunings agree."""
+    from tergpu import workload
+
+    keys = workload.synthetic_root(sizes=(100_000, 200_000, 200_000), quotient_bits=69,
+                                   seed=0xBEEF, planted=64)
+    r1 = tg.run_gpu_root(keys)
+    r2 = tg.run_gpu_root(keys, tg.Config(family_bits=9, filter_bits=17))
+    t1 = sorted(map(tuple, r1.triples.tolist()))
+    assert t1 == sorted(map(tuple, r2.triples.tolist()))
+    n = [len(x) for x in keys.lo]
+    planted = {(n[0] - 1 - i, n[1] - 1 - i, n[2] - 1 - i) for i in range(64)}
+    assert planted <= set(t1)
+    for a, b, c in t1:
+        va = int(keys.lo[0][a]) | (int(keys.hi[0][a]) << 64)
+        vb = int(keys.lo[1][b]) | (int(keys.hi[1][b]) << 64)
+        vd = int(keys.lo[2][c]) | (int(keys.hi[2][c]) << 64)
+        assert (va + vb - vd) % (1 << 69) == 0
+    assert r1.telemetry.logical_pairs == n[0] * n[1]

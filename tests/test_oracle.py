@@ -1,0 +1,80 @@
+"""The oracle restatement pinned against the reference's own outputs (CPU only)."""
+import numpy as np
+import pytest
+
+from conftest import hexint
+
+ANCHOR_SEED = 19797034556212562
+
+
+def test_params_known_answers(oracle_mod, golden):
+    # n=36 from the reference run; n=72 / n=108 from the reference's published
+    # snapshot records (r1 = 25 / 39, r2 = 7 / 12).
+    final = golden["n36_attempts"][0]["final"]
+    assert oracle_mod.params(36) == (final["r1"], final["r2"]) == (12, 3)
+    assert oracle_mod.params(72) == (25, 7)
+    assert oracle_mod.params(108) == (39, 12)
+    for n in (48, 60, 84, 96, 0, 35):
+        assert oracle_mod.params(n) is None
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_n36_attempts_match_reference(oracle_mod, golden, case):
+    g = golden["n36_attempts"][case]
+    for row in g["attempts"]:
+        got = oracle_mod.attempt(36, g["seed"], row["attempt"], kind=g["kind"])
+        for key in ("level2", "level1", "level0", "l3_modular", "l2_modular", "root_prefilter",
+                    "root_quotient_rejects", "root_modular", "valid_roots"):
+            assert got[key] == row[key], (g["kind"], g["seed"], row["attempt"], key)
+        assert got["status"] == (1 if row["status"] == 1 else 0)
+        if got["status"] == 1:
+            assert got["witness_verified"] == 1
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_synthetic_roots_match_reference_brute_force(oracle_mod, golden, case):
+    g = golden["synthetic_roots"][case]
+    lo, hi = oracle_mod.synthetic_root(g["bits"], g["seed"], g["size"], g["pool"])
+    assert [len(a) for a in lo] == g["sizes"]
+    d, trip = oracle_mod.root_join(g["bits"], lo, hi, capacity=4096)
+    for k in ("triples", "triple_sum", "triple_xor", "triple_sum2"):
+        assert d[k] == hexint(g["brute"][k]), k
+    # the same multiset from the explicit triple list
+    assert oracle_mod.digest_of(trip)["triple_sum"] == d["triple_sum"]
+    # ARWLF's projected hits (k = 19 + mid bits) by brute force
+    assert oracle_mod.projected_count(g["arwlf"]["projected_bits"], lo) == g["arwlf"]["projected_hits"]
+    # the reference's declared 700-cell subsample
+    cells = oracle_mod.select_cells(700)
+    assert int(cells.sum()) == 700
+    ds, _ = oracle_mod.root_join(g["bits"], lo, hi, cells=cells)
+    for k in ("triples", "triple_sum", "triple_xor", "triple_sum2"):
+        assert ds[k] == hexint(g["subsample700"][k]), k
+
+
+def test_planted_synthetic_triples_satisfy_equation(oracle_mod):
+    lo, hi = oracle_mod.synthetic_root(69, 0x1234, 200, 0)
+    _, trip = oracle_mod.root_join(69, lo, hi, capacity=1000)
+    for a, b, c in trip:
+        va = int(lo[0][a]) | (int(hi[0][a]) << 64)
+        vb = int(lo[1][b]) | (int(hi[1][b]) << 64)
+        vd = int(lo[2][c]) | (int(hi[2][c]) << 64)
+        assert (va + vb - vd) % (1 << 69) == 0
+
+
+def test_n72_anchor_level_sizes(oracle_mod, golden):
+    g = golden["n72_roots"][0]
+    got = oracle_mod.attempt(72, ANCHOR_SEED, 0)
+    assert got["level1"] == g["level1"] == [19109, 32496, 33505]
+    assert got["level2"] == g["level2"]
+
+
+def test_instance_generators(oracle_mod):
+    values, target, planted = oracle_mod.build_instance(108, 0x1001, "auth")
+    assert planted.sum() == 54 and planted[:27].all() and planted[54:81].all()
+    v, t, p = oracle_mod.build_instance(36, 7, "build")
+    assert p.sum() == 18
+    acc = 0
+    for i in range(36):
+        if p[i]:
+            acc += int(v[i][0])
+    assert acc % (1 << 36) == int(t[0])
