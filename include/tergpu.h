@@ -51,6 +51,9 @@ enum tergpu_status {
 #define TERGPU_ROOT_COUNT_ONLY 1u    /* count triples, write none */
 #define TERGPU_ROOT_DEVICE_INPUTS 2u /* key_lo / key_hi / id / cells are device pointers of
                                         `device`, already resident: nothing is uploaded */
+#define TERGPU_ROOT_SWEEP_V1 4u      /* use the first sweep variant (A in registers, B
+                                        broadcast) instead of the default (B in registers,
+                                        B families sorted, A broadcast); same results */
 
 /*
  * One L1 -> L0 root on full quotient keys.

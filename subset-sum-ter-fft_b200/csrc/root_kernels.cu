@@ -275,14 +275,281 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
   }
 }
 
+
+// Builds the shared filter bitmap and exact-lookup hash of D family u
+// (identical layout for both sweep variants).
+template <bool ALIGNED>
+__device__ __forceinline__ void build_target(const SweepArgs& a, uint32_t yoff, uint32_t ny,
+                                             uint64_t mmask, uint32_t* bm, uint32_t* ywin,
+                                             uint32_t* yhash, bool yshared) {
+  const uint32_t wb = a.wb;
+  for (uint32_t i = threadIdx.x; i < (1u << wb); i += blockDim.x) bm[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < (1u << kYHashBits); i += blockDim.x) yhash[i] = 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
+    const uint32_t w = window_of<ALIGNED>(a.y.res[yoff + i] & mmask, a.mrb);
+    const uint32_t word = (~w) >> (32u - wb);
+    const uint32_t bit = ALIGNED ? ((w >> (27u - wb)) & 31u) : (w & 31u);
+    atomicOr(&bm[word], 1u << bit);
+    if (yshared) {
+      ywin[i] = w;
+      uint32_t h = yhash_of(w);
+      // at most kYCap entries in 2 * kYCap slots: an empty slot always exists
+      while (atomicCAS(&yhash[h], 0u, i + 1u) != 0u) h = (h + 1u) & ((1u << kYHashBits) - 1u);
+    }
+  }
+  __syncthreads();
+}
+
+template <bool ALIGNED, int R>
+__global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) {
+  static_assert(R == 4 || R == 8, "32 tests per mask");
+  constexpr int QPC = 32 / R;  // A entries per 32-test mask
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t item_counter;
+  const uint32_t nfam = 1u << a.fb;
+  const uint32_t fmask = nfam - 1u;
+  const uint32_t wb = a.wb;
+  uint32_t* bm = smem;
+  uint32_t* ywin = bm + (1u << wb);
+  uint32_t* yhash = ywin + kYCap;
+  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
+  uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweepWarps * kQueueCap);
+
+  const uint32_t u = blockIdx.x % nfam;
+  const uint32_t part = blockIdx.x / nfam;
+  const uint32_t s_per = (nfam + a.s_split - 1u) / a.s_split;
+  const uint32_t s0 = part * s_per;
+  const uint32_t s1 = min(nfam, s0 + s_per);
+  const uint32_t ny = a.y.cnt[u];
+  if (s0 >= s1 || ny == 0u) return;  // uniform across the block
+  const uint32_t yoff = a.y.off[u];
+  const uint64_t mmask = a.mrb >= 64 ? ~0ull : ((1ull << a.mrb) - 1ull);
+  const bool yshared = ny <= kYCap;
+  if (threadIdx.x == 0) item_counter = 0u;
+  build_target<ALIGNED>(a, yoff, ny, mmask, bm, ywin, yhash, yshared);
+
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  uint2* wq = queues + warp * kQueueCap;
+  constexpr uint32_t kChunk = 32u * R;
+  uint32_t* xs = xstage + warp * kChunk;  // this warp's B windows, slot r at [r * 32, r * 32 + 32)
+  const uint32_t xc_max = static_cast<uint32_t>((a.counters[kMaxX] + kChunk - 1ull) / kChunk);
+  const uint32_t total_items = (s1 - s0) * xc_max;
+  unsigned long long c_surv = 0, c_fast = 0, c_proj = 0, c_fall = 0;
+  const uint32_t kap_shift = ALIGNED ? (32u - a.mrb) : 0u;
+  const uint32_t rot_shift = ALIGNED ? (27u - wb) : 0u;
+  const uint32_t hi_mask = (1u << a.hi_bits) - 1u;
+  const uint32_t word_mul = 1u << wb;  // word index = umulhi(t, 2^wb) = t >> (32 - wb)
+
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total_items) break;
+    const uint32_t s = s0 + item / xc_max;
+    const uint32_t xc = item % xc_max;
+    const uint32_t t = (u - s) & fmask;
+    const uint32_t kap = s > u ? 1u : 0u;
+    if (a.cells != nullptr && a.cells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
+    const uint32_t nq = a.q.cnt[s];
+    const uint32_t nx = a.x.cnt[t];
+    const uint32_t xbase = xc * kChunk;
+    if (xbase >= nx || nq == 0u) continue;
+    const uint32_t qoff = a.q.off[s];
+    const uint32_t xoff = a.x.off[t];
+
+    uint32_t xw[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const uint32_t xi = xbase + r * 32u + lane;
+      xw[r] = xi < nx ? window_of<ALIGNED>(a.x.res[xoff + xi] & mmask, a.mrb) : 0u;
+      xs[r * 32u + lane] = xw[r];
+    }
+    const uint32_t kapw = kap << kap_shift;
+
+    uint32_t qlen = 0;
+    auto drain = [&]() {
+      __syncwarp();
+      for (uint32_t e = lane; e < qlen; e += 32u) {
+        const uint2 rec = wq[e];
+        const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
+        uint32_t mm = rec.y;
+        while (mm != 0u) {
+          const uint32_t b = __ffs(mm) - 1u;
+          mm &= mm - 1u;
+          const uint32_t k = 31u - b;
+          const uint32_t qi = j + k / R;
+          const uint32_t xi = xbase + (k % R) * 32u + ln;
+          if (qi >= nq || xi >= nx) continue;
+          ++c_surv;
+          // the 32-bit window of the sum from the A residual (L1-resident: the
+          // warp just streamed it) and the staged B window; full residuals are
+          // read only when a D entry carries the same window
+          const uint64_t rq = a.q.res[qoff + qi];
+          const uint32_t w = window_of<ALIGNED>(rq & mmask, a.mrb) + kapw + xs[(k % R) * 32u + ln];
+          auto check = [&](uint32_t idx) {
+            const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
+            const uint64_t ms = sum & mmask;
+            if ((a.y.res[yoff + idx] & mmask) != ms) return;
+            if (a.project) {
+              ++c_proj;
+              return;
+            }
+            ++c_fast;
+            if (a.hi_bits != 0u) {
+              const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                     static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+              if (high != a.y.hi[yoff + idx]) return;
+            }
+            const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+            if (slot < a.cap) {
+              a.triples[3 * slot] = a.q.id[qoff + qi];
+              a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+              a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+            }
+          };
+          if (yshared) {
+            uint32_t h = yhash_of(w);
+            for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+              if (ywin[v - 1u] == w) check(v - 1u);
+              h = (h + 1u) & ((1u << kYHashBits) - 1u);
+            }
+          } else {
+            ++c_fall;
+            for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
+          }
+        }
+      }
+      __syncwarp();
+      qlen = 0;
+    };
+
+    const uint64_t* qr = a.q.res + qoff;
+    for (uint32_t j = 0; j < nq; j += QPC) {
+      uint32_t m = 0;
+#pragma unroll
+      for (int p = 0; p < QPC / 2; ++p) {
+        // uniform address: one broadcast load of two A residuals (families start
+        // on even entries; the array carries slack past its end)
+        const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qr + j + 2 * p);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const uint32_t nqw = ~(window_of<ALIGNED>((e ? qq.y : qq.x) & mmask, a.mrb) + kapw);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const uint32_t tt = nqw - xw[r];
+            const uint32_t w = bm[__umulhi(tt, word_mul)];
+            m = __funnelshift_l(__funnelshift_l(w, w, tt >> rot_shift), m, 1);
+          }
+        }
+      }
+      if (__any_sync(kFull, m != 0u)) {
+        // one record per lane: test k = (2p + e) * R + r sits at bit 31 - k
+        const bool has = m != 0u;
+        const uint32_t ball = __ballot_sync(kFull, has);
+        if (qlen + __popc(ball) > kQueueCap) drain();
+        if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
+        qlen += __popc(ball);
+      }
+    }
+    drain();
+  }
+
+  for (int d = 16; d > 0; d >>= 1) {
+    c_surv += __shfl_down_sync(kFull, c_surv, d);
+    c_fast += __shfl_down_sync(kFull, c_fast, d);
+    c_proj += __shfl_down_sync(kFull, c_proj, d);
+    c_fall += __shfl_down_sync(kFull, c_fall, d);
+  }
+  if (lane == 0) {
+    if (c_surv) atomicAdd(&a.counters[kSurvivors], c_surv);
+    if (c_fast) atomicAdd(&a.counters[kFast], c_fast);
+    if (c_proj) atomicAdd(&a.counters[kProjected], c_proj);
+    if (c_fall) atomicAdd(&a.counters[kFallback], c_fall);
+  }
+}
+
+// Exclusive scan of n counters in shared memory by one CTA of 256 threads.
+__device__ void block_exclusive_scan256(uint32_t* a, uint32_t n) {
+  __shared__ uint32_t warp_sums[8];
+  const uint32_t per = (n + 255u) / 256u;
+  const uint32_t begin = threadIdx.x * per;
+  const uint32_t end = min(n, begin + per);
+  uint32_t local = 0;
+  for (uint32_t i = begin; i < end; ++i) local += a[i];
+  uint32_t v = local;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  if (lane == 31u) warp_sums[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < 8u ? warp_sums[lane] : 0u;
+    for (int d = 1; d < 8; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, w, d);
+      if (lane >= (uint32_t)d) w += o;
+    }
+    if (lane < 8u) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = v - local + (warp > 0 ? warp_sums[warp - 1] : 0u);
+  for (uint32_t i = begin; i < end; ++i) {
+    const uint32_t c = a[i];
+    a[i] = run;
+    run += c;
+  }
+  __syncthreads();
+}
+
+template <bool ALIGNED>
+__global__ void __launch_bounds__(256) k_family_sort(uint64_t* __restrict__ res,
+                                                     uint8_t* __restrict__ hi,
+                                                     uint32_t* __restrict__ id,
+                                                     const uint32_t* __restrict__ off,
+                                                     const uint32_t* __restrict__ cnt,
+                                                     uint32_t mrb, uint32_t sb) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint64_t* keys = reinterpret_cast<uint64_t*>(smem);
+  uint32_t* ids = reinterpret_cast<uint32_t*>(keys + kSortCap);
+  uint32_t* hist = ids + kSortCap;
+  uint8_t* his = reinterpret_cast<uint8_t*>(hist + (1u << sb));
+  const uint32_t f = blockIdx.x;
+  const uint32_t n = cnt[f];
+  if (n < 2u || n > kSortCap) return;  // uniform across the block
+  const uint32_t base = off[f];
+  const uint64_t mmask = mrb >= 64 ? ~0ull : ((1ull << mrb) - 1ull);
+  for (uint32_t i = threadIdx.x; i < (1u << sb); i += blockDim.x) hist[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    keys[i] = res[base + i];
+    ids[i] = id[base + i];
+    his[i] = hi[base + i];
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    atomicAdd(&hist[window_of<ALIGNED>(keys[i] & mmask, mrb) >> (32u - sb)], 1u);
+  }
+  __syncthreads();
+  block_exclusive_scan256(hist, 1u << sb);
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t b = window_of<ALIGNED>(keys[i] & mmask, mrb) >> (32u - sb);
+    const uint32_t pos = atomicAdd(&hist[b], 1u);
+    res[base + pos] = keys[i];
+    id[base + pos] = ids[i];
+    hi[base + pos] = his[i];
+  }
+}
+
 __global__ void k_max_family(const uint32_t* __restrict__ cnt, uint32_t nfam,
-                             unsigned long long* __restrict__ counters) {
+                             unsigned long long* __restrict__ counters, int slot) {
   uint32_t m = 0;
   for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < nfam; f += gridDim.x * blockDim.x) {
     m = max(m, cnt[f]);
   }
   for (int d = 16; d > 0; d >>= 1) m = max(m, __shfl_down_sync(kFull, m, d));
-  if ((threadIdx.x & 31u) == 0u && m != 0u) atomicMax(&counters[kMaxQ], (unsigned long long)m);
+  if ((threadIdx.x & 31u) == 0u && m != 0u) atomicMax(&counters[slot], (unsigned long long)m);
 }
 
 __global__ void k_record_keys(const RecordKeyArgs a) {
@@ -384,9 +651,9 @@ void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_
                                              res, hi, out_id);
 }
 
-void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters,
+void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters, int slot,
                        cudaStream_t st) {
-  k_max_family<<<(nfam + 255) / 256, 256, 0, st>>>(cnt, nfam, counters);
+  k_max_family<<<(nfam + 255) / 256, 256, 0, st>>>(cnt, nfam, counters, slot);
 }
 
 size_t sweep_smem_bytes(uint32_t wb) {
@@ -403,6 +670,31 @@ void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st) {
   } else {
     cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_sweep<false><<<grid, kSweepThreads, smem, st>>>(a);
+  }
+}
+
+void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
+  const size_t smem = sweep_smem_bytes(a.wb) + static_cast<size_t>(kSweepWarps) * 32 * 8 * 4;
+  const unsigned grid = (1u << a.fb) * a.s_split;
+  if (aligned) {
+    cudaFuncSetAttribute(k_sweep2<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sweep2<true, 8><<<grid, kSweepThreads, smem, st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_sweep2<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sweep2<false, 8><<<grid, kSweepThreads, smem, st>>>(a);
+  }
+}
+
+void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
+                        const uint32_t* cnt, uint32_t nfam, uint32_t mrb, uint32_t sb,
+                        cudaStream_t st) {
+  const size_t smem = static_cast<size_t>(kSortCap) * (8 + 4 + 1) + (static_cast<size_t>(4) << sb) + 16;
+  if (mrb < 32) {
+    cudaFuncSetAttribute(k_family_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_family_sort<true><<<nfam, 256, smem, st>>>(res, hi, id, off, cnt, mrb, sb);
+  } else {
+    cudaFuncSetAttribute(k_family_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_family_sort<false><<<nfam, 256, smem, st>>>(res, hi, id, off, cnt, mrb, sb);
   }
 }
 

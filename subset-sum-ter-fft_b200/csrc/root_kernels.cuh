@@ -23,6 +23,7 @@ constexpr int kSweepWarps = kSweepThreads / 32;
 constexpr int kQueueCap = 128;         // survivor slots per warp
 constexpr uint32_t kYHashBits = 12;    // shared exact-lookup table: 4096 slots
 constexpr uint32_t kYCap = 2048;       // D-family entries the shared table takes
+constexpr uint32_t kSortCap = 4096;    // B-family entries the in-family sort takes
 
 struct ListView {
   const uint64_t* res;
@@ -50,7 +51,8 @@ struct SweepArgs {
 // counters[kMaxQ] holds the largest A family (set by launch_max_family before
 // the sweep reads it), so no host round trip separates partition and sweep.
 enum Counter {
-  kTriples = 0, kSurvivors = 1, kFast = 2, kProjected = 3, kFallback = 4, kMaxQ = 5, kCounters = 8
+  kTriples = 0, kSurvivors = 1, kFast = 2, kProjected = 3, kFallback = 4, kMaxQ = 5, kMaxX = 6,
+  kCounters = 8
 };
 
 // Host-callable launchers (root_kernels.cu).
@@ -60,10 +62,20 @@ void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cu
 void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, uint64_t n,
                     uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
                     uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st);
-void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters,
+void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters, int slot,
                        cudaStream_t st);
 size_t sweep_smem_bytes(uint32_t wb);
+// v1: A windows in registers, B broadcast (any family order).
 void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st);
+// v2: B windows in registers (32 consecutive entries per lane slot), A broadcast.
+// Exact for any family order; conflict-free filter probes once every B family
+// is sorted by the filter's word bits (launch_family_sort).
+void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st);
+// Sorts every family of one partitioned list (of at most kSortCap entries) by
+// the top `sb` bits of its sweep window, in place; larger families stay as they are.
+void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
+                        const uint32_t* cnt, uint32_t nfam, uint32_t mrb, uint32_t sb,
+                        cudaStream_t st);
 
 // Keys from captured L1 records: q = ((R - c) mod 2^n) >> r1 over Q bits,
 // list 2 turned into d = tau - q_C.

@@ -100,30 +100,40 @@ uint32_t ceil_log2(uint64_t v) {
 }
 
 struct Tuning {
-  uint32_t fb = 6, wb = 12, s_split = 1;
+  uint32_t fb = 6, wb = 12, s_split = 1, sort_bits = 0;
+  bool v2 = true;
 };
 
-// Family radix: about 1024 D entries per family; the filter: about 256 bits
-// per D entry of the largest-average family (false-pass rate near 1/256).
-Tuning choose_tuning(uint64_t n_d, uint32_t fast_bits, uint32_t projected, uint32_t fb_req,
-                     uint32_t filter_req) {
+// v1: about 1024 D entries per family and about 256 filter bits per D entry.
+// v2: about 2048 D entries per family; the filter has about 4x as many words as
+// a B family has entries, so a warp's 32 probes (32 consecutive sorted B
+// entries) span ~128 consecutive words: a few-way bank conflict at most, while
+// the false-pass rate stays near |D_u| / 2^(wb+5) ~ 0.6 %.
+Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
+                     uint32_t fb_req, uint32_t filter_req, bool v2) {
   Tuning t;
+  t.v2 = v2;
   uint32_t fb_max = std::min<uint32_t>(14, fast_bits - 2);
   if (projected != 0) fb_max = std::min<uint32_t>(fb_max, projected - 6);
   if (fb_req != 0) {
     t.fb = fb_req;
   } else {
-    const double ideal = std::log2(std::max<double>(1.0, static_cast<double>(n_d) / 1024.0));
+    const double per = v2 ? 2048.0 : 1024.0;
+    const double ideal = std::log2(std::max<double>(1.0, static_cast<double>(n_d) / per));
     t.fb = static_cast<uint32_t>(std::max(6.0, std::floor(ideal + 0.5)));
     t.fb = std::min(t.fb, fb_max);
     t.fb = std::max<uint32_t>(t.fb, 6);
   }
-  const uint64_t avg = std::max<uint64_t>(1, n_d >> t.fb);
+  const uint64_t avg_d = std::max<uint64_t>(1, n_d >> t.fb);
+  const uint64_t avg_x = std::max<uint64_t>(1, n_x >> t.fb);
   if (filter_req != 0) {
     t.wb = filter_req - 5;
+  } else if (v2) {
+    t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 2, 6, 14);
   } else {
-    t.wb = std::clamp<uint32_t>(ceil_log2(avg * 256) - 5, 10, 14);
+    t.wb = std::clamp<uint32_t>(ceil_log2(avg_d * 256) - 5, 10, 14);
   }
+  t.sort_bits = std::min<uint32_t>(t.wb, 12);
   const uint32_t nfam = 1u << t.fb;
   const uint32_t target_ctas = 148 * 2 * 8;
   t.s_split = std::clamp<uint32_t>((target_ctas + nfam - 1) / nfam, 1, nfam);
@@ -144,6 +154,7 @@ struct JoinInput {
   uint64_t memory_limit_bytes;
   uint64_t capacity;
   bool count_only;
+  bool sweep_v1;
   cudaStream_t stream;
 };
 
@@ -173,7 +184,8 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   const uint32_t Q = in.quotient_bits;
   const uint32_t F = std::min<uint32_t>(Q, 64);
   const uint32_t hi_bits = Q - F;
-  r.tuning = choose_tuning(in.count[2], F, in.projected_bits, in.family_bits, in.filter_bits);
+  r.tuning = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, in.family_bits,
+                           in.filter_bits, !in.sweep_v1);
   const Tuning& tu = r.tuning;
   if (tu.fb < 6 || tu.fb > 16 || tu.fb + 2 > F || tu.wb < 5 || tu.wb > 15 ||
       (in.projected_bits != 0 && (in.projected_bits > F || in.projected_bits < tu.fb + 1))) {
@@ -224,8 +236,14 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     views[l] = ListView{res[l], hi[l], ids[l], off[l], cnt[l]};
     r.launches += (in.count[l] != 0 ? 2 : 0) + 1;
   }
-  launch_max_family(cnt[0], nfam, counters, st);
-  r.launches += 1;
+  launch_max_family(cnt[0], nfam, counters, kMaxQ, st);
+  launch_max_family(cnt[1], nfam, counters, kMaxX, st);
+  r.launches += 2;
+  if (tu.v2 && in.count[1] != 0) {
+    // B families sorted by the top filter-word bits of the full-width window
+    launch_family_sort(res[1], hi[1], ids[1], off[1], cnt[1], nfam, F - tu.fb, tu.sort_bits, st);
+    r.launches += 1;
+  }
   check(cudaGetLastError(), "partition launch");
   check(cudaEventRecord(w.mid, st), "event");
   SweepArgs a{};
@@ -244,13 +262,21 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   if (!in.count_only || in.projected_bits == 0) {
     a.project = 0;
     a.mrb = F - tu.fb;
-    launch_sweep(a, a.mrb < 32, st);
+    if (tu.v2) {
+      launch_sweep2(a, a.mrb < 32, st);
+    } else {
+      launch_sweep(a, a.mrb < 32, st);
+    }
     r.launches += 1;
   }
   if (in.projected_bits != 0) {
     a.project = 1;
     a.mrb = in.projected_bits - tu.fb;
-    launch_sweep(a, a.mrb < 32, st);
+    if (tu.v2) {
+      launch_sweep2(a, a.mrb < 32, st);
+    } else {
+      launch_sweep(a, a.mrb < 32, st);
+    }
     r.launches += 1;
   }
   check(cudaGetLastError(), "sweep launch");
@@ -403,6 +429,7 @@ int root_run_body(const void* vin, void* vout) {
   j.memory_limit_bytes = in->memory_limit_bytes;
   j.capacity = count_only ? 0 : out->capacity;
   j.count_only = count_only;
+  j.sweep_v1 = (in->flags & TERGPU_ROOT_SWEEP_V1) != 0;
   const JoinResult res = run_join(w, j, input_bytes);
   fill_out(res, out);
   int status = TERGPU_COMPLETED;
@@ -530,6 +557,7 @@ int root_records_body(const void* vin, void* vout) {
   j.memory_limit_bytes = in->memory_limit_bytes;
   j.capacity = count_only ? 0 : out->root.capacity;
   j.count_only = count_only;
+  j.sweep_v1 = (in->flags & TERGPU_ROOT_SWEEP_V1) != 0;
   const JoinResult res = run_join(w, j, input_bytes);
   fill_out(res, &out->root);
   out->residue_exact = out->structural = out->valid_roots = 0;

@@ -37,6 +37,7 @@ STATUS_NAMES = {
 
 ROOT_COUNT_ONLY = 1
 ROOT_DEVICE_INPUTS = 2
+ROOT_SWEEP_V1 = 4
 MAX_QUOTIENT_BITS = 72
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)

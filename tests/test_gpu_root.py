@@ -33,36 +33,39 @@ def assert_digest(got, expected):
         assert got[k] == hexint(expected[k]), (k, got[k], expected[k])
 
 
+@pytest.mark.parametrize("v1", [False, True])
 @pytest.mark.parametrize("case", range(6))
-def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case):
+def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case, v1):
     from tergpu import workload
 
     g = golden["synthetic_roots"][case]
     lo, hi, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
-    res = tg.run_gpu_root(keys, tg.Config(projected_bits=g["arwlf"]["projected_bits"]))
+    res = tg.run_gpu_root(keys, tg.Config(projected_bits=g["arwlf"]["projected_bits"], sweep_v1=v1))
     assert_digest(workload.digest(res.triples), g["brute"])
     assert res.telemetry.logical_pairs == g["arwlf"]["logical_pairs"]
     assert res.telemetry.projected_hits == g["arwlf"]["projected_hits"]
     assert res.telemetry.full_hits == g["brute"]["triples"]
     # the reference's declared 700-cell subsample
-    sub = tg.run_gpu_root(keys, tg.Config(), cells=oracle_mod.select_cells(700))
+    sub = tg.run_gpu_root(keys, tg.Config(sweep_v1=v1), cells=oracle_mod.select_cells(700))
     assert_digest(workload.digest(sub.triples), g["subsample700"])
     assert sub.telemetry.logical_pairs == g["subsample700"]["logical_pairs"]
 
 
+@pytest.mark.parametrize("v1", [False, True])
 @pytest.mark.parametrize("fb,filt", [(6, 10), (6, 19), (7, 12), (8, 15), (9, 20), (10, 11)])
-def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt):
+def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt, v1):
     from tergpu import workload
 
     g = golden["synthetic_roots"][0]
     _, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
-    res = tg.run_gpu_root(keys, tg.Config(family_bits=fb, filter_bits=filt))
+    res = tg.run_gpu_root(keys, tg.Config(family_bits=fb, filter_bits=filt, sweep_v1=v1))
     assert res.telemetry.family_bits == fb and res.telemetry.filter_bits == filt
     assert_digest(workload.digest(res.triples), g["brute"])
 
 
+@pytest.mark.parametrize("v1", [False, True])
 @pytest.mark.parametrize("bits", [24, 33, 40, 47, 58, 64, 65, 69, 72])
-def test_widths_against_oracle(tg, oracle_mod, bits):
+def test_widths_against_oracle(tg, oracle_mod, bits, v1):
     """Every key width from the n=36 root (24) to the one-byte high limit (72),
     with the carry, multiplicity and high-bit plants; projected counts at two k."""
     from tergpu import workload
@@ -70,7 +73,7 @@ def test_widths_against_oracle(tg, oracle_mod, bits):
     lo, hi, keys = keys_of(oracle_mod, bits, 0xABC0 + bits, 3000, 0)
     expected, _ = oracle_mod.root_join(bits, lo, hi)
     k = min(bits, 64) - 3
-    res = tg.run_gpu_root(keys, tg.Config(projected_bits=k))
+    res = tg.run_gpu_root(keys, tg.Config(projected_bits=k, sweep_v1=v1))
     got = workload.digest(res.triples)
     for key in DIGEST_KEYS:
         assert got[key] == expected[key], key
@@ -198,7 +201,7 @@ def test_large_planted_root_is_exact_and_deterministic(tg):
     keys = workload.synthetic_root(sizes=(100_000, 200_000, 200_000), quotient_bits=69,
                                    seed=0xBEEF, planted=64)
     r1 = tg.run_gpu_root(keys)
-    r2 = tg.run_gpu_root(keys, tg.Config(family_bits=9, filter_bits=17))
+    r2 = tg.run_gpu_root(keys, tg.Config(family_bits=9, filter_bits=17, sweep_v1=True))
     t1 = sorted(map(tuple, r1.triples.tolist()))
     assert t1 == sorted(map(tuple, r2.triples.tolist()))
     n = [len(x) for x in keys.lo]
