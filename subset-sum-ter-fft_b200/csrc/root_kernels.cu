@@ -90,6 +90,34 @@ __global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __
   }
 }
 
+// Builds the shared filter bitmap and exact-lookup hash of D family u
+// (identical layout for both sweep variants).
+template <bool ALIGNED>
+__device__ __forceinline__ void build_target(const SweepArgs& a, uint32_t yoff, uint32_t ny,
+                                             uint64_t mmask, uint32_t* bm, uint32_t* ywin,
+                                             uint16_t* yhash, bool yshared) {
+  const uint32_t wb = a.wb;
+  for (uint32_t i = threadIdx.x; i < (1u << wb); i += blockDim.x) bm[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < (1u << kYHashBits); i += blockDim.x) yhash[i] = 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
+    const uint32_t w = window_of<ALIGNED>(a.y.res[yoff + i] & mmask, a.mrb);
+    const uint32_t word = (~w) >> (32u - wb);
+    const uint32_t bit = ALIGNED ? ((w >> (27u - wb)) & 31u) : (w & 31u);
+    atomicOr(&bm[word], 1u << bit);
+    if (yshared) {
+      ywin[i] = w;
+      uint32_t h = yhash_of(w);
+      // at most kYCap entries in 2 * kYCap slots: an empty slot always exists
+      while (atomicCAS(reinterpret_cast<unsigned short*>(&yhash[h]), (unsigned short)0,
+                       static_cast<unsigned short>(i + 1u)) != 0) {
+        h = (h + 1u) & ((1u << kYHashBits) - 1u);
+      }
+    }
+  }
+  __syncthreads();
+}
+
 template <bool ALIGNED>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -99,7 +127,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
   const uint32_t wb = a.wb;
   uint32_t* bm = smem;
   uint32_t* ywin = bm + (1u << wb);
-  uint32_t* yhash = ywin + kYCap;
+  uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kYCap);
   uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
 
   const uint32_t u = blockIdx.x % nfam;
@@ -113,24 +141,9 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
   const uint64_t mmask = a.mrb >= 64 ? ~0ull : ((1ull << a.mrb) - 1ull);
   const uint32_t tid = threadIdx.x;
 
-  for (uint32_t i = tid; i < (1u << wb); i += kSweepThreads) bm[i] = 0u;
-  for (uint32_t i = tid; i < (1u << kYHashBits); i += kSweepThreads) yhash[i] = 0u;
   if (tid == 0) item_counter = 0u;
-  __syncthreads();
   const bool yshared = ny <= kYCap;
-  for (uint32_t i = tid; i < ny; i += kSweepThreads) {
-    const uint32_t w = window_of<ALIGNED>(a.y.res[yoff + i] & mmask, a.mrb);
-    const uint32_t word = (~w) >> (32u - wb);
-    const uint32_t bit = ALIGNED ? ((w >> (27u - wb)) & 31u) : (w & 31u);
-    atomicOr(&bm[word], 1u << bit);
-    if (yshared) {
-      ywin[i] = w;
-      uint32_t h = yhash_of(w);
-      // at most kYCap entries in 2 * kYCap slots: an empty slot always exists
-      while (atomicCAS(&yhash[h], 0u, i + 1u) != 0u) h = (h + 1u) & ((1u << kYHashBits) - 1u);
-    }
-  }
-  __syncthreads();
+  build_target<ALIGNED>(a, yoff, ny, mmask, bm, ywin, yhash, yshared);
 
   const uint32_t warp = tid >> 5, lane = tid & 31u;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
@@ -276,31 +289,6 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
 }
 
 
-// Builds the shared filter bitmap and exact-lookup hash of D family u
-// (identical layout for both sweep variants).
-template <bool ALIGNED>
-__device__ __forceinline__ void build_target(const SweepArgs& a, uint32_t yoff, uint32_t ny,
-                                             uint64_t mmask, uint32_t* bm, uint32_t* ywin,
-                                             uint32_t* yhash, bool yshared) {
-  const uint32_t wb = a.wb;
-  for (uint32_t i = threadIdx.x; i < (1u << wb); i += blockDim.x) bm[i] = 0u;
-  for (uint32_t i = threadIdx.x; i < (1u << kYHashBits); i += blockDim.x) yhash[i] = 0u;
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
-    const uint32_t w = window_of<ALIGNED>(a.y.res[yoff + i] & mmask, a.mrb);
-    const uint32_t word = (~w) >> (32u - wb);
-    const uint32_t bit = ALIGNED ? ((w >> (27u - wb)) & 31u) : (w & 31u);
-    atomicOr(&bm[word], 1u << bit);
-    if (yshared) {
-      ywin[i] = w;
-      uint32_t h = yhash_of(w);
-      // at most kYCap entries in 2 * kYCap slots: an empty slot always exists
-      while (atomicCAS(&yhash[h], 0u, i + 1u) != 0u) h = (h + 1u) & ((1u << kYHashBits) - 1u);
-    }
-  }
-  __syncthreads();
-}
-
 template <bool ALIGNED, int R>
 __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) {
   static_assert(R == 4 || R == 8, "32 tests per mask");
@@ -312,7 +300,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
   const uint32_t wb = a.wb;
   uint32_t* bm = smem;
   uint32_t* ywin = bm + (1u << wb);
-  uint32_t* yhash = ywin + kYCap;
+  uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kYCap);
   uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
   uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweepWarps * kQueueCap);
 
@@ -657,8 +645,8 @@ void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* c
 }
 
 size_t sweep_smem_bytes(uint32_t wb) {
-  return (static_cast<size_t>(1) << wb) * 4 + kYCap * 4 + (static_cast<size_t>(1) << kYHashBits) * 4 +
-         static_cast<size_t>(kSweepWarps) * kQueueCap * sizeof(uint2);
+  return (static_cast<size_t>(1) << wb) * 4 + kYCap * 4 + (static_cast<size_t>(1) << kYHashBits) * 2 +
+         static_cast<size_t>(kSweepWarps) * kQueueCap * sizeof(uint2);  // yhash: 2 bytes a slot
 }
 
 void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st) {

@@ -21,8 +21,8 @@ namespace tergpu {
 constexpr int kSweepThreads = 256;
 constexpr int kSweepWarps = kSweepThreads / 32;
 constexpr int kQueueCap = 128;         // survivor slots per warp
-constexpr uint32_t kYHashBits = 12;    // shared exact-lookup table: 4096 slots
-constexpr uint32_t kYCap = 2048;       // D-family entries the shared table takes
+constexpr uint32_t kYHashBits = 13;    // shared exact-lookup table: 8192 slots of 16 bits
+constexpr uint32_t kYCap = 4096;       // D-family entries the shared table takes
 constexpr uint32_t kSortCap = 4096;    // B-family entries the in-family sort takes
 
 struct ListView {
