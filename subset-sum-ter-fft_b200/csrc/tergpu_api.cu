@@ -105,10 +105,10 @@ struct Tuning {
 };
 
 // v1: about 1024 D entries per family and about 256 filter bits per D entry.
-// v2: about 2048 D entries per family; the filter has about 4x as many words as
-// a B family has entries, so a warp's 32 probes (32 consecutive sorted B
-// entries) span ~128 consecutive words: a few-way bank conflict at most, while
-// the false-pass rate stays near |D_u| / 2^(wb+5) ~ 0.6 %.
+// v2: about 2048 D entries per family; the filter has about 8x as many words as
+// a B family has entries (measured best at n=108: 19 filter bits, false-pass
+// rate |D_u| / 2^(wb+5) ~ 0.3 %); narrower filters make the probes of 32
+// consecutive sorted B entries nearly conflict-free but pass too many pairs.
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
                      uint32_t fb_req, uint32_t filter_req, bool v2) {
   Tuning t;
@@ -129,7 +129,7 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   if (filter_req != 0) {
     t.wb = filter_req - 5;
   } else if (v2) {
-    t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 2, 6, 14);
+    t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 3, 6, 14);
   } else {
     t.wb = std::clamp<uint32_t>(ceil_log2(avg_d * 256) - 5, 10, 14);
   }
