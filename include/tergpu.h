@@ -165,6 +165,33 @@ typedef struct {
  * (ter2_root/campaign/ter_arwlf_solve.cpp:41-178). */
 int tergpu_root_run_records(const tergpu_root_records_in *in, tergpu_root_records_out *out);
 
+/*
+ * The root join for callers that cannot allocate device memory.  This entry
+ * has no counterpart in the reference: it exists for callers such as a host
+ * framework that owns every device allocation through its own pool, a process
+ * whose device memory is reserved up front, or a service loop that must not
+ * risk an allocation's synchronization or failure.
+ *
+ * The caller passes device-resident inputs (flags must include
+ * TERGPU_ROOT_DEVICE_INPUTS; key_lo / key_hi / id / cells are device pointers)
+ * and a DEVICE buffer out->triples of out->capacity triples.  All
+ * intermediates live in one fixed 32 MiB device array inside the library
+ * (held by every GPU that loads the library until the process exits); a root
+ * whose intermediates do not fit (about 2.4 million key entries over the three
+ * lists) is refused with TERGPU_RESOURCE_LIMIT.  Projected counts are not
+ * offered here; family bits are limited to 6..10.
+ *
+ * The first call on a device looks up the array's device address (a lookup,
+ * not an allocation); make that first call before any stream capture.  Every
+ * call reuses the same array, so calls whose work overlaps on the GPU race:
+ * issue them one after another.  join_ms / partition_ms / sweep_ms are not
+ * measured (no events are created) and read 0.
+ */
+int tergpu_root_run_noalloc(const tergpu_root_in *in, tergpu_root_out *out);
+
+/* Error text of the calling thread's last tergpu_root_run_noalloc call. */
+const char *tergpu_noalloc_last_error(void);
+
 /* FNV-1a-64 over size bytes starting from state (0xcbf29ce484222325 for a fresh
  * hash): the list and header checksums of the .snap format
  * (reference ter2_root/frozen/ter_root_snapshot.cpp:94-101).  Host code only. */

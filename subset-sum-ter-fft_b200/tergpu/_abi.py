@@ -89,7 +89,8 @@ class RootRecordsOut(ctypes.Structure):
 
 EXPORTED = (
     "tergpu_root_run", "tergpu_root_run_records", "tergpu_device_count", "tergpu_abi_version",
-    "tergpu_release", "tergpu_last_error", "tergpu_fnv1a",
+    "tergpu_release", "tergpu_last_error", "tergpu_fnv1a", "tergpu_root_run_noalloc",
+    "tergpu_noalloc_last_error",
 )
 
 _lib = None
@@ -113,6 +114,9 @@ def load(path: os.PathLike | str | None = None):
     lib.tergpu_abi_version.restype = ctypes.c_int
     lib.tergpu_last_error.restype = ctypes.c_char_p
     lib.tergpu_release.restype = None
+    lib.tergpu_root_run_noalloc.argtypes = [ctypes.POINTER(RootIn), ctypes.POINTER(RootOut)]
+    lib.tergpu_root_run_noalloc.restype = ctypes.c_int
+    lib.tergpu_noalloc_last_error.restype = ctypes.c_char_p
     if path is None:
         _lib = lib
     return lib
