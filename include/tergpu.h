@@ -166,6 +166,79 @@ typedef struct {
 int tergpu_root_run_records(const tergpu_root_records_in *in, tergpu_root_records_out *out);
 
 /*
+ * Exact depth-3 TER attempts on the device: the attempt loop of solve_full_ter
+ * (reference src/full_ter.cpp:2933-3521, FiniteSanity shape, Random targets).
+ *
+ * Per attempt a in [attempt_first, attempt_first + attempt_count): targets from
+ * SplitMix64(seed + a) (src/full_ter.cpp:2364-2386), nine L3 -> L2 binary merges
+ * (src/full_ter.cpp:827-933), three L2 -> L1 ternary merges on the projected
+ * quotient (src/full_ter.cpp:1138-1356), each level in the reference's canonical
+ * order (sorted by packed digit words, duplicates dropped), then the root with
+ * the device authority (as tergpu_root_run_records).  A valid root stops the
+ * loop: the lowest parent in canonical order is verified on the host (binary,
+ * weight n/2, sum of the chosen weights == target mod 2^n,
+ * src/full_ter.cpp:2879-2908) and returned as the witness.
+ *
+ * Statuses: TERGPU_FOUND, TERGPU_ATTEMPT_LIMIT_REACHED (budget spent, never UNSAT),
+ * TERGPU_CANCELLED (*cancel != 0 before an attempt or stage),
+ * TERGPU_RESOURCE_LIMIT (the predicted device bytes exceed memory_limit_bytes,
+ * refused before any allocation), TERGPU_INVALID_CONFIGURATION (36 does not
+ * divide n, or n > 108), TERGPU_INVARIANT_VIOLATION (a witness that fails
+ * verification).
+ */
+typedef struct {
+  uint32_t attempt;
+  int32_t status;              /* TERGPU_FOUND or TERGPU_NO_WITNESS_THIS_ATTEMPT */
+  uint64_t level2_sizes[9];
+  uint64_t level1_sizes[3];
+  uint64_t level0_size;        /* distinct valid parents */
+  uint64_t l3_modular;         /* L3 -> L2 pairs meeting the congruence */
+  uint64_t l2_modular;         /* L2 -> L1 triples meeting the quotient congruence */
+  uint64_t root_modular;       /* full-Q root triples (residue-exact) */
+  uint64_t valid_roots;        /* ... with a binary weight-n/2 parent (pre-dedup) */
+  uint64_t root_pairs;         /* |L1_0| * |L1_1| */
+  double l2_ms, l1_ms, root_ms, total_ms;
+} tergpu_attempt_stats;
+
+/* tergpu_attempt_in.flags */
+#define TERGPU_ATTEMPT_CAPTURE_ONLY 1u /* stop after L1 (export only): the device
+                                          counterpart of stream_full_ter_root_lists */
+
+typedef struct {
+  uint32_t n;                  /* 36, 72 or 108 */
+  uint32_t flags;
+  const uint64_t *values_le;   /* n * ceil(n/64) words: the weights */
+  const uint64_t *target_le;   /* ceil(n/64) words */
+  uint64_t seed;               /* attempt a draws its targets from seed + a */
+  uint32_t attempt_first;
+  uint32_t attempt_count;
+  uint64_t memory_limit_bytes; /* 0: no ceiling */
+  const volatile int32_t *cancel; /* host flag, polled between stages; may be NULL */
+  int32_t device;
+} tergpu_attempt_in;
+
+typedef struct {
+  int32_t status;
+  uint32_t r1, r2;
+  uint64_t level3_size;        /* entries per half */
+  uint32_t attempts_run;
+  uint32_t found_attempt;
+  uint8_t witness[128];        /* digits 0/1 of the verified witness when FOUND */
+  tergpu_attempt_stats *stats; /* attempt_count entries (may be NULL) */
+  uint8_t *l1_records[3];      /* optional: L1 lists of the last attempt run, as
+                                  .snap records (capacity l1_capacity[l] records) */
+  uint64_t l1_capacity[3];
+  uint32_t child_targets[3][4];/* the last attempt's L1 targets (words32) */
+  uint32_t root_target[4];
+  uint64_t device_bytes;
+  double total_ms;
+} tergpu_attempt_out;
+
+/* Replaces: solve_full_ter's attempt loop (src/full_ter.cpp:3125-3515) and
+ * stream_full_ter_root_lists (src/full_ter.cpp:3926-4195) for the L1 export. */
+int tergpu_attempt_run(const tergpu_attempt_in *in, tergpu_attempt_out *out);
+
+/*
  * The root join for callers that cannot allocate device memory.  This entry
  * has no counterpart in the reference: it exists for callers such as a host
  * framework that owns every device allocation through its own pool, a process

@@ -1,0 +1,495 @@
+// tergpu_attempt_run: exact depth-3 TER attempts on the device (include/tergpu.h).
+//
+// Host side of the attempt loop: FiniteSanity parameters, per-attempt targets,
+// the stage sequence and its memory preflight, witness selection and
+// verification.  Device work: attempt_kernels.cu (levels 3..1) and the root
+// join of root_kernels.cu / tergpu_api.cu.
+
+#include "attempt_kernels.cuh"
+#include "root_kernels.cuh"
+#include "tergpu.h"
+#include "tergpu_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace tergpu {
+namespace {
+
+typedef unsigned __int128 u128;
+
+u128 mask128(uint32_t bits) { return bits >= 128 ? ~(u128)0 : ((((u128)1) << bits) - 1); }
+
+// ---- FiniteSanity parameters: r = floor(log2 R) / 2 with
+// R1 = (n/2)! / ((n/6)!)^3 and R2 = (n/6)! / ((n/18)!)^3 (every epsilon zero;
+// reference src/full_ter.cpp:2699-2759).  Exact small bignum arithmetic.
+uint32_t floor_log2_multinomial3(uint32_t total, uint32_t part) {
+  std::vector<uint32_t> w{1};
+  auto mul = [&w](uint32_t m) {
+    uint64_t carry = 0;
+    for (auto& x : w) {
+      const uint64_t t = (uint64_t)x * m + carry;
+      x = (uint32_t)t;
+      carry = t >> 32;
+    }
+    if (carry) w.push_back((uint32_t)carry);
+  };
+  auto div = [&w](uint32_t d) {
+    uint64_t rem = 0;
+    for (size_t i = w.size(); i-- > 0;) {
+      const uint64_t cur = (rem << 32) | w[i];
+      w[i] = (uint32_t)(cur / d);
+      rem = cur % d;
+    }
+    while (w.size() > 1 && w.back() == 0) w.pop_back();
+  };
+  for (uint32_t i = 2; i <= total; ++i) mul(i);
+  for (int copy = 0; copy < 3; ++copy)
+    for (uint32_t i = 2; i <= part; ++i) div(i);
+  uint32_t top = w.back(), bits = 0;
+  while (top >>= 1) ++bits;
+  return (uint32_t)(w.size() - 1) * 32 + bits;
+}
+
+// ---- targets of one attempt: SplitMix64(seed), one draw per 32-bit word, even
+// words take the low half (src/full_ter.cpp:519-532, 2364-2386).
+struct SplitMix {
+  uint64_t s;
+  uint64_t next() {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  }
+  u128 residue(uint32_t bits) {
+    const uint32_t words = (bits + 31) / 32;
+    u128 v = 0;
+    for (uint32_t i = 0; i < words; ++i) {
+      const uint64_t r = next();
+      v |= ((u128)(uint32_t)(i % 2 == 0 ? r : r >> 32)) << (32 * i);
+    }
+    return v & mask128(bits);
+  }
+};
+
+struct Targets {
+  u128 t1[3];
+  u128 t2[9];
+};
+
+Targets random_targets(uint64_t seed, uint32_t r1, uint32_t r2, u128 T) {
+  SplitMix rng{seed};
+  Targets t;
+  t.t1[0] = rng.residue(r1);
+  t.t1[1] = rng.residue(r1);
+  t.t1[2] = (T - t.t1[0] - t.t1[1]) & mask128(r1);
+  for (int g = 0; g < 3; ++g) {
+    t.t2[3 * g] = rng.residue(r2);
+    t.t2[3 * g + 1] = rng.residue(r2);
+    t.t2[3 * g + 2] = (t.t1[g] - t.t2[3 * g] - t.t2[3 * g + 1]) & mask128(r2);
+  }
+  return t;
+}
+
+uint64_t binom_host(uint32_t m, uint32_t k) {
+  if (k > m) return 0;
+  uint64_t r = 1;
+  for (uint32_t i = 0; i < k; ++i) r = r * (m - i) / (i + 1);
+  return r;
+}
+
+enum : int {
+  S_L3 = kAttemptSlotBase,        // +0..+7: left and right halves
+  S_WEIGHTS = S_L3 + 8,
+  S_BCNT, S_BOFF, S_BCUR, S_ORDER,
+  S_L2RAW,                        // +0..+3
+  S_L2CNT = S_L2RAW + 4, S_L2START, S_SCAN,
+  S_L2 = S_SCAN + 1,              // 9 lists x 4 arrays
+  S_SORT = S_L2 + 36, S_PERM, S_FLAGS, S_STARTS, S_SCAN2, S_ACC,
+  S_KEYS,                         // +0..+2
+  S_CAND = S_KEYS + 3,            // +0..+3
+  S_L1 = S_CAND + 4,              // 3 lists x 4 arrays
+  S_REC = S_L1 + 12,              // +0..+2
+  S_RKLO = S_REC + 3,             // +0..+2
+  S_RKHI = S_RKLO + 3,            // +0..+2
+  S_AFLAGS = S_RKHI + 3, S_ACOUNT
+};
+
+EntryArrays entry_slot(Workspace& w, int slot, uint64_t count) {
+  const size_t b = (count + 16) * 8;
+  return EntryArrays{ensure<uint64_t>(w, slot, b), ensure<uint64_t>(w, slot + 1, b),
+                     ensure<uint64_t>(w, slot + 2, b), ensure<uint64_t>(w, slot + 3, b)};
+}
+
+ConstEntryArrays as_const(const EntryArrays& e) {
+  return ConstEntryArrays{e.pos0, e.pos1, e.res_lo, e.res_hi};
+}
+
+template <typename T>
+void download(T* dst, const T* src, size_t n, cudaStream_t st) {
+  check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, st), "download");
+  check(cudaStreamSynchronize(st), "sync");
+}
+
+// Canonical order of `count` entries in `raw`: radix sort + unique into `dst`.
+uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, int dst_slot, EntryArrays* dst,
+                      cudaStream_t st) {
+  *dst = entry_slot(w, dst_slot, count);
+  unsigned long long* acc = ensure<unsigned long long>(w, S_ACC, 64);
+  if (count == 0) return 0;
+  launch_or_reduce(as_const(raw), count, acc, st);
+  unsigned long long vary[2];
+  download(vary, acc, 2, st);
+  uint32_t* scratch = ensure<uint32_t>(w, S_SORT, radix_scratch_words(count) * 4);
+  uint32_t* perm = ensure<uint32_t>(w, S_PERM, (count + 16) * 4);
+  radix_sort_entries(as_const(raw), count, vary[0], vary[1], perm, scratch, st);
+  uint32_t* flags = ensure<uint32_t>(w, S_FLAGS, (count + 16) * 4);
+  uint32_t* starts = ensure<uint32_t>(w, S_STARTS, (count + 16) * 4);
+  uint32_t* scan2 = ensure<uint32_t>(w, S_SCAN2, (count / 2048 + 64) * 4);
+  launch_gather_unique(as_const(raw), perm, count, *dst, flags, starts, scan2, acc + 2, st);
+  unsigned long long kept = 0;
+  download(&kept, acc + 2, 1, st);
+  return kept;
+}
+
+void cancelled_check(const tergpu_attempt_in* in) {
+  if (in->cancel != nullptr && *in->cancel != 0) {
+    t_error = "cancelled";
+    throw Failure{TERGPU_CANCELLED};
+  }
+}
+
+double ms_since(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
+int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
+  const auto t_call = std::chrono::steady_clock::now();
+  const uint32_t n = in->n;
+  if (n == 0 || n % 36 != 0 || n > 108) {
+    t_error = "full TER on the device requires n in {36, 72, 108}";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
+  if (in->values_le == nullptr || in->target_le == nullptr || in->attempt_count == 0) {
+    t_error = "instance or attempt range missing";
+    return TERGPU_INVALID_INPUT;
+  }
+  const uint32_t r1 = floor_log2_multinomial3(n / 2, n / 6) / 2;
+  const uint32_t r2 = floor_log2_multinomial3(n / 6, n / 18) / 2;
+  out->r1 = r1;
+  out->r2 = r2;
+  if (r2 == 0 || r2 >= r1 || r1 >= n || r1 - r2 > 32) {
+    t_error = "finite representation counts do not yield a supported 0 < r2 < r1 < n";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
+  const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
+  const u128 nmask = mask128(n);
+  u128 T = in->target_le[0];
+  if (w64 > 1) T |= (u128)in->target_le[1] << 64;
+  T &= nmask;
+  const uint64_t l3 = binom_host(n / 2, n / 36);
+  out->level3_size = l3;
+
+  // Preflight against the ceiling, from the expected level sizes (2x margin).
+  const double l2_est = (double)l3 * l3 / std::ldexp(1.0, r2) * 1.3 + 64;
+  const double cand_est = std::pow(l2_est, 3) / std::ldexp(1.0, r1 - r2) * 1.3 + 64;
+  const double l1_est = cand_est * 0.6;
+  const double rec = 16.0 * w64 + 4.0 * w32;
+  const double predicted = 2.0 * (2 * l3 * 32.0 + 9 * l2_est * 32 + l2_est * 120 + cand_est * (32 + 12 + 60) +
+                                  3 * l1_est * (32 + rec + 40));
+  out->device_bytes = (uint64_t)predicted;
+  if (in->memory_limit_bytes != 0 && predicted > (double)in->memory_limit_bytes) {
+    t_error = "predicted device bytes exceed the declared ceiling";
+    return TERGPU_RESOURCE_LIMIT;
+  }
+
+  Workspace& w = workspace(in->device);
+  std::lock_guard<std::mutex> lock(w.mu);
+  check(cudaSetDevice(w.device), "cudaSetDevice");
+  cudaStream_t st = w.stream;
+
+  // ---- level 3 (once per call): both halves, lexicographic k-subsets
+  std::vector<uint64_t> weights(2 * n, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    weights[2 * i] = in->values_le[i * w64];
+    weights[2 * i + 1] = w64 > 1 ? in->values_le[i * w64 + 1] : 0;
+  }
+  uint64_t* d_weights = ensure<uint64_t>(w, S_WEIGHTS, weights.size() * 8);
+  check(cudaMemcpyAsync(d_weights, weights.data(), weights.size() * 8, cudaMemcpyHostToDevice, st), "weights");
+  EntryArrays left = entry_slot(w, S_L3, l3), right = entry_slot(w, S_L3 + 4, l3);
+  launch_enumerate_half(d_weights, n, 0, l3, left, st);
+  launch_enumerate_half(d_weights, n, 1, l3, right, st);
+  const uint32_t nbk = 1u << r2;
+  uint32_t* bcnt = ensure<uint32_t>(w, S_BCNT, (nbk + 16) * 4ull);
+  uint32_t* boff = ensure<uint32_t>(w, S_BOFF, (nbk + 16) * 4ull);
+  uint32_t* bcur = ensure<uint32_t>(w, S_BCUR, (2ull * nbk + 64) * 4);
+  uint32_t* order = ensure<uint32_t>(w, S_ORDER, (l3 + 16) * 4);
+  launch_bucket_right(as_const(right), l3, r2, bcnt, boff, bcur, order, st);
+  check(cudaGetLastError(), "level 3");
+
+  int status = TERGPU_ATTEMPT_LIMIT_REACHED;
+  out->attempts_run = 0;
+  for (uint32_t k = 0; k < in->attempt_count; ++k) {
+    const uint32_t attempt = in->attempt_first + k;
+    cancelled_check(in);
+    const auto t_att = std::chrono::steady_clock::now();
+    tergpu_attempt_stats stat;
+    std::memset(&stat, 0, sizeof stat);
+    stat.attempt = attempt;
+    const Targets tg = random_targets(in->seed + attempt, r1, r2, T);
+
+    // ---- L3 -> L2: nine binary merges, each in canonical order
+    std::array<EntryArrays, 9> l2;
+    std::array<uint64_t, 9> l2n{};
+    uint32_t* counts = ensure<uint32_t>(w, S_L2CNT, (l3 + 16) * 4);
+    uint32_t* starts = ensure<uint32_t>(w, S_L2START, (l3 + 16) * 4);
+    uint32_t* scan = ensure<uint32_t>(w, S_SCAN, (l3 / 2048 + 64) * 4);
+    for (int i = 0; i < 9; ++i) {
+      const uint64_t t = (uint64_t)(tg.t2[i] & mask128(r2));
+      launch_l2_count(as_const(left), l3, boff, r2, t, counts, st);
+      launch_scan_u32(counts, l3, starts, scan, st);
+      uint32_t total = 0;
+      download(&total, starts + l3, 1, st);
+      EntryArrays raw = entry_slot(w, S_L2RAW, total);
+      launch_l2_fill(as_const(left), l3, as_const(right), boff, order, r2, t, n, starts, raw, st);
+      l2n[i] = canonicalize(w, raw, total, S_L2 + 4 * i, &l2[i], st);
+      stat.level2_sizes[i] = l2n[i];
+      stat.l3_modular += total;
+    }
+    check(cudaGetLastError(), "L3 -> L2");
+    stat.l2_ms = ms_since(t_att);
+    cancelled_check(in);
+
+    // ---- L2 -> L1: three ternary merges on the projected quotient
+    const auto t_l1 = std::chrono::steady_clock::now();
+    const uint32_t b1 = std::min(r1, r2 + 32);
+    const uint32_t qbits = b1 - r2;
+    std::array<EntryArrays, 3> l1;
+    std::array<uint64_t, 3> l1n{};
+    for (int g = 0; g < 3; ++g) {
+      const u128 m1 = mask128(b1), m2 = mask128(r2);
+      const u128 ta = tg.t2[3 * g] & m2, tb = tg.t2[3 * g + 1] & m2, t1 = tg.t1[g] & m1;
+      const u128 tc = (t1 - ta - tb) & m2;
+      if (tc != (tg.t2[3 * g + 2] & m2)) {
+        t_error = "derived third L2 target disagrees with the stored target";
+        return TERGPU_INVARIANT_VIOLATION;
+      }
+      const uint64_t tau = (uint64_t)((((t1 - ta - tb - tc) & m1) >> r2));
+      uint64_t* keys[3];
+      const u128 tt[3] = {ta, tb, tc};
+      for (int l = 0; l < 3; ++l) {
+        keys[l] = ensure<uint64_t>(w, S_KEYS + l, (l2n[3 * g + l] + 16) * 8);
+        launch_l2_quotients(as_const(l2[3 * g + l]), l2n[3 * g + l], b1, r2, (uint64_t)tt[l],
+                            (uint64_t)(tt[l] >> 64), l == 2, tau, keys[l], st);
+      }
+      JoinInput j{};
+      j.quotient_bits = qbits;
+      for (int l = 0; l < 3; ++l) {
+        j.count[l] = l2n[3 * g + l];
+        j.key_lo[l] = keys[l];
+        j.key_hi[l] = nullptr;
+        j.id[l] = nullptr;
+      }
+      // families so that at most 17 residual bits remain: the filter is exact
+      j.family_bits = std::max<uint32_t>(6, qbits > 17 ? qbits - 17 : 6);
+      if (j.family_bits + 2 > qbits) j.family_bits = 6;
+      j.filter_bits = std::clamp<uint32_t>(qbits - j.family_bits, 10, 20);
+      j.stream = st;
+      const double est = (double)j.count[0] * j.count[1] * j.count[2] / std::ldexp(1.0, qbits);
+      j.capacity = (uint64_t)(est * 1.25) + 4096;
+      JoinResult jr = run_join(w, j, 0);
+      if (jr.triples > j.capacity) {
+        j.capacity = jr.triples + 16;
+        jr = run_join(w, j, 0);
+      }
+      stat.l2_modular += jr.triples;
+      EntryArrays cand = entry_slot(w, S_CAND, jr.triples);
+      unsigned long long* acc = ensure<unsigned long long>(w, S_ACC, 64);
+      launch_l1_parents(jr.d_triples, jr.triples, as_const(l2[3 * g]), as_const(l2[3 * g + 1]),
+                        as_const(l2[3 * g + 2]), n, n / 6, cand, acc + 4, st);
+      unsigned long long ncand = 0;
+      download(&ncand, acc + 4, 1, st);
+      l1n[g] = canonicalize(w, cand, ncand, S_L1 + 4 * g, &l1[g], st);
+      stat.level1_sizes[g] = l1n[g];
+    }
+    check(cudaGetLastError(), "L2 -> L1");
+    stat.l1_ms = ms_since(t_l1);
+    cancelled_check(in);
+
+    // ---- root: records, device keys, join, authority
+    const auto t_root = std::chrono::steady_clock::now();
+    const uint32_t rb = 16 * w64 + 4 * w32;
+    uint8_t* recs[3];
+    for (int l = 0; l < 3; ++l) {
+      recs[l] = ensure<uint8_t>(w, S_REC + l, (l1n[l] + 16) * rb);
+      launch_pack_records(as_const(l1[l]), l1n[l], n, recs[l], st);
+    }
+    auto export_l1 = [&]() {
+      for (int l = 0; l < 3; ++l) {
+        for (uint32_t q = 0; q < 4; ++q) out->child_targets[l][q] = q < w32 ? (uint32_t)(tg.t1[l] >> (32 * q)) : 0u;
+        if (out->l1_records[l] != nullptr && out->l1_capacity[l] >= l1n[l] && l1n[l] != 0) {
+          check(cudaMemcpyAsync(out->l1_records[l], recs[l], l1n[l] * rb, cudaMemcpyDeviceToHost, st), "export");
+        }
+        out->l1_capacity[l] = l1n[l];
+      }
+      for (uint32_t q = 0; q < 4; ++q) out->root_target[q] = q < w32 ? (uint32_t)(T >> (32 * q)) : 0u;
+      check(cudaStreamSynchronize(st), "export");
+    };
+    if (in->flags & TERGPU_ATTEMPT_CAPTURE_ONLY) {
+      stat.status = TERGPU_NO_WITNESS_THIS_ATTEMPT;
+      stat.total_ms = ms_since(t_att);
+      if (out->stats != nullptr) out->stats[k] = stat;
+      out->attempts_run = k + 1;
+      export_l1();
+      continue;
+    }
+    const uint32_t Q = n - r1;
+    u128 tau_res = T;
+    for (int l = 0; l < 3; ++l) tau_res = (tau_res - tg.t1[l]) & nmask;
+    const u128 tau = (tau_res >> r1) & mask128(Q);
+    JoinInput j{};
+    j.quotient_bits = Q;
+    for (int l = 0; l < 3; ++l) {
+      uint64_t* klo = ensure<uint64_t>(w, S_RKLO + l, (l1n[l] + 16) * 8);
+      uint8_t* khi = ensure<uint8_t>(w, S_RKHI + l, l1n[l] + 16);
+      RecordKeyArgs ka{};
+      ka.records = recs[l];
+      ka.count = l1n[l];
+      ka.record_bytes = rb;
+      ka.res_offset = 16 * w64;
+      ka.words32 = w32;
+      ka.n = n;
+      ka.r1 = r1;
+      ka.qbits = Q;
+      ka.child_lo = (uint64_t)tg.t1[l];
+      ka.child_hi = (uint64_t)(tg.t1[l] >> 64);
+      ka.tau_lo = (uint64_t)tau;
+      ka.tau_hi = (uint64_t)(tau >> 64);
+      ka.negate = l == 2;
+      ka.key_lo = klo;
+      ka.key_hi = khi;
+      launch_record_keys(ka, st);
+      j.count[l] = l1n[l];
+      j.key_lo[l] = klo;
+      j.key_hi[l] = khi;
+      j.id[l] = nullptr;
+    }
+    j.stream = st;
+    j.capacity = 4096;
+    JoinResult jr = run_join(w, j, 0);
+    if (jr.triples > j.capacity) {
+      j.capacity = jr.triples + 16;
+      jr = run_join(w, j, 0);
+    }
+    stat.root_pairs = jr.pairs;
+    stat.root_modular = jr.triples;
+    std::vector<uint32_t> htrip;
+    std::vector<uint8_t> hflags;
+    if (jr.triples != 0) {
+      uint8_t* dflags = ensure<uint8_t>(w, S_AFLAGS, jr.triples + 16);
+      unsigned long long* acount = ensure<unsigned long long>(w, S_ACOUNT, 64);
+      check(cudaMemsetAsync(acount, 0, 64, st), "memset");
+      AuthorityArgs au{};
+      for (int l = 0; l < 3; ++l) au.records[l] = recs[l];
+      au.record_bytes = rb;
+      au.res_offset = 16 * w64;
+      au.words32 = w32;
+      au.words64 = w64;
+      au.n = n;
+      au.root_lo = (uint64_t)T;
+      au.root_hi = (uint64_t)(T >> 64);
+      au.triples = jr.d_triples;
+      au.count = jr.triples;
+      au.flags = dflags;
+      au.counters = acount;
+      launch_authority(au, st);
+      check(cudaGetLastError(), "authority");
+      htrip.resize(jr.triples * 3);
+      hflags.resize(jr.triples);
+      check(cudaMemcpyAsync(htrip.data(), jr.d_triples, jr.triples * 12, cudaMemcpyDeviceToHost, st), "d2h");
+      check(cudaMemcpyAsync(hflags.data(), dflags, jr.triples, cudaMemcpyDeviceToHost, st), "d2h");
+      check(cudaStreamSynchronize(st), "sync");
+    }
+    // valid roots: parents of the flagged triples, canonical (sorted, unique)
+    std::vector<std::array<uint64_t, 2>> parents;
+    for (uint64_t i = 0; i < jr.triples; ++i) {
+      if ((hflags[i] & 4) == 0) continue;
+      ++stat.valid_roots;
+      std::array<uint64_t, 2> p{0, 0};
+      for (int l = 0; l < 3; ++l) {
+        uint32_t wds[4];
+        check(cudaMemcpy(wds, recs[l] + (uint64_t)htrip[3 * i + l] * rb, 4 * w64 * 4, cudaMemcpyDeviceToHost),
+              "record download");
+        p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
+        if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
+      }
+      parents.push_back(p);
+    }
+    std::sort(parents.begin(), parents.end());
+    parents.erase(std::unique(parents.begin(), parents.end()), parents.end());
+    stat.level0_size = parents.size();
+    stat.root_ms = ms_since(t_root);
+    stat.total_ms = ms_since(t_att);
+    stat.status = parents.empty() ? TERGPU_NO_WITNESS_THIS_ATTEMPT : TERGPU_FOUND;
+    if (out->stats != nullptr) out->stats[k] = stat;
+    out->attempts_run = k + 1;
+
+    // L1 export of the attempt (records + targets), when the caller asked for it
+    export_l1();
+
+    if (!parents.empty()) {
+      // verify the lowest parent: binary digits, weight n/2, weights sum to the target
+      const auto& p = parents.front();
+      u128 acc = 0;
+      uint32_t weight = 0;
+      std::memset(out->witness, 0, sizeof out->witness);
+      for (uint32_t i = 0; i < n; ++i) {
+        const bool on = ((i < 64 ? p[0] >> i : p[1] >> (i - 64)) & 1) != 0;
+        if (!on) continue;
+        out->witness[i] = 1;
+        ++weight;
+        acc = (acc + ((u128)weights[2 * i + 1] << 64 | weights[2 * i])) & nmask;
+      }
+      if (weight != n / 2 || acc != T) {
+        t_error = "root witness fails verification";
+        return TERGPU_INVARIANT_VIOLATION;
+      }
+      out->found_attempt = attempt;
+      status = TERGPU_FOUND;
+      break;
+    }
+  }
+  out->status = status;
+  out->total_ms = ms_since(t_call);
+  return status;
+}
+
+}  // namespace
+}  // namespace tergpu
+
+extern "C" int tergpu_attempt_run(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
+  using namespace tergpu;
+  t_error.clear();
+  if (in == nullptr || out == nullptr) {
+    t_error = "null argument";
+    return TERGPU_INVALID_INPUT;
+  }
+  try {
+    const int st = attempt_body(in, out);
+    out->status = st;
+    return st;
+  } catch (const Failure& f) {
+    out->status = f.status;
+    return f.status;
+  } catch (const std::bad_alloc&) {
+    t_error = "host allocation failed";
+    out->status = TERGPU_RESOURCE_LIMIT;
+    return TERGPU_RESOURCE_LIMIT;
+  }
+}

@@ -8,6 +8,7 @@
 
 #include "tergpu.h"
 #include "root_kernels.cuh"
+#include "tergpu_internal.h"
 
 #include <cuda_runtime.h>
 
@@ -21,7 +22,6 @@
 #include <vector>
 
 namespace tergpu {
-namespace {
 
 thread_local std::string t_error;
 
@@ -31,25 +31,8 @@ enum Slot {
   kSlotCounters = 29, kSlotRecords = 30, kSlotFlags = 33, kSlots = 34
 };
 
-struct Buffer {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-};
-
-struct Workspace {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t start = nullptr, mid = nullptr, stop = nullptr;
-  Buffer buf[kSlots];
-  std::mutex mu;
-};
-
 std::mutex g_mu;
 std::vector<std::unique_ptr<Workspace>> g_ws;
-
-struct Failure {
-  int status;
-};
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -79,8 +62,7 @@ Workspace& workspace(int device) {
   return *g_ws.back();
 }
 
-template <typename T>
-T* ensure(Workspace& w, int slot, size_t bytes) {
+void* ensure_bytes(Workspace& w, int slot, size_t bytes) {
   bytes = std::max<size_t>(bytes, 256);
   Buffer& b = w.buf[slot];
   if (b.bytes < bytes) {
@@ -90,7 +72,7 @@ T* ensure(Workspace& w, int slot, size_t bytes) {
     check(cudaMalloc(&b.ptr, bytes), "cudaMalloc");
     b.bytes = bytes;
   }
-  return static_cast<T*>(b.ptr);
+  return b.ptr;
 }
 
 uint32_t ceil_log2(uint64_t v) {
@@ -98,11 +80,6 @@ uint32_t ceil_log2(uint64_t v) {
   while ((1ull << b) < v) ++b;
   return b;
 }
-
-struct Tuning {
-  uint32_t fb = 6, wb = 12, s_split = 1, sort_bits = 0;
-  bool v2 = true;
-};
 
 // v1: about 1024 D entries per family and about 256 filter bits per D entry.
 // v2: about 2048 D entries per family; the filter has about 8x as many words as
@@ -139,33 +116,6 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   t.s_split = std::clamp<uint32_t>((target_ctas + nfam - 1) / nfam, 1, nfam);
   return t;
 }
-
-// Device-resident inputs of one join: keys per list.
-struct JoinInput {
-  uint32_t quotient_bits;
-  uint64_t count[3];
-  const uint64_t* key_lo[3];  // device
-  const uint8_t* key_hi[3];   // device or null
-  const uint32_t* id[3];      // device or null
-  const uint8_t* cells;       // host or null
-  const uint8_t* cells_device;  // device or null (takes precedence)
-  uint32_t projected_bits;
-  uint32_t family_bits, filter_bits;
-  uint64_t memory_limit_bytes;
-  uint64_t capacity;
-  bool count_only;
-  bool sweep_v1;
-  cudaStream_t stream;
-};
-
-struct JoinResult {
-  uint64_t triples = 0, pairs = 0, survivors = 0, fast = 0, projected = 0;
-  uint64_t device_bytes = 0;
-  float join_ms = 0, partition_ms = 0, sweep_ms = 0;
-  uint32_t launches = 0;
-  Tuning tuning;
-  uint32_t* d_triples = nullptr;
-};
 
 uint64_t partition_bytes(const uint64_t count[3], uint32_t fb) {
   uint64_t b = 0;
@@ -603,7 +553,6 @@ int root_records_body(const void* vin, void* vout) {
   return status;
 }
 
-}  // namespace
 }  // namespace tergpu
 
 extern "C" {
@@ -638,10 +587,10 @@ void tergpu_release(void) {
   for (auto& w : tergpu::g_ws) {
     std::lock_guard<std::mutex> inner(w->mu);
     cudaSetDevice(w->device);
-    for (auto& b : w->buf) {
-      if (b.ptr != nullptr) cudaFree(b.ptr);
-      b.ptr = nullptr;
-      b.bytes = 0;
+    for (auto& kv : w->buf) {
+      if (kv.second.ptr != nullptr) cudaFree(kv.second.ptr);
+      kv.second.ptr = nullptr;
+      kv.second.bytes = 0;
     }
     if (w->start) cudaEventDestroy(w->start);
     if (w->mid) cudaEventDestroy(w->mid);

@@ -1,0 +1,152 @@
+"""Full TER attempts on the device: the host mirror of solve_full_ter's attempt loop.
+
+`solve_full_ter(instance, config)` mirrors the reference's entry point
+(include/ter/full_ter.hpp:255-256, src/full_ter.cpp:2933-3521) for the
+FiniteSanity shape with random targets: attempt a uses SplitMix64(seed + a);
+the result carries the status, the verified witness and per-attempt telemetry
+(level sizes and candidate counts).  `instance` comes from tergpu.instance.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from .root import TergpuError
+
+
+class AttemptStats(ctypes.Structure):
+    _fields_ = [
+        ("attempt", ctypes.c_uint32), ("status", ctypes.c_int32),
+        ("level2_sizes", ctypes.c_uint64 * 9), ("level1_sizes", ctypes.c_uint64 * 3),
+        ("level0_size", ctypes.c_uint64), ("l3_modular", ctypes.c_uint64),
+        ("l2_modular", ctypes.c_uint64), ("root_modular", ctypes.c_uint64),
+        ("valid_roots", ctypes.c_uint64), ("root_pairs", ctypes.c_uint64),
+        ("l2_ms", ctypes.c_double), ("l1_ms", ctypes.c_double), ("root_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+class AttemptIn(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+        ("values_le", ctypes.POINTER(ctypes.c_uint64)), ("target_le", ctypes.POINTER(ctypes.c_uint64)),
+        ("seed", ctypes.c_uint64), ("attempt_first", ctypes.c_uint32),
+        ("attempt_count", ctypes.c_uint32), ("memory_limit_bytes", ctypes.c_uint64),
+        ("cancel", ctypes.POINTER(ctypes.c_int32)), ("device", ctypes.c_int32),
+    ]
+
+
+class AttemptOut(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32), ("r1", ctypes.c_uint32), ("r2", ctypes.c_uint32),
+        ("level3_size", ctypes.c_uint64), ("attempts_run", ctypes.c_uint32),
+        ("found_attempt", ctypes.c_uint32), ("witness", ctypes.c_uint8 * 128),
+        ("stats", ctypes.POINTER(AttemptStats)), ("l1_records", ctypes.POINTER(ctypes.c_uint8) * 3),
+        ("l1_capacity", ctypes.c_uint64 * 3), ("child_targets", (ctypes.c_uint32 * 4) * 3),
+        ("root_target", ctypes.c_uint32 * 4), ("device_bytes", ctypes.c_uint64),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+@dataclass
+class FullTerConfig:
+    """The fields of the reference's FullTerConfig this path honours."""
+    seed: int = 1
+    attempt_limit: int = 1
+    attempt_first: int = 0
+    memory_limit_bytes: int = 0
+    device: int = 0
+    export_l1_capacity: int = 0   # > 0: return the last attempt's L1 lists as a Snapshot
+    capture_only: bool = False    # stop after L1 (the device stream_full_ter_root_lists)
+
+
+@dataclass
+class FullTerResult:
+    status: int
+    r1: int = 0
+    r2: int = 0
+    level3_size: int = 0
+    witness: np.ndarray | None = None
+    found_attempt: int | None = None
+    attempts: list = field(default_factory=list)
+    snapshot: object | None = None
+    total_ms: float = 0.0
+
+    @property
+    def status_name(self) -> str:
+        return _abi.STATUS_NAMES.get(self.status, str(self.status))
+
+
+def _stats_dict(s: AttemptStats) -> dict:
+    return {
+        "attempt": int(s.attempt), "status": int(s.status),
+        "level2": [int(v) for v in s.level2_sizes], "level1": [int(v) for v in s.level1_sizes],
+        "level0": int(s.level0_size), "l3_modular": int(s.l3_modular),
+        "l2_modular": int(s.l2_modular), "root_modular": int(s.root_modular),
+        "valid_roots": int(s.valid_roots), "root_pairs": int(s.root_pairs),
+        "l2_ms": float(s.l2_ms), "l1_ms": float(s.l1_ms), "root_ms": float(s.root_ms),
+        "total_ms": float(s.total_ms),
+    }
+
+
+def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -> FullTerResult:
+    """Runs attempts [attempt_first, attempt_first + attempt_limit) on the device.
+
+    `cancel` may be a ctypes.c_int32 whose value the caller sets from another
+    thread; the loop stops with Cancelled at the next stage boundary."""
+    config = config or FullTerConfig()
+    lib = _abi.load()
+    lib.tergpu_attempt_run.argtypes = [ctypes.POINTER(AttemptIn), ctypes.POINTER(AttemptOut)]
+    lib.tergpu_attempt_run.restype = ctypes.c_int
+    values = np.ascontiguousarray(instance.values_le, dtype=np.uint64).reshape(-1)
+    target = np.ascontiguousarray(instance.target_le, dtype=np.uint64)
+    ain = AttemptIn()
+    ain.n = instance.n
+    ain.flags = 1 if config.capture_only else 0
+    ain.values_le = values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+    ain.target_le = target.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+    ain.seed = config.seed & (2**64 - 1)
+    ain.attempt_first = config.attempt_first
+    ain.attempt_count = config.attempt_limit
+    ain.memory_limit_bytes = config.memory_limit_bytes
+    ain.cancel = ctypes.pointer(cancel) if cancel is not None else None
+    ain.device = config.device
+    stats = (AttemptStats * max(1, config.attempt_limit))()
+    out = AttemptOut()
+    out.stats = ctypes.cast(stats, ctypes.POINTER(AttemptStats))
+    w64, w32 = (instance.n + 63) // 64, (instance.n + 31) // 32
+    rb = 16 * w64 + 4 * w32
+    bufs = []
+    if config.export_l1_capacity > 0:
+        for l in range(3):
+            b = np.zeros(config.export_l1_capacity * rb, dtype=np.uint8)
+            bufs.append(b)
+            out.l1_records[l] = b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+            out.l1_capacity[l] = config.export_l1_capacity
+    st = lib.tergpu_attempt_run(ctypes.byref(ain), ctypes.byref(out))
+    if st not in (_abi.FOUND, _abi.ATTEMPT_LIMIT_REACHED, _abi.CANCELLED, _abi.RESOURCE_LIMIT,
+                  _abi.INVALID_CONFIGURATION):
+        raise TergpuError(st, _abi.last_error())
+    res = FullTerResult(status=st, r1=int(out.r1), r2=int(out.r2), level3_size=int(out.level3_size),
+                        total_ms=float(out.total_ms),
+                        attempts=[_stats_dict(stats[i]) for i in range(int(out.attempts_run))])
+    if st == _abi.FOUND:
+        res.witness = np.array(out.witness[: instance.n], dtype=np.uint8)
+        res.found_attempt = int(out.found_attempt)
+    if bufs and out.attempts_run > 0:
+        from .snapshot import Snapshot
+
+        sizes = [int(out.l1_capacity[l]) for l in range(3)]
+        if all(sizes[l] <= config.export_l1_capacity for l in range(3)):
+            last = res.attempts[-1]
+            res.snapshot = Snapshot(
+                n=instance.n, r1=res.r1, r2=res.r2, attempt=last["attempt"], seed=config.seed,
+                attempt_seed=(config.seed + last["attempt"]) & (2**64 - 1),
+                records=[bufs[l][: sizes[l] * rb].copy() for l in range(3)],
+                child_targets=[np.array(out.child_targets[l][:w32], dtype=np.uint32) for l in range(3)],
+                root_target=np.array(out.root_target[:w32], dtype=np.uint32),
+                level2_sizes=last["level2"])
+    return res
