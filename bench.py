@@ -1,11 +1,13 @@
 #!/usr/bin/env python
 """Benchmark of the B200 root join: n=108 root logical pairs/s.
 
-Workload: one whole n=108 root (the L1 list sizes of seed 0x1001 attempt 0:
-3,650,689 x 6,900,048 logical pairs against 6,896,564 targets, 69-bit root
-quotient), synthetic uniform keys from a seeded counter-based generator plus 8
-planted full-Q triples.  A step = one full pass of the hot path (device radix
-partition of all three lists + the sweep over all 2.5e13 pairs + exact
+Workload: one whole authentic n=108 root -- the three L1 lists of the
+reference's benchmark instance, seed 0x1001, attempt 0 (3,650,689 x 6,900,048
+logical pairs against 6,896,564 targets, 69-bit root quotient), produced on the
+device by this library's attempt pipeline (level sizes equal the reference's
+published capture).  --synthetic swaps in uniform seeded keys of the same sizes
+with 8 planted full-Q triples.  A step = one full pass of the hot path (device
+radix partition of all three lists + the sweep over all 2.5e13 pairs + exact
 resolution).  Inputs (226 MB) exceed L2 (126 MB), so no flush is needed.
 
   value  : pairs/s with keys already resident in HBM (CUDA events on the
@@ -62,6 +64,8 @@ def parse():
                    help="cells of the reference's declared subsample timed on one core")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--synthetic", action="store_true",
+                   help="uniform seeded keys (+8 planted triples) instead of the authentic root")
     return p.parse_args()
 
 
@@ -69,9 +73,32 @@ def sizes_for(args):
     return tuple(max(1, int(round(s * args.scale))) for s in SIZES)
 
 
-def workload_name(sizes):
-    return (f"n=108 whole root: {sizes[0]} x {sizes[1]} logical pairs against {sizes[2]} "
-            f"targets, Q={QBITS}, uniform seeded keys + {PLANTED} planted full-Q triples")
+def workload_name(sizes, synthetic=True, seed=0x1001):
+    if synthetic:
+        return (f"n=108 whole root: {sizes[0]} x {sizes[1]} logical pairs against {sizes[2]} "
+                f"targets, Q={QBITS}, uniform seeded keys + {PLANTED} planted full-Q triples")
+    return (f"n=108 whole authentic root (benchmark instance seed {seed:#x}, attempt 0): "
+            f"{sizes[0]} x {sizes[1]} logical pairs against {sizes[2]} targets, Q={QBITS}")
+
+
+def authentic_root(seed: int):
+    """L1 lists of attempt 0 of the n=108 benchmark instance, from the device
+    attempt pipeline, as root keys (list 2 = tau - q_C)."""
+    import tergpu
+    from tergpu import attempt, instance, snapshot
+
+    t0 = time.perf_counter()
+    inst = instance.benchmark_instance(108, seed)
+    res = attempt.solve_full_ter(inst, attempt.FullTerConfig(seed=seed, attempt_limit=1,
+                                                             capture_only=True,
+                                                             export_l1_capacity=7_500_000))
+    if res.snapshot is None:
+        raise RuntimeError(f"attempt pipeline failed: {res.status_name}")
+    capture_ms = res.attempts[0]["total_ms"]
+    q, lo, hi, _ = snapshot.root_keys(res.snapshot)
+    keys = tergpu.RootKeys(quotient_bits=q, lo=lo, hi=hi)
+    return keys, {"capture_ms": capture_ms, "level2": res.attempts[0]["level2"],
+                  "level1": res.attempts[0]["level1"], "setup_s": time.perf_counter() - t0}
 
 
 class ClockSampler:
@@ -142,11 +169,18 @@ def run_tergpu(args):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    sizes = sizes_for(args)
-    keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=args.seed + rank,
-                                   planted=PLANTED)
-    planted = {(sizes[0] - 1 - i, sizes[1] - 1 - i, sizes[2] - 1 - i) for i in range(PLANTED)}
+    capture = None
+    if args.synthetic:
+        sizes = sizes_for(args)
+        keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=args.seed + rank,
+                                       planted=PLANTED)
+        planted = {(sizes[0] - 1 - i, sizes[1] - 1 - i, sizes[2] - 1 - i) for i in range(PLANTED)}
+    else:
+        keys, capture = authentic_root(args.seed + rank)
+        sizes = tuple(len(a) for a in keys.lo)
+        planted = set()
     lib = _abi.load()
+    first_triples = []
 
     # device-resident keys (torch is only the allocator here)
     d_lo = [torch.from_numpy(k.view(np.int64)).cuda() for k in keys.lo]
@@ -184,9 +218,13 @@ def run_tergpu(args):
         if st != _abi.COMPLETED:
             raise RuntimeError(f"tergpu_root_run status {st}: {_abi.last_error()}")
         n = int(out.triples_count)
-        got = {tuple(t) for t in host_trip[: 3 * n].reshape(-1, 3).tolist()}
-        if not planted <= got:
+        got = sorted(tuple(t) for t in host_trip[: 3 * n].reshape(-1, 3).tolist())
+        if not planted <= set(got):
             raise RuntimeError("a planted full-Q triple is missing")
+        if not first_triples:
+            first_triples.append(got)
+        elif got != first_triples[0]:
+            raise RuntimeError("two passes over the same root reported different triples")
         return out
 
     def barrier():
@@ -259,8 +297,12 @@ def run_tergpu(args):
             "metric": METRIC, "value": world * pairs / (ms / 1000.0), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u64", "data": "synthetic",
-            "config": {"workload": workload_name(sizes), "seed": args.seed,
+            "dtype": "u64",
+            "data": ("synthetic" if args.synthetic else
+                     "authentic: L1 lists generated on the device by this library's attempt "
+                     "pipeline from the reference's benchmark instance (sizes equal its published capture)"),
+            "config": {"workload": workload_name(sizes, args.synthetic, args.seed), "seed": args.seed,
+                       "capture": capture,
                        "l2_flush": "inputs (226 MB) larger than L2 (126 MB)",
                        "family_bits": int(outs[-1].family_bits),
                        "filter_bits": int(outs[-1].filter_bits),
@@ -345,7 +387,7 @@ def run_reference(args):
     binary = ref_binary()
     base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "config": {"workload": workload_name(sizes), "seed": args.seed,
+            "config": {"workload": workload_name(sizes, args.synthetic, args.seed), "seed": args.seed,
                        "parallelism": "host processes"}}
     if not binary.exists():
         base["unavailable"] = "reference harness oracle/_ref/terref was not built on this host"
@@ -353,8 +395,15 @@ def run_reference(args):
         return
     from tergpu import workload
 
-    keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=args.seed,
-                                   planted=PLANTED)
+    if args.synthetic:
+        keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=args.seed,
+                                       planted=PLANTED)
+    else:
+        # the authentic root's L1 lists come from the device attempt pipeline
+        # (bit-identical to the reference's capture); only ARWLF is timed
+        keys, _ = authentic_root(args.seed)
+        sizes = tuple(len(a) for a in keys.lo)
+        base["config"]["workload"] = workload_name(sizes, False, args.seed)
     procs_n = max(1, min(os.cpu_count() or 1, 64))
     cells_per = max(1, args.cpu_cells)
     reps = max(1, args.steps + args.warmup)
