@@ -19,7 +19,10 @@ resolution).  Inputs (226 MB) exceed L2 (126 MB), so no flush is needed.
            disjoint cells of the same root.
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own independent
-root (seed + rank) -- weak scaling, no data-path collective.
+root (seed + rank) -- weak scaling, no data-path collective.  --shard-root
+splits ONE root over the ranks instead (rank r joins the D entries with
+key_d == r (mod G), G the power of two >= N; each step ends with one all-gather
+of the triples) -- strong scaling.
 """
 from __future__ import annotations
 
@@ -64,6 +67,8 @@ def parse():
                    help="cells of the reference's declared subsample timed on one core")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--shard-root", action="store_true",
+                   help="N>1: split one root over the ranks (strong scaling) instead of replicas")
     p.add_argument("--synthetic", action="store_true",
                    help="uniform seeded keys (+8 planted triples) instead of the authentic root")
     return p.parse_args()
@@ -169,14 +174,20 @@ def run_tergpu(args):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from tergpu.shard import shard_count_for, shards_of_rank
+
+    sharded = args.shard_root and world > 1
+    my_shards = shards_of_rank(rank, world) if sharded else [0]
+    shard_count = shard_count_for(world) if sharded else 1
+    root_seed = args.seed if sharded else args.seed + rank
     capture = None
     if args.synthetic:
         sizes = sizes_for(args)
-        keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=args.seed + rank,
+        keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=root_seed,
                                        planted=PLANTED)
         planted = {(sizes[0] - 1 - i, sizes[1] - 1 - i, sizes[2] - 1 - i) for i in range(PLANTED)}
     else:
-        keys, capture = authentic_root(args.seed + rank)
+        keys, capture = authentic_root(root_seed)
         sizes = tuple(len(a) for a in keys.lo)
         planted = set()
     lib = _abi.load()
@@ -189,7 +200,7 @@ def run_tergpu(args):
     cap = 4096
     host_trip = np.zeros(cap * 3, dtype=np.uint32)
 
-    def make_in(resident: bool, lo_src, hi_src):
+    def make_in(resident: bool, lo_src, hi_src, shard: int = 0):
         rin = _abi.RootIn()
         rin.quotient_bits = QBITS
         rin.flags = (_abi.ROOT_DEVICE_INPUTS if resident else 0) | \
@@ -208,30 +219,57 @@ def run_tergpu(args):
         rin.family_bits = args.family_bits
         rin.filter_bits = args.filter_bits
         rin.stream = ctypes.c_void_p(stream.cuda_stream)
+        rin.shard_index = shard
+        rin.shard_count = shard_count
         return rin
 
-    def call(rin):
-        out = _abi.RootOut()
-        out.triples = host_trip.ctypes.data_as(_abi._u32p)
-        out.capacity = cap
-        st = lib.tergpu_root_run(ctypes.byref(rin), ctypes.byref(out))
-        if st != _abi.COMPLETED:
-            raise RuntimeError(f"tergpu_root_run status {st}: {_abi.last_error()}")
-        n = int(out.triples_count)
-        got = sorted(tuple(t) for t in host_trip[: 3 * n].reshape(-1, 3).tolist())
+    def gather(got):
+        """One all-gather of this rank's triples (count + 12-byte records)."""
+        if not sharded:
+            return got
+        mine = torch.tensor(got, dtype=torch.int64, device="cuda").reshape(-1, 3)
+        counts = [torch.zeros(1, dtype=torch.int64, device="cuda") for _ in range(world)]
+        dist.all_gather(counts, torch.tensor([len(got)], dtype=torch.int64, device="cuda"))
+        width = max(1, max(int(c.item()) for c in counts))
+        pad = torch.zeros((width, 3), dtype=torch.int64, device="cuda")
+        pad[: len(got)] = mine
+        bufs = [torch.zeros_like(pad) for _ in range(world)]
+        dist.all_gather(bufs, pad)
+        return sorted(tuple(t) for b, c in zip(bufs, counts) for t in b[: int(c.item())].tolist())
+
+    def call(rins):
+        """One step: this rank's shard(s) of the root, then the gather."""
+        got, outs_ = [], []
+        for rin in rins:
+            out = _abi.RootOut()
+            out.triples = host_trip.ctypes.data_as(_abi._u32p)
+            out.capacity = cap
+            st = lib.tergpu_root_run(ctypes.byref(rin), ctypes.byref(out))
+            if st != _abi.COMPLETED:
+                raise RuntimeError(f"tergpu_root_run status {st}: {_abi.last_error()}")
+            n = int(out.triples_count)
+            got += [tuple(t) for t in host_trip[: 3 * n].reshape(-1, 3).tolist()]
+            outs_.append(out)
+        got = gather(sorted(got))
         if not planted <= set(got):
             raise RuntimeError("a planted full-Q triple is missing")
         if not first_triples:
             first_triples.append(got)
         elif got != first_triples[0]:
             raise RuntimeError("two passes over the same root reported different triples")
+        out = outs_[0]
+        for o in outs_[1:]:
+            for f in ("logical_pairs", "filter_survivors", "triples_count", "kernel_launches"):
+                setattr(out, f, getattr(out, f) + getattr(o, f))
+            for f in ("sweep_ms", "partition_ms", "join_ms"):
+                setattr(out, f, getattr(out, f) + getattr(o, f))
         return out
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    rin = make_in(True, d_lo, d_hi)
+    rin = [make_in(True, d_lo, d_hi, i) for i in my_shards]
     for _ in range(max(3, args.warmup)):
         out = call(rin)
     barrier()
@@ -248,7 +286,7 @@ def run_tergpu(args):
     ms = ev0.elapsed_time(ev1) / args.steps
     sweep_ms = statistics.median(o.sweep_ms for o in outs)
     part_ms = statistics.median(o.partition_ms for o in outs)
-    pairs = int(outs[-1].logical_pairs)
+    pairs = local_pairs = int(outs[-1].logical_pairs)
     launches = sum(int(o.kernel_launches) for o in outs)
     survivors = int(outs[-1].filter_survivors)
     triples = int(outs[-1].triples_count)
@@ -256,13 +294,17 @@ def run_tergpu(args):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+        # whole-job pairs: the shards of one root, or every rank's own root
+        t = torch.tensor([pairs], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        pairs = int(t.item())
 
     # e2e: pinned host keys through the C ABI, copies inside the timed region
     e2e = None
     if not args.no_e2e:
         h_lo = [torch.from_numpy(k.view(np.int64)).pin_memory() for k in keys.lo]
         h_hi = [torch.from_numpy(h).pin_memory() for h in keys.hi]
-        rin_h = make_in(False, h_lo, h_hi)
+        rin_h = [make_in(False, h_lo, h_hi, i) for i in my_shards]
         call(rin_h)
         barrier()
         torch.cuda.synchronize()
@@ -274,9 +316,9 @@ def run_tergpu(args):
             t = torch.tensor([e_ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e_ms = float(t.item())
-        h2d = sum(s * 9 for s in sizes)
+        h2d = sum(s * 9 for s in sizes) * len(my_shards)
         d2h = triples * 12 + 8 * 8 + 2 * 4 * (1 << e_outs[-1].family_bits)
-        e2e = {"value": world * pairs / (e_ms / 1000.0), "unit": UNIT, "ms_per_step": e_ms,
+        e2e = {"value": pairs / (e_ms / 1000.0), "unit": UNIT, "ms_per_step": e_ms,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     result = None
@@ -294,9 +336,10 @@ def run_tergpu(args):
         part_bytes = sum(sizes) * (2 * 9 + 8 + 13 + 4)  # hist read, scatter read + write
         issue_peak = 148 * 4 * 32 * sm_mhz * 1e6 / OPS_PER_PAIR
         result = {
-            "metric": METRIC, "value": world * pairs / (ms / 1000.0), "unit": UNIT,
+            "metric": METRIC, "value": pairs / (ms / 1000.0), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
             "dtype": "u64",
             "data": ("synthetic" if args.synthetic else
                      "authentic: L1 lists generated on the device by this library's attempt "
@@ -308,15 +351,16 @@ def run_tergpu(args):
                        "filter_bits": int(outs[-1].filter_bits),
                        "partition_ms": part_ms, "sweep_ms": sweep_ms,
                        "filter_survivors": survivors, "full_q_triples": triples,
-                       "parallelism": f"replicas{world}"},
+                       "parallelism": (f"shards{shard_count}-over-{world}" if sharded
+                                       else f"replicas{world}")},
             "roofline": {"bound": "hbm", "kernel": "k_sweep",
                          "achieved": sweep_bytes / (sweep_ms / 1000.0) / 1e9, "peak": hbm,
                          "unit": "GB/s", "frac": sweep_bytes / (sweep_ms / 1000.0) / 1e9 / hbm,
                          "peak_source": peak_src, "traffic": None,
                          "note": "the sweep is issue-bound, not HBM-bound: see issue_roofline"},
             "issue_roofline": {"bound": "int32-issue", "kernel": "k_sweep", "unit": "pairs/s",
-                               "achieved": pairs / (sweep_ms / 1000.0), "peak": issue_peak,
-                               "frac": pairs / (sweep_ms / 1000.0) / issue_peak,
+                               "achieved": local_pairs / (sweep_ms / 1000.0), "peak": issue_peak,
+                               "frac": local_pairs / (sweep_ms / 1000.0) / issue_peak,
                                "ops_per_pair": OPS_PER_PAIR, "sm_mhz": sm_mhz},
             "partition_roofline": {"bound": "hbm", "unit": "GB/s",
                                    "achieved": part_bytes / (part_ms / 1000.0) / 1e9, "peak": hbm,

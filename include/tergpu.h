@@ -87,6 +87,12 @@ typedef struct {
   uint32_t family_bits;        /* 0: autotuned; else the device partition radix (6..16) */
   uint32_t filter_bits;        /* 0: autotuned; else log2 of the filter bitmap bits (10..20) */
   void *stream;                /* cudaStream_t to launch on; NULL: the library's own */
+  uint32_t shard_index;        /* join only the pairs whose sum key_a + key_b is */
+  uint32_t shard_count;        /* == shard_index (mod shard_count), i.e. the D entries with
+                                  key_d == shard_index (mod shard_count); shard_count 0 or 1:
+                                  the whole root, else a power of two <= 64.  The shards of
+                                  one root are disjoint and together give the whole root
+                                  (the multi-GPU split: one shard per GPU) */
 } tergpu_root_in;
 
 typedef struct {
@@ -147,6 +153,8 @@ typedef struct {
   uint64_t memory_limit_bytes;
   uint32_t family_bits;
   uint32_t filter_bits;
+  uint32_t shard_index;        /* as tergpu_root_in.shard_index / shard_count */
+  uint32_t shard_count;
 } tergpu_root_records_in;
 
 typedef struct {

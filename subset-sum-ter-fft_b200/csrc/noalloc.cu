@@ -203,6 +203,8 @@ extern "C" int tergpu_root_run_noalloc(const tergpu_root_in* in, tergpu_root_out
   a.cells = in->cells;  // device pointer or null
   a.fb = fb;
   a.s_split = s_split;
+  a.shard = 0;
+  a.shards = 1;
   a.wb = wb;
   a.rb = F - fb;
   a.mrb = F - fb;

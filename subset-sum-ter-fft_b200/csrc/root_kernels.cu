@@ -130,8 +130,9 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
   uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kYCap);
   uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
 
-  const uint32_t u = blockIdx.x % nfam;
-  const uint32_t part = blockIdx.x / nfam;
+  const uint32_t nloc = nfam / a.shards;  // target families of this shard
+  const uint32_t u = a.shard + a.shards * (blockIdx.x % nloc);
+  const uint32_t part = blockIdx.x / nloc;
   const uint32_t s_per = (nfam + a.s_split - 1u) / a.s_split;
   const uint32_t s0 = part * s_per;
   const uint32_t s1 = min(nfam, s0 + s_per);
@@ -304,8 +305,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
   uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
   uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweepWarps * kQueueCap);
 
-  const uint32_t u = blockIdx.x % nfam;
-  const uint32_t part = blockIdx.x / nfam;
+  const uint32_t nloc = nfam / a.shards;  // target families of this shard
+  const uint32_t u = a.shard + a.shards * (blockIdx.x % nloc);
+  const uint32_t part = blockIdx.x / nloc;
   const uint32_t s_per = (nfam + a.s_split - 1u) / a.s_split;
   const uint32_t s0 = part * s_per;
   const uint32_t s1 = min(nfam, s0 + s_per);
@@ -651,7 +653,7 @@ size_t sweep_smem_bytes(uint32_t wb) {
 
 void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st) {
   const size_t smem = sweep_smem_bytes(a.wb);
-  const unsigned grid = (1u << a.fb) * a.s_split;
+  const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
   if (aligned) {
     cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_sweep<true><<<grid, kSweepThreads, smem, st>>>(a);
@@ -663,7 +665,7 @@ void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st) {
 
 void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
   const size_t smem = sweep_smem_bytes(a.wb) + static_cast<size_t>(kSweepWarps) * 32 * 8 * 4;
-  const unsigned grid = (1u << a.fb) * a.s_split;
+  const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
   if (aligned) {
     cudaFuncSetAttribute(k_sweep2<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_sweep2<true, 8><<<grid, kSweepThreads, smem, st>>>(a);

@@ -87,7 +87,7 @@ uint32_t ceil_log2(uint64_t v) {
 // rate |D_u| / 2^(wb+5) ~ 0.3 %); narrower filters make the probes of 32
 // consecutive sorted B entries nearly conflict-free but pass too many pairs.
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
-                     uint32_t fb_req, uint32_t filter_req, bool v2) {
+                     uint32_t fb_req, uint32_t filter_req, bool v2, uint32_t shards) {
   Tuning t;
   t.v2 = v2;
   uint32_t fb_max = std::min<uint32_t>(14, fast_bits - 2);
@@ -112,8 +112,9 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   }
   t.sort_bits = std::min<uint32_t>(t.wb, 12);
   const uint32_t nfam = 1u << t.fb;
+  const uint32_t nloc = std::max<uint32_t>(1, nfam / shards);  // target families per shard
   const uint32_t target_ctas = 148 * 2 * 8;
-  t.s_split = std::clamp<uint32_t>((target_ctas + nfam - 1) / nfam, 1, nfam);
+  t.s_split = std::clamp<uint32_t>((target_ctas + nloc - 1) / nloc, 1, nfam);
   return t;
 }
 
@@ -127,6 +128,15 @@ uint64_t partition_bytes(const uint64_t count[3], uint32_t fb) {
   return b;
 }
 
+uint32_t checked_shards(uint32_t index, uint32_t count) {
+  const uint32_t n = count == 0 ? 1u : count;
+  if (n > 64 || (n & (n - 1)) != 0 || index >= n) {
+    t_error = "shard_count must be 0 or a power of two <= 64, and shard_index below it";
+    throw Failure{TERGPU_INVALID_INPUT};
+  }
+  return n;
+}
+
 // Partition + sweep(s) on keys already on the device.  The only host
 // synchronization is the final download of counters and family sizes.
 JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
@@ -135,8 +145,9 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   const uint32_t F = std::min<uint32_t>(Q, 64);
   const uint32_t hi_bits = Q - F;
   r.tuning = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, in.family_bits,
-                           in.filter_bits, !in.sweep_v1);
+                           in.filter_bits, !in.sweep_v1, in.shards);
   const Tuning& tu = r.tuning;
+  checked_shards(in.shard, in.shards);
   if (tu.fb < 6 || tu.fb > 16 || tu.fb + 2 > F || tu.wb < 5 || tu.wb > 15 ||
       (in.projected_bits != 0 && (in.projected_bits > F || in.projected_bits < tu.fb + 1))) {
     t_error = "family/filter bits outside the supported range for this quotient width";
@@ -203,6 +214,8 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   a.cells = d_cells;
   a.fb = tu.fb;
   a.s_split = tu.s_split;
+  a.shard = in.shard;
+  a.shards = in.shards;
   a.wb = tu.wb;
   a.rb = F - tu.fb;
   a.hi_bits = hi_bits;
@@ -254,6 +267,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   }
   for (uint32_t s = 0; s < nfam; ++s) {
     for (uint32_t t = 0; t < nfam; ++t) {
+      if (((s + t) & (nfam - 1u) & (in.shards - 1u)) != in.shard) continue;
       if (!hcells.empty() && hcells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
       r.pairs += static_cast<uint64_t>(hcnt[0][s]) * hcnt[1][t];
     }
@@ -380,6 +394,8 @@ int root_run_body(const void* vin, void* vout) {
   j.capacity = count_only ? 0 : out->capacity;
   j.count_only = count_only;
   j.sweep_v1 = (in->flags & TERGPU_ROOT_SWEEP_V1) != 0;
+  j.shard = in->shard_index;
+  j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);
   fill_out(res, out);
   int status = TERGPU_COMPLETED;
@@ -508,6 +524,8 @@ int root_records_body(const void* vin, void* vout) {
   j.capacity = count_only ? 0 : out->root.capacity;
   j.count_only = count_only;
   j.sweep_v1 = (in->flags & TERGPU_ROOT_SWEEP_V1) != 0;
+  j.shard = in->shard_index;
+  j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);
   fill_out(res, &out->root);
   out->residue_exact = out->structural = out->valid_roots = 0;

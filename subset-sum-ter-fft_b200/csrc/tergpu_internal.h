@@ -64,6 +64,7 @@ struct JoinInput {
   uint64_t capacity;
   bool count_only;
   bool sweep_v1;
+  uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
   cudaStream_t stream;
 };
 
@@ -75,6 +76,11 @@ struct JoinResult {
   Tuning tuning;
   uint32_t* d_triples = nullptr;  // device, capacity triples (valid until the next join)
 };
+
+// Checks a (shard_index, shard_count) pair of the C ABI and returns the shard
+// count (count 0 means 1).  Throws Failure(InvalidInput) unless the count is a
+// power of two in [1, 64] and the index is below it.
+uint32_t checked_shards(uint32_t index, uint32_t count);
 
 // Partition + sweep on keys already on the device (throws Failure).
 JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes);

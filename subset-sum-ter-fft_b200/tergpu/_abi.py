@@ -52,7 +52,8 @@ class RootIn(ctypes.Structure):
         ("id", _u32p * 3), ("cells", _u8p), ("projected_bits", ctypes.c_uint32),
         ("device", ctypes.c_int32), ("memory_limit_bytes", ctypes.c_uint64),
         ("family_bits", ctypes.c_uint32), ("filter_bits", ctypes.c_uint32),
-        ("stream", ctypes.c_void_p),
+        ("stream", ctypes.c_void_p), ("shard_index", ctypes.c_uint32),
+        ("shard_count", ctypes.c_uint32),
     ]
 
 
@@ -75,7 +76,8 @@ class RootRecordsIn(ctypes.Structure):
         ("records", _u8p * 3), ("child_target", _u32p * 3), ("root_target", _u32p),
         ("cells", _u8p), ("projected_bits", ctypes.c_uint32), ("device", ctypes.c_int32),
         ("memory_limit_bytes", ctypes.c_uint64), ("family_bits", ctypes.c_uint32),
-        ("filter_bits", ctypes.c_uint32),
+        ("filter_bits", ctypes.c_uint32), ("shard_index", ctypes.c_uint32),
+        ("shard_count", ctypes.c_uint32),
     ]
 
 

@@ -48,6 +48,8 @@ class Config:
     count_only: bool = False
     capacity: int = 1 << 16
     sweep_v1: bool = False
+    shard_index: int = 0
+    shard_count: int = 1  # power of two <= 64: join only D entries with key_d == index (mod count)
 
 
 @dataclass
@@ -124,6 +126,8 @@ def run_gpu_root(keys: RootKeys, config: Config | None = None,
     rin.memory_limit_bytes = config.memory_limit_bytes
     rin.family_bits = config.family_bits
     rin.filter_bits = config.filter_bits
+    rin.shard_index = config.shard_index
+    rin.shard_count = config.shard_count
     capacity = max(1, config.capacity)
     for _ in range(2):
         buf = np.zeros(capacity * 3, dtype=np.uint32)
@@ -168,6 +172,8 @@ def run_gpu_root_records(snap, config: Config | None = None,
     rin.memory_limit_bytes = config.memory_limit_bytes
     rin.family_bits = config.family_bits
     rin.filter_bits = config.filter_bits
+    rin.shard_index = config.shard_index
+    rin.shard_count = config.shard_count
     capacity = max(1, config.capacity)
     for _ in range(2):
         buf = np.zeros(capacity * 3, dtype=np.uint32)

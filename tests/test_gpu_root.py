@@ -213,3 +213,43 @@ def test_large_planted_root_is_exact_and_deterministic(tg):
         vd = int(keys.lo[2][c]) | (int(keys.hi[2][c]) << 64)
         assert (va + vb - vd) % (1 << 69) == 0
     assert r1.telemetry.logical_pairs == n[0] * n[1]
+
+
+@pytest.mark.parametrize("v1", [False, True])
+@pytest.mark.parametrize("count", [2, 8, 64])
+def test_shards_union_equals_whole_root(tg, oracle_mod, golden, count, v1):
+    """The multi-GPU split run shard by shard on one device: disjoint shards
+    whose union is the whole root (and, under the 700-cell subsample, the
+    subsample), every triple in the shard its D key names."""
+    from tergpu import workload
+
+    g = golden["synthetic_roots"][0]
+    lo, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
+    sub = oracle_mod.select_cells(700)
+    trip, pairs, sub_trip = [], 0, []
+    for i in range(count):
+        res = tg.run_gpu_root(keys, tg.Config(shard_index=i, shard_count=count, sweep_v1=v1))
+        assert all(int(lo[2][c]) % count == i for _, _, c in res.triples)
+        trip.extend(map(tuple, res.triples.tolist()))
+        pairs += res.telemetry.logical_pairs
+        part = tg.run_gpu_root(keys, tg.Config(shard_index=i, shard_count=count, sweep_v1=v1),
+                               cells=sub)
+        sub_trip.extend(map(tuple, part.triples.tolist()))
+    assert len(trip) == g["brute"]["triples"]
+    assert_digest(workload.digest(trip), g["brute"])
+    assert pairs == g["arwlf"]["logical_pairs"]
+    assert_digest(workload.digest(sub_trip), g["subsample700"])
+
+
+def test_sharded_root_in_one_process_and_bad_shard_counts(tg, oracle_mod, golden):
+    from tergpu import workload
+    from tergpu.shard import run_sharded_root
+
+    g = golden["synthetic_roots"][2]
+    _, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
+    res = run_sharded_root(keys)  # a world of one: the whole root
+    assert_digest(workload.digest(res.triples), g["brute"])
+    for index, count in ((0, 3), (2, 2), (0, 128)):
+        with pytest.raises(tg.TergpuError) as e:
+            tg.run_gpu_root(keys, tg.Config(shard_index=index, shard_count=count))
+        assert e.value.status == 66  # InvalidInput
