@@ -62,7 +62,8 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="list-size multiplier (smaller runs)")
     p.add_argument("--family-bits", type=int, default=0)
     p.add_argument("--filter-bits", type=int, default=0)
-    p.add_argument("--sweep-v1", action="store_true", help="first sweep variant (A/B runs)")
+    p.add_argument("--sweep-v1", action="store_true", help="sweep variant 1 (A/B runs)")
+    p.add_argument("--sweep-v2", action="store_true", help="sweep variant 2 (A/B runs)")
     p.add_argument("--cpu-cells", type=int, default=6,
                    help="cells of the reference's declared subsample timed on one core")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -204,7 +205,8 @@ def run_tergpu(args):
         rin = _abi.RootIn()
         rin.quotient_bits = QBITS
         rin.flags = (_abi.ROOT_DEVICE_INPUTS if resident else 0) | \
-            (_abi.ROOT_SWEEP_V1 if args.sweep_v1 else 0)
+            (_abi.ROOT_SWEEP_V1 if args.sweep_v1 else 0) | \
+            (_abi.ROOT_SWEEP_V2 if args.sweep_v2 else 0)
         for l in range(3):
             rin.count[l] = sizes[l]
             if resident:

@@ -21,7 +21,9 @@
 extern "C" {
 #endif
 
-#define TERGPU_ABI_VERSION 1
+/* 2: tergpu_root_in / tergpu_root_records_in gained shard_index and shard_count;
+ * callers compiled against another version must not call in (the adapter checks). */
+#define TERGPU_ABI_VERSION 2
 
 enum tergpu_status {
   TERGPU_COMPLETED = 0,
@@ -51,9 +53,14 @@ enum tergpu_status {
 #define TERGPU_ROOT_COUNT_ONLY 1u    /* count triples, write none */
 #define TERGPU_ROOT_DEVICE_INPUTS 2u /* key_lo / key_hi / id / cells are device pointers of
                                         `device`, already resident: nothing is uploaded */
-#define TERGPU_ROOT_SWEEP_V1 4u      /* use the first sweep variant (A in registers, B
-                                        broadcast) instead of the default (B in registers,
-                                        B families sorted, A broadcast); same results */
+#define TERGPU_ROOT_SWEEP_V1 4u      /* sweep variant 1: A in registers, B broadcast */
+#define TERGPU_ROOT_SWEEP_V2 8u      /* sweep variant 2: B in registers (families sorted by
+                                        window), A broadcast.  Default (neither flag):
+                                        variant 3, variant 2 with B families laid out in
+                                        lane slots of distinct residual classes and filter
+                                        words picked by the low probe bits (bank-free
+                                        shared-memory probes; needs 32 or more residual
+                                        bits, else variant 2 runs).  Same results */
 
 /*
  * One L1 -> L0 root on full quotient keys.
@@ -211,6 +218,11 @@ typedef struct {
 /* tergpu_attempt_in.flags */
 #define TERGPU_ATTEMPT_CAPTURE_ONLY 1u /* stop after L1 (export only): the device
                                           counterpart of stream_full_ter_root_lists */
+#define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
+                                          device bytes (out->device_bytes), check them
+                                          against memory_limit_bytes and return
+                                          TERGPU_COMPLETED without device work; the
+                                          instance may be NULL (ter_full_bench --preflight) */
 
 typedef struct {
   uint32_t n;                  /* 36, 72 or 108 */

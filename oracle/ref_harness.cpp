@@ -20,10 +20,19 @@
 //   terref keysroot KEYS BACKEND CELLS REPS PROJ
 //       one backend over key lists read from KEYS (list 2 holds d), sink without
 //       authority; REPS timed repetitions.
+//   terref plant SNAP COUNT SEED
+//       the whole-root runner's positive construction
+//       (ter2_root/campaign/ter_arwlf_whole_root_main.cpp:240-247): PlantedTargets
+//       on the anchor microproblem (select_microproblems(index, 1)); prints the
+//       appended D keys and the expected final outputs.
+//   terref report SNAP POLICY
+//       report_full_ter_root (src/full_ter.cpp:3722) on the capture held by SNAP
+//       (POLICY = first | count | canon), plus count_full_ter_root (:3861).
 // BACKEND: arwlf | k2wide | k2 | hash | gpu | brute
 
 #include "ter_a64_chqr.hpp"
 #include "ter_arwlf.hpp"
+#include "ter_arwlf_campaign.hpp"
 #include "ter_gpu_root.hpp"
 #include "ter_hash_join_root.hpp"
 #include "ter_root_generalization_workload.hpp"
@@ -360,6 +369,101 @@ int cmd_keysroot(int argc, char** argv) {
   return 0;
 }
 
+int cmd_plant(int argc, char** argv) {
+  if (argc < 5) { return 2; }
+  const auto count = static_cast<std::uint32_t>(std::strtoul(argv[3], nullptr, 0));
+  const std::uint64_t seed = std::strtoull(argv[4], nullptr, 0);
+  auto workload = rg::load_snapshot_workload(argv[2], true);
+  if (workload->status != rg::WorkloadStatus::Completed || !workload->authority.ok) {
+    std::cout << "{\"error\":\"" << rg::status_label(workload->status) << "\"}\n";
+    return 1;
+  }
+  std::uint32_t anchor = 4096U;
+  {
+    rg::RootIndex probe;
+    rg::build_root_index(*workload->data, probe);
+    rg::select_microproblems(probe, 1U);
+    for (std::uint32_t cell = 0U; cell < 4096U; ++cell) {
+      anchor = probe.selected[cell] != 0U ? cell : anchor;
+    }
+  }
+  const std::size_t before = workload->key_lo[2].size();
+  const ter::arwlf_campaign::PlantedTargets planted(
+      *workload, anchor,
+      ter::arwlf_campaign::Plant{ter::arwlf_campaign::PlantKind::Positive, count, seed});
+  std::cout << "{\"anchor_cell\":" << anchor << ",\"first_planted\":" << planted.first_planted()
+            << ",\"d_lo\":[";
+  for (std::size_t i = before; i < workload->key_lo[2].size(); ++i) {
+    std::cout << (i > before ? "," : "") << "\"" << workload->key_lo[2][i] << "\"";
+  }
+  std::cout << "],\"d_hi\":[";
+  for (std::size_t i = before; i < workload->key_hi[2].size(); ++i) {
+    std::cout << (i > before ? "," : "") << static_cast<int>(workload->key_hi[2][i]);
+  }
+  std::cout << "],\"expected\":[";
+  for (std::size_t i = 0; i < planted.expected().size(); ++i) {
+    const auto& w = planted.expected()[i];
+    std::cout << (i ? "," : "") << "[" << w[0] << "," << w[1] << "," << w[2] << "]";
+  }
+  std::cout << "]}\n";
+  return 0;
+}
+
+int cmd_report(int argc, char** argv) {
+  if (argc < 4) { return 2; }
+  rs::Snapshot snap;
+  std::string error;
+  if (!rs::load(argv[2], snap, error)) {
+    std::cout << "{\"error\":\"" << error << "\"}\n";
+    return 1;
+  }
+  const std::string policy_name = argv[3];
+  const ter::RootOutputPolicy policy =
+      policy_name == "count" ? ter::RootOutputPolicy::CountOnly
+      : policy_name == "canon" ? ter::RootOutputPolicy::FullCanonicalOutput
+                               : ter::RootOutputPolicy::FirstWitness;
+  const std::uint32_t n = snap.header.n;
+  ter::FullTerRootCapture capture;
+  const auto params = ter::derive_full_ter_parameters(ter::ShapeFamily::FiniteSanity, n, n);
+  capture.status = params.status;
+  capture.parameters = params.value;
+  capture.seed = snap.header.seed;
+  capture.execution_mode = ter::TerExecutionMode::FullTer;
+  for (std::size_t l = 0; l < 3; ++l) {
+    const std::uint64_t count = snap.header.entries[l];
+    capture.children[l].resize(count);
+    capture.residues_words_le[l].resize(count);
+    for (std::uint64_t i = 0; i < count; ++i) {
+      auto& digits = capture.children[l][i];
+      digits.resize(n);
+      for (std::uint32_t c = 0; c < n; ++c) {
+        digits[c] = static_cast<std::int8_t>(snap.digit(l, i, c));
+      }
+      const auto res = snap.residue(l, i);
+      capture.residues_words_le[l][i].assign(res.begin(), res.end());
+    }
+    const auto ct = snap.child_target(l);
+    capture.child_targets_words_le[l].assign(ct.begin(), ct.end());
+  }
+  const auto rt = snap.root_target();
+  capture.root_target_words_le.assign(rt.begin(), rt.end());
+  ter::FullTerConfig config = rg::authentic_config(snap.header.seed);
+  config.memory_limit_bytes = std::uint64_t{64} << 30;
+  const auto start = Clock::now();
+  const auto report = ter::report_full_ter_root(capture, config, policy);
+  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+  const auto count = ter::count_full_ter_root(capture, config);
+  std::cout << "{\"status\":" << static_cast<int>(report.status)
+            << ",\"policy\":" << static_cast<int>(report.effective_root_output_policy)
+            << ",\"valid_root_count\":" << report.valid_root_count
+            << ",\"retained_root_count\":" << report.retained_root_count
+            << ",\"count_status\":" << static_cast<int>(count.status)
+            << ",\"count_valid_root_count\":" << count.valid_root_count
+            << ",\"modular\":" << report.telemetry.modular_candidates
+            << ",\"ms\":" << ms << ",\"message\":\"" << report.message << "\"}\n";
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -374,6 +478,8 @@ int main(int argc, char** argv) {
   else if (cmd == "snaproot") { rc = cmd_snaproot(argc, argv); }
   else if (cmd == "synth") { rc = cmd_synth(argc, argv); }
   else if (cmd == "keysroot") { rc = cmd_keysroot(argc, argv); }
+  else if (cmd == "report") { rc = cmd_report(argc, argv); }
+  else if (cmd == "plant") { rc = cmd_plant(argc, argv); }
   if (rc == 2) { std::cerr << "bad arguments for " << cmd << "\n"; }
   return rc;
 }

@@ -16,8 +16,10 @@ namespace {
 
 // The C ABI is resolved on first use, so a host without the GPU library still
 // runs every other backend.  TERGPU_LIBRARY names the shared object; otherwise
-// the dynamic linker's search path finds libtergpu.so.
+// the dynamic linker's search path finds libtergpu.so.  A library built for
+// another ABI version (a different tergpu_root_in layout) is not used.
 using RootRunFn = int (*)(const tergpu_root_in*, tergpu_root_out*);
+using AbiVersionFn = int (*)(void);
 
 RootRunFn resolve_root_run() noexcept {
   static std::once_flag once;
@@ -26,7 +28,10 @@ RootRunFn resolve_root_run() noexcept {
     const char* path = std::getenv("TERGPU_LIBRARY");
     void* handle = dlopen(path != nullptr ? path : "libtergpu.so", RTLD_NOW | RTLD_LOCAL);
     if (handle != nullptr) {
-      fn = reinterpret_cast<RootRunFn>(dlsym(handle, "tergpu_root_run"));
+      const auto version = reinterpret_cast<AbiVersionFn>(dlsym(handle, "tergpu_abi_version"));
+      if (version != nullptr && version() == TERGPU_ABI_VERSION) {
+        fn = reinterpret_cast<RootRunFn>(dlsym(handle, "tergpu_root_run"));
+      }
     }
   });
   return fn;

@@ -176,7 +176,9 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
     t_error = "full TER on the device requires n in {36, 72, 108}";
     return TERGPU_INVALID_CONFIGURATION;
   }
-  if (in->values_le == nullptr || in->target_le == nullptr || in->attempt_count == 0) {
+  const bool preflight = (in->flags & TERGPU_ATTEMPT_PREFLIGHT) != 0;
+  if (!preflight &&
+      (in->values_le == nullptr || in->target_le == nullptr || in->attempt_count == 0)) {
     t_error = "instance or attempt range missing";
     return TERGPU_INVALID_INPUT;
   }
@@ -190,9 +192,6 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
   }
   const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
   const u128 nmask = mask128(n);
-  u128 T = in->target_le[0];
-  if (w64 > 1) T |= (u128)in->target_le[1] << 64;
-  T &= nmask;
   const uint64_t l3 = binom_host(n / 2, n / 36);
   out->level3_size = l3;
 
@@ -208,6 +207,10 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
     t_error = "predicted device bytes exceed the declared ceiling";
     return TERGPU_RESOURCE_LIMIT;
   }
+  if (preflight) return TERGPU_COMPLETED;
+  u128 T = in->target_le[0];
+  if (w64 > 1) T |= (u128)in->target_le[1] << 64;
+  T &= nmask;
 
   Workspace& w = workspace(in->device);
   std::lock_guard<std::mutex> lock(w.mu);

@@ -460,6 +460,287 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
   }
 }
 
+// v3 (windows of 32 or more residual bits): the filter word of a probe is
+// picked by the LOW bits of T = ~(w_q + kappa) - w_x, so the shared-memory bank
+// of a probe is (~(w_q + kappa) - w_x) mod 32 -- borrow-free -- and lanes whose
+// B windows differ mod 32 never share a bank, whatever the A entry.
+// k_family_arrange lays every B family out so that each lane slot (32
+// consecutive entries) holds distinct classes w_x mod 32 wherever the class
+// counts allow.  Key of T: word T mod 2^wb, bit 31 - T[25, 30) of that word.
+__device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff, uint32_t ny,
+                                              uint32_t* bm, uint32_t* ywin, uint16_t* yhash,
+                                              bool yshared) {
+  const uint32_t wb = a.wb;
+  for (uint32_t i = threadIdx.x; i < (1u << wb); i += blockDim.x) bm[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < (1u << kYHashBits); i += blockDim.x) yhash[i] = 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
+    const uint32_t w = static_cast<uint32_t>(a.y.res[yoff + i]);  // mrb >= 32: the low 32 bits
+    const uint32_t T = ~w;
+    atomicOr(&bm[T & ((1u << wb) - 1u)], 1u << (31u - ((T >> 25) & 31u)));
+    if (yshared) {
+      ywin[i] = w;
+      uint32_t h = yhash_of(w);
+      while (atomicCAS(reinterpret_cast<unsigned short*>(&yhash[h]), (unsigned short)0,
+                       static_cast<unsigned short>(i + 1u)) != 0) {
+        h = (h + 1u) & ((1u << kYHashBits) - 1u);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <int R>
+__global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) {
+  static_assert(R == 4 || R == 8, "32 tests per mask");
+  constexpr int QPC = 32 / R;  // A entries per 32-test mask
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t item_counter;
+  const uint32_t nfam = 1u << a.fb;
+  const uint32_t fmask = nfam - 1u;
+  const uint32_t wb = a.wb;
+  uint32_t* bm = smem;
+  uint32_t* ywin = bm + (1u << wb);
+  uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kYCap);
+  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
+  uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweepWarps * kQueueCap);
+
+  const uint32_t nloc = nfam / a.shards;
+  const uint32_t u = a.shard + a.shards * (blockIdx.x % nloc);
+  const uint32_t part = blockIdx.x / nloc;
+  const uint32_t s_per = (nfam + a.s_split - 1u) / a.s_split;
+  const uint32_t s0 = part * s_per;
+  const uint32_t s1 = min(nfam, s0 + s_per);
+  const uint32_t ny = a.y.cnt[u];
+  if (s0 >= s1 || ny == 0u) return;  // uniform across the block
+  const uint32_t yoff = a.y.off[u];
+  const uint64_t mmask = a.mrb >= 64 ? ~0ull : ((1ull << a.mrb) - 1ull);
+  const bool yshared = ny <= kYCap;
+  if (threadIdx.x == 0) item_counter = 0u;
+  build_target3(a, yoff, ny, bm, ywin, yhash, yshared);
+
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  uint2* wq = queues + warp * kQueueCap;
+  constexpr uint32_t kChunk = 32u * R;
+  uint32_t* xs = xstage + warp * kChunk;
+  const uint32_t xc_max = static_cast<uint32_t>((a.counters[kMaxX] + kChunk - 1ull) / kChunk);
+  const uint32_t total_items = (s1 - s0) * xc_max;
+  unsigned long long c_surv = 0, c_fast = 0, c_proj = 0, c_fall = 0;
+  const uint32_t hi_mask = (1u << a.hi_bits) - 1u;
+  const uint32_t amask = ((1u << wb) - 1u) << 2;  // byte offset of word T mod 2^wb
+  const char* bmb = reinterpret_cast<const char*>(bm);
+
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total_items) break;
+    const uint32_t s = s0 + item / xc_max;
+    const uint32_t xc = item % xc_max;
+    const uint32_t t = (u - s) & fmask;
+    const uint32_t kap = s > u ? 1u : 0u;
+    if (a.cells != nullptr && a.cells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
+    const uint32_t nq = a.q.cnt[s];
+    const uint32_t nx = a.x.cnt[t];
+    const uint32_t xbase = xc * kChunk;
+    if (xbase >= nx || nq == 0u) continue;
+    const uint32_t qoff = a.q.off[s];
+    const uint32_t xoff = a.x.off[t];
+
+    uint32_t x4[R];  // 4 * w_x
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const uint32_t xi = xbase + r * 32u + lane;
+      const uint32_t wx = xi < nx ? static_cast<uint32_t>(a.x.res[xoff + xi]) : 0u;
+      x4[r] = wx << 2;
+      xs[r * 32u + lane] = wx;
+    }
+    const uint32_t cadd = 0u - 4u * kap - 4u;  // 4 * ~(w + kap) = -4 w - 4 kap - 4
+
+    uint32_t qlen = 0;
+    auto drain = [&]() {
+      __syncwarp();
+      for (uint32_t e = lane; e < qlen; e += 32u) {
+        const uint2 rec = wq[e];
+        const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
+        uint32_t mm = rec.y;
+        while (mm != 0u) {
+          const uint32_t b = __ffs(mm) - 1u;
+          mm &= mm - 1u;
+          const uint32_t k = 31u - b;
+          const uint32_t qi = j + k / R;
+          const uint32_t xi = xbase + (k % R) * 32u + ln;
+          if (qi >= nq || xi >= nx) continue;
+          ++c_surv;
+          const uint64_t rq = a.q.res[qoff + qi];
+          const uint32_t w = static_cast<uint32_t>(rq) + kap + xs[(k % R) * 32u + ln];
+          auto check = [&](uint32_t idx) {
+            const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
+            const uint64_t ms = sum & mmask;
+            if ((a.y.res[yoff + idx] & mmask) != ms) return;
+            if (a.project) {
+              ++c_proj;
+              return;
+            }
+            ++c_fast;
+            if (a.hi_bits != 0u) {
+              const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                     static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+              if (high != a.y.hi[yoff + idx]) return;
+            }
+            const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+            if (slot < a.cap) {
+              a.triples[3 * slot] = a.q.id[qoff + qi];
+              a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+              a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+            }
+          };
+          if (yshared) {
+            uint32_t h = yhash_of(w);
+            for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+              if (ywin[v - 1u] == w) check(v - 1u);
+              h = (h + 1u) & ((1u << kYHashBits) - 1u);
+            }
+          } else {
+            ++c_fall;
+            for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
+          }
+        }
+      }
+      __syncwarp();
+      qlen = 0;
+    };
+
+    const uint64_t* qr = a.q.res + qoff;
+    for (uint32_t j = 0; j < nq; j += QPC) {
+      uint32_t m = 0;
+#pragma unroll
+      for (int p = 0; p < QPC / 2; ++p) {
+        const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qr + j + 2 * p);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const uint32_t c4 = static_cast<uint32_t>(e ? qq.y : qq.x) * 0xFFFFFFFCu + cadd;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const uint32_t t4 = c4 - x4[r];
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(bmb + (t4 & amask));
+            m = __funnelshift_l(__funnelshift_l(w, w, __umulhi(t4, 32u)), m, 1);
+          }
+        }
+      }
+      if (__any_sync(kFull, m != 0u)) {
+        const bool has = m != 0u;
+        const uint32_t ball = __ballot_sync(kFull, has);
+        if (qlen + __popc(ball) > kQueueCap) drain();
+        if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
+        qlen += __popc(ball);
+      }
+    }
+    drain();
+  }
+
+  for (int d = 16; d > 0; d >>= 1) {
+    c_surv += __shfl_down_sync(kFull, c_surv, d);
+    c_fast += __shfl_down_sync(kFull, c_fast, d);
+    c_proj += __shfl_down_sync(kFull, c_proj, d);
+    c_fall += __shfl_down_sync(kFull, c_fall, d);
+  }
+  if (lane == 0) {
+    if (c_surv) atomicAdd(&a.counters[kSurvivors], c_surv);
+    if (c_fast) atomicAdd(&a.counters[kFast], c_fast);
+    if (c_proj) atomicAdd(&a.counters[kProjected], c_proj);
+    if (c_fall) atomicAdd(&a.counters[kFallback], c_fall);
+  }
+}
+
+// Lays every B family of at most kSortCap entries out in lane slots of 32
+// consecutive entries whose classes (residual mod 32, the bank selector of the
+// v3 probe) are distinct wherever the class counts allow: slot by slot, one
+// entry of every class that still has entries, then the remaining positions
+// from the classes with the most entries left (fewest repeats in the slot
+// first).  A permutation inside the family: the sweep is exact for any order,
+// the layout only decides bank conflicts.  Larger families stay as they are.
+__global__ void __launch_bounds__(256) k_family_arrange(uint64_t* __restrict__ res,
+                                                        uint8_t* __restrict__ hi,
+                                                        uint32_t* __restrict__ id,
+                                                        const uint32_t* __restrict__ off,
+                                                        const uint32_t* __restrict__ cnt) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint64_t* keys = reinterpret_cast<uint64_t*>(smem);
+  uint32_t* ids = reinterpret_cast<uint32_t*>(keys + kSortCap);
+  uint16_t* order = reinterpret_cast<uint16_t*>(ids + kSortCap);  // entries grouped by class
+  uint16_t* perm = order + kSortCap;                               // position -> entry
+  uint8_t* his = reinterpret_cast<uint8_t*>(perm + kSortCap);
+  __shared__ uint32_t cend[32], cstart[32];
+  const uint32_t f = blockIdx.x;
+  const uint32_t n = cnt[f];
+  if (n < 2u || n > kSortCap) return;  // uniform across the block
+  const uint32_t base = off[f];
+  if (threadIdx.x < 32u) cend[threadIdx.x] = 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    keys[i] = res[base + i];
+    ids[i] = id[base + i];
+    his[i] = hi[base + i];
+    atomicAdd(&cend[static_cast<uint32_t>(keys[i]) & 31u], 1u);
+  }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  if (threadIdx.x < 32u) {
+    const uint32_t c = cend[lane];
+    uint32_t incl = c;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, incl, d);
+      if (lane >= (uint32_t)d) incl += o;
+    }
+    cstart[lane] = incl - c;
+    cend[lane] = incl - c;  // cursor while grouping; the class end afterwards
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t pos = atomicAdd(&cend[static_cast<uint32_t>(keys[i]) & 31u], 1u);
+    order[pos] = static_cast<uint16_t>(i);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32u) {
+    uint32_t cur = cstart[lane];
+    uint32_t rem = cend[lane] - cstart[lane];
+    const uint32_t slots = (n + 31u) / 32u;
+    for (uint32_t j = 0; j < slots; ++j) {
+      // take <= sum of rem, and every lane with rem > 0 takes one, so at most
+      // `take` lanes take one here and the loop below always finds a lane
+      const uint32_t take = min(32u, n - 32u * j);
+      uint32_t mult = rem > 0u ? 1u : 0u;
+      uint32_t k = __popc(__ballot_sync(kFull, mult != 0u));
+      while (k < take) {
+        const uint32_t avail = rem - mult;
+        const uint32_t key = avail > 0u ? ((mult << 16) | (0xFFFFu - avail)) : 0xFFFFFFFFu;
+        const uint32_t best = __reduce_min_sync(kFull, key);
+        const uint32_t win = __ffs(__ballot_sync(kFull, key == best)) - 1u;
+        if (lane == win) ++mult;
+        ++k;
+      }
+      uint32_t incl = mult;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(kFull, incl, d);
+        if (lane >= (uint32_t)d) incl += o;
+      }
+      const uint32_t first = 32u * j + incl - mult;
+      for (uint32_t i = 0; i < mult; ++i) perm[first + i] = order[cur + i];
+      cur += mult;
+      rem -= mult;
+    }
+  }
+  __syncthreads();
+  for (uint32_t p = threadIdx.x; p < n; p += blockDim.x) {
+    const uint32_t src = perm[p];
+    res[base + p] = keys[src];
+    id[base + p] = ids[src];
+    hi[base + p] = his[src];
+  }
+}
+
 // Exclusive scan of n counters in shared memory by one CTA of 256 threads.
 __device__ void block_exclusive_scan256(uint32_t* a, uint32_t n) {
   __shared__ uint32_t warp_sums[8];
@@ -673,6 +954,20 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
     cudaFuncSetAttribute(k_sweep2<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_sweep2<false, 8><<<grid, kSweepThreads, smem, st>>>(a);
   }
+}
+
+void launch_sweep3(const SweepArgs& a, cudaStream_t st) {
+  const size_t smem = sweep_smem_bytes(a.wb) + static_cast<size_t>(kSweepWarps) * 32 * 8 * 4;
+  const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
+  cudaFuncSetAttribute(k_sweep3<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_sweep3<8><<<grid, kSweepThreads, smem, st>>>(a);
+}
+
+void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
+                           const uint32_t* cnt, uint32_t nfam, cudaStream_t st) {
+  const size_t smem = static_cast<size_t>(kSortCap) * (8 + 4 + 2 + 2 + 1);
+  cudaFuncSetAttribute(k_family_arrange, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_family_arrange<<<nfam, 256, smem, st>>>(res, hi, id, off, cnt);
 }
 
 void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,

@@ -73,6 +73,14 @@ void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st);
 // Exact for any family order; conflict-free filter probes once every B family
 // is sorted by the filter's word bits (launch_family_sort).
 void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st);
+// v3 (needs mrb >= 32): the filter word is picked by the low bits of the probe
+// value, so the bank is borrow-free; conflict-free once every B family is laid
+// out by launch_family_arrange.  Exact for any family order.
+void launch_sweep3(const SweepArgs& a, cudaStream_t st);
+// Lays every B family (of at most kSortCap entries) out in lane slots of 32
+// entries with distinct residual classes mod 32 wherever the counts allow.
+void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
+                           const uint32_t* cnt, uint32_t nfam, cudaStream_t st);
 // Sorts every family of one partitioned list (of at most kSortCap entries) by
 // the top `sb` bits of its sweep window, in place; larger families stay as they are.
 void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,

@@ -87,9 +87,10 @@ uint32_t ceil_log2(uint64_t v) {
 // rate |D_u| / 2^(wb+5) ~ 0.3 %); narrower filters make the probes of 32
 // consecutive sorted B entries nearly conflict-free but pass too many pairs.
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
-                     uint32_t fb_req, uint32_t filter_req, bool v2, uint32_t shards) {
+                     uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards) {
   Tuning t;
-  t.v2 = v2;
+  t.variant = variant == 0 ? 3u : variant;
+  const bool v2 = t.variant != 1;
   uint32_t fb_max = std::min<uint32_t>(14, fast_bits - 2);
   if (projected != 0) fb_max = std::min<uint32_t>(fb_max, projected - 6);
   if (fb_req != 0) {
@@ -128,6 +129,12 @@ uint64_t partition_bytes(const uint64_t count[3], uint32_t fb) {
   return b;
 }
 
+uint32_t sweep_variant(uint32_t flags) {
+  if ((flags & TERGPU_ROOT_SWEEP_V1) != 0) return 1;
+  if ((flags & TERGPU_ROOT_SWEEP_V2) != 0) return 2;
+  return 3;
+}
+
 uint32_t checked_shards(uint32_t index, uint32_t count) {
   const uint32_t n = count == 0 ? 1u : count;
   if (n > 64 || (n & (n - 1)) != 0 || index >= n) {
@@ -145,7 +152,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   const uint32_t F = std::min<uint32_t>(Q, 64);
   const uint32_t hi_bits = Q - F;
   r.tuning = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, in.family_bits,
-                           in.filter_bits, !in.sweep_v1, in.shards);
+                           in.filter_bits, in.sweep_variant, in.shards);
   const Tuning& tu = r.tuning;
   checked_shards(in.shard, in.shards);
   if (tu.fb < 6 || tu.fb > 16 || tu.fb + 2 > F || tu.wb < 5 || tu.wb > 15 ||
@@ -200,11 +207,27 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   launch_max_family(cnt[0], nfam, counters, kMaxQ, st);
   launch_max_family(cnt[1], nfam, counters, kMaxX, st);
   r.launches += 2;
-  if (tu.v2 && in.count[1] != 0) {
+  // v3 needs full 32-bit windows (mrb >= 32); below that the B-in-registers
+  // sweep (v2) runs, exact for any family order.
+  const uint32_t main_variant = tu.variant == 3 && F - tu.fb < 32 ? 2u : tu.variant;
+  if (main_variant == 3 && in.count[1] != 0) {
+    // B families in lane slots of distinct residual classes mod 32 (bank-free probes)
+    launch_family_arrange(res[1], hi[1], ids[1], off[1], cnt[1], nfam, st);
+    r.launches += 1;
+  } else if (main_variant == 2 && in.count[1] != 0) {
     // B families sorted by the top filter-word bits of the full-width window
     launch_family_sort(res[1], hi[1], ids[1], off[1], cnt[1], nfam, F - tu.fb, tu.sort_bits, st);
     r.launches += 1;
   }
+  auto sweep = [&](const SweepArgs& sa) {
+    if (main_variant == 3 && sa.mrb >= 32) {
+      launch_sweep3(sa, st);
+    } else if (main_variant == 1) {
+      launch_sweep(sa, sa.mrb < 32, st);
+    } else {
+      launch_sweep2(sa, sa.mrb < 32, st);
+    }
+  };
   check(cudaGetLastError(), "partition launch");
   check(cudaEventRecord(w.mid, st), "event");
   SweepArgs a{};
@@ -225,21 +248,13 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   if (!in.count_only || in.projected_bits == 0) {
     a.project = 0;
     a.mrb = F - tu.fb;
-    if (tu.v2) {
-      launch_sweep2(a, a.mrb < 32, st);
-    } else {
-      launch_sweep(a, a.mrb < 32, st);
-    }
+    sweep(a);
     r.launches += 1;
   }
   if (in.projected_bits != 0) {
     a.project = 1;
     a.mrb = in.projected_bits - tu.fb;
-    if (tu.v2) {
-      launch_sweep2(a, a.mrb < 32, st);
-    } else {
-      launch_sweep(a, a.mrb < 32, st);
-    }
+    sweep(a);
     r.launches += 1;
   }
   check(cudaGetLastError(), "sweep launch");
@@ -393,7 +408,7 @@ int root_run_body(const void* vin, void* vout) {
   j.memory_limit_bytes = in->memory_limit_bytes;
   j.capacity = count_only ? 0 : out->capacity;
   j.count_only = count_only;
-  j.sweep_v1 = (in->flags & TERGPU_ROOT_SWEEP_V1) != 0;
+  j.sweep_variant = sweep_variant(in->flags);
   j.shard = in->shard_index;
   j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);
@@ -523,7 +538,7 @@ int root_records_body(const void* vin, void* vout) {
   j.memory_limit_bytes = in->memory_limit_bytes;
   j.capacity = count_only ? 0 : out->root.capacity;
   j.count_only = count_only;
-  j.sweep_v1 = (in->flags & TERGPU_ROOT_SWEEP_V1) != 0;
+  j.sweep_variant = sweep_variant(in->flags);
   j.shard = in->shard_index;
   j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);

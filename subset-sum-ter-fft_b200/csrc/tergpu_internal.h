@@ -46,7 +46,7 @@ T* ensure(Workspace& w, int slot, size_t bytes) {
 
 struct Tuning {
   uint32_t fb = 6, wb = 12, s_split = 1, sort_bits = 0;
-  bool v2 = true;
+  uint32_t variant = 3;  // sweep: 1 (A in registers), 2 (B in registers), 3 (v2 + bank-free probes)
 };
 
 // Device-resident inputs of one join: keys per list.
@@ -63,7 +63,7 @@ struct JoinInput {
   uint64_t memory_limit_bytes;
   uint64_t capacity;
   bool count_only;
-  bool sweep_v1;
+  uint32_t sweep_variant;  // 0: default (3), else 1, 2 or 3
   uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
   cudaStream_t stream;
 };

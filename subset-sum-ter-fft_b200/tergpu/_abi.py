@@ -37,7 +37,9 @@ STATUS_NAMES = {
 
 ROOT_COUNT_ONLY = 1
 ROOT_DEVICE_INPUTS = 2
+ABI_VERSION = 2  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
 ROOT_SWEEP_V1 = 4
+ROOT_SWEEP_V2 = 8
 MAX_QUOTIENT_BITS = 72
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -119,6 +121,9 @@ def load(path: os.PathLike | str | None = None):
     lib.tergpu_root_run_noalloc.argtypes = [ctypes.POINTER(RootIn), ctypes.POINTER(RootOut)]
     lib.tergpu_root_run_noalloc.restype = ctypes.c_int
     lib.tergpu_noalloc_last_error.restype = ctypes.c_char_p
+    if lib.tergpu_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{p} implements ABI {lib.tergpu_abi_version()}, this package "
+                           f"ABI {ABI_VERSION}: rebuild it (__graft_entry__.build())")
     if path is None:
         _lib = lib
     return lib

@@ -47,7 +47,8 @@ class Config:
     filter_bits: int = 0
     count_only: bool = False
     capacity: int = 1 << 16
-    sweep_v1: bool = False
+    sweep_v1: bool = False  # sweep variant 1 (A in registers)
+    sweep_v2: bool = False  # sweep variant 2 (B in registers, windows sorted); default: variant 3
     shard_index: int = 0
     shard_count: int = 1  # power of two <= 64: join only D entries with key_d == index (mod count)
 
@@ -114,7 +115,8 @@ def run_gpu_root(keys: RootKeys, config: Config | None = None,
     rin = _abi.RootIn()
     rin.quotient_bits = keys.quotient_bits
     rin.flags = (_abi.ROOT_COUNT_ONLY if config.count_only else 0) | \
-        (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0)
+        (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
+        (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0)
     for l in range(3):
         rin.count[l] = len(lo[l])
         rin.key_lo[l] = _p(lo[l], ctypes.c_uint64)
@@ -155,7 +157,8 @@ def run_gpu_root_records(snap, config: Config | None = None,
     rin.n = snap.n
     rin.r1 = snap.r1
     rin.flags = (_abi.ROOT_COUNT_ONLY if config.count_only else 0) | \
-        (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0)
+        (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
+        (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0)
     rin.record_bytes = snap.record_bytes
     recs = [np.ascontiguousarray(r, dtype=np.uint8) for r in snap.records]
     targets = [np.ascontiguousarray(t, dtype=np.uint32) for t in snap.child_targets]

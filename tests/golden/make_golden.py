@@ -79,19 +79,77 @@ def n36_snapshot(tmp: Path):
             "file_bytes": cap["file_bytes"]}
 
 
+def root_reports(tmp: Path):
+    """report_full_ter_root / count_full_ter_root on captured roots, per policy."""
+    sys.path.insert(0, str(HERE.parent.parent / "subset-sum-ter-fft_b200"))
+    import numpy as np
+
+    from tergpu import snapshot
+
+    out = []
+    sources = [("n36_anchor_a0", HERE / "n36_anchor_a0.snap", 36, ANCHOR_SEED, 0, None)]
+    for n, seed, attempt in ((36, 358, 0), (72, ANCHOR_SEED, 0), (72, 0x7201, 21)):
+        snap = tmp / f"r{n}_{seed:x}_{attempt}.snap"
+        O.ref_run("capture", n, seed, attempt, "auth", snap)
+        sources.append((f"n{n}_{seed:x}_{attempt}", snap, n, seed, attempt, None))
+    # the positive n=72 root with the witness's list-0 record appended once more:
+    # two accepted triples, one distinct parent (pre-dedup count vs retained roots)
+    s = snapshot.load(tmp / "r72_7201_21.snap")
+    rec = s.records[0].reshape(-1, s.record_bytes)
+    s.records[0] = np.concatenate([rec, rec[2877:2878]]).reshape(-1)
+    snapshot.save(s, tmp / "r72_7201_21_dup.snap", git_commit="reference")
+    sources.append(("n72_7201_21_dup0_2877", tmp / "r72_7201_21_dup.snap", 72, 0x7201, 21,
+                    {"list": 0, "record": 2877}))
+    for name, path, n, seed, attempt, dup in sources:
+        row = {"name": name, "n": n, "seed": seed, "attempt": attempt, "duplicate": dup}
+        for policy in ("first", "count", "canon"):
+            r = O.ref_run("report", path, policy)[0]
+            row[policy] = {k: r[k] for k in ("status", "valid_root_count", "retained_root_count",
+                                             "count_valid_root_count")}
+        out.append(row)
+    return out
+
+
+def whole_root_plants(tmp: Path):
+    """The whole-root runner's positive construction (one planted final output,
+    seed 0xB1A57001, on the anchor microproblem) on authentic roots: the planted
+    D keys and the expected outputs, as the reference computes them.  The n=108
+    root is the published 0x1001 attempt-0 capture (about 150 s to capture)."""
+    out = []
+    for n, seed in ((72, ANCHOR_SEED), (108, 0x1001)):
+        snap = tmp / f"w{n}_{seed:x}.snap"
+        O.ref_run("capture", n, seed, 0, "auth", snap, timeout=1800)
+        p = O.ref_run("plant", snap, 1, 0xB1A57001, timeout=1800)[0]
+        out.append({"n": n, "seed": seed, "attempt": 0, "plant_seed": 0xB1A57001,
+                    "anchor_cell": p["anchor_cell"], "first_planted": p["first_planted"],
+                    "d_lo": [int(v) for v in p["d_lo"]], "d_hi": p["d_hi"],
+                    "expected": p["expected"]})
+    return out
+
+
+SECTIONS = {
+    "n36_attempts": lambda tmp: n36_attempts(),
+    "n36_snapshot": n36_snapshot,
+    "synthetic_roots": synthetic_roots,
+    "n72_roots": n72_roots,
+    "root_reports": root_reports,
+    "whole_root_plants": whole_root_plants,
+}
+
+
 def main():
+    """python tests/golden/make_golden.py [SECTION ...]: regenerates the named
+    sections (all when none is named) and keeps the others as they are."""
     if not O.ref_available():
         raise SystemExit("oracle/_ref/terref missing: build it where the reference sources exist")
+    wanted = sys.argv[1:] or list(SECTIONS)
+    target = HERE / "reference_golden.json"
+    golden = json.loads(target.read_text()) if target.exists() else {}
     with tempfile.TemporaryDirectory() as d:
-        tmp = Path(d)
-        golden = {
-            "n36_attempts": n36_attempts(),
-            "n36_snapshot": n36_snapshot(tmp),
-            "synthetic_roots": synthetic_roots(tmp),
-            "n72_roots": n72_roots(tmp),
-        }
-    (HERE / "reference_golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True) + "\n")
-    print("wrote", HERE / "reference_golden.json")
+        for name in wanted:
+            golden[name] = SECTIONS[name](Path(d))
+    target.write_text(json.dumps(golden, indent=1, sort_keys=True) + "\n")
+    print("wrote", target, "sections", wanted)
 
 
 if __name__ == "__main__":

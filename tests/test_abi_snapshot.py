@@ -19,7 +19,8 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(_abi.EXPORTED) <= declared
-    assert lib.tergpu_abi_version() == 1
+    version = re.search(r"#define TERGPU_ABI_VERSION (\d+)", header).group(1)
+    assert lib.tergpu_abi_version() == int(version)
 
 
 def test_fnv1a_known_answers():

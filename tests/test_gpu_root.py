@@ -28,44 +28,49 @@ def keys_of(oracle_mod, bits, seed, size, pool):
     return lo, hi, tergpu.RootKeys(quotient_bits=bits, lo=lo, hi=[h.astype(np.uint8) for h in hi])
 
 
+def vcfg(variant):
+    """Config keywords selecting sweep variant 1, 2 or 3 (the default)."""
+    return {"sweep_v1": variant == 1, "sweep_v2": variant == 2}
+
+
 def assert_digest(got, expected):
     for k in DIGEST_KEYS:
         assert got[k] == hexint(expected[k]), (k, got[k], expected[k])
 
 
-@pytest.mark.parametrize("v1", [False, True])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("case", range(6))
-def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case, v1):
+def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case, variant):
     from tergpu import workload
 
     g = golden["synthetic_roots"][case]
     lo, hi, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
-    res = tg.run_gpu_root(keys, tg.Config(projected_bits=g["arwlf"]["projected_bits"], sweep_v1=v1))
+    res = tg.run_gpu_root(keys, tg.Config(projected_bits=g["arwlf"]["projected_bits"], **vcfg(variant)))
     assert_digest(workload.digest(res.triples), g["brute"])
     assert res.telemetry.logical_pairs == g["arwlf"]["logical_pairs"]
     assert res.telemetry.projected_hits == g["arwlf"]["projected_hits"]
     assert res.telemetry.full_hits == g["brute"]["triples"]
     # the reference's declared 700-cell subsample
-    sub = tg.run_gpu_root(keys, tg.Config(sweep_v1=v1), cells=oracle_mod.select_cells(700))
+    sub = tg.run_gpu_root(keys, tg.Config(**vcfg(variant)), cells=oracle_mod.select_cells(700))
     assert_digest(workload.digest(sub.triples), g["subsample700"])
     assert sub.telemetry.logical_pairs == g["subsample700"]["logical_pairs"]
 
 
-@pytest.mark.parametrize("v1", [False, True])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("fb,filt", [(6, 10), (6, 19), (7, 12), (8, 15), (9, 20), (10, 11)])
-def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt, v1):
+def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt, variant):
     from tergpu import workload
 
     g = golden["synthetic_roots"][0]
     _, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
-    res = tg.run_gpu_root(keys, tg.Config(family_bits=fb, filter_bits=filt, sweep_v1=v1))
+    res = tg.run_gpu_root(keys, tg.Config(family_bits=fb, filter_bits=filt, **vcfg(variant)))
     assert res.telemetry.family_bits == fb and res.telemetry.filter_bits == filt
     assert_digest(workload.digest(res.triples), g["brute"])
 
 
-@pytest.mark.parametrize("v1", [False, True])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("bits", [24, 33, 40, 47, 58, 64, 65, 69, 72])
-def test_widths_against_oracle(tg, oracle_mod, bits, v1):
+def test_widths_against_oracle(tg, oracle_mod, bits, variant):
     """Every key width from the n=36 root (24) to the one-byte high limit (72),
     with the carry, multiplicity and high-bit plants; projected counts at two k."""
     from tergpu import workload
@@ -73,7 +78,7 @@ def test_widths_against_oracle(tg, oracle_mod, bits, v1):
     lo, hi, keys = keys_of(oracle_mod, bits, 0xABC0 + bits, 3000, 0)
     expected, _ = oracle_mod.root_join(bits, lo, hi)
     k = min(bits, 64) - 3
-    res = tg.run_gpu_root(keys, tg.Config(projected_bits=k, sweep_v1=v1))
+    res = tg.run_gpu_root(keys, tg.Config(projected_bits=k, **vcfg(variant)))
     got = workload.digest(res.triples)
     for key in DIGEST_KEYS:
         assert got[key] == expected[key], key
@@ -202,8 +207,9 @@ def test_large_planted_root_is_exact_and_deterministic(tg):
                                    seed=0xBEEF, planted=64)
     r1 = tg.run_gpu_root(keys)
     r2 = tg.run_gpu_root(keys, tg.Config(family_bits=9, filter_bits=17, sweep_v1=True))
+    r3 = tg.run_gpu_root(keys, tg.Config(family_bits=11, filter_bits=18, sweep_v2=True))
     t1 = sorted(map(tuple, r1.triples.tolist()))
-    assert t1 == sorted(map(tuple, r2.triples.tolist()))
+    assert t1 == sorted(map(tuple, r2.triples.tolist())) == sorted(map(tuple, r3.triples.tolist()))
     n = [len(x) for x in keys.lo]
     planted = {(n[0] - 1 - i, n[1] - 1 - i, n[2] - 1 - i) for i in range(64)}
     assert planted <= set(t1)
@@ -215,9 +221,9 @@ def test_large_planted_root_is_exact_and_deterministic(tg):
     assert r1.telemetry.logical_pairs == n[0] * n[1]
 
 
-@pytest.mark.parametrize("v1", [False, True])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("count", [2, 8, 64])
-def test_shards_union_equals_whole_root(tg, oracle_mod, golden, count, v1):
+def test_shards_union_equals_whole_root(tg, oracle_mod, golden, count, variant):
     """The multi-GPU split run shard by shard on one device: disjoint shards
     whose union is the whole root (and, under the 700-cell subsample, the
     subsample), every triple in the shard its D key names."""
@@ -228,11 +234,11 @@ def test_shards_union_equals_whole_root(tg, oracle_mod, golden, count, v1):
     sub = oracle_mod.select_cells(700)
     trip, pairs, sub_trip = [], 0, []
     for i in range(count):
-        res = tg.run_gpu_root(keys, tg.Config(shard_index=i, shard_count=count, sweep_v1=v1))
+        res = tg.run_gpu_root(keys, tg.Config(shard_index=i, shard_count=count, **vcfg(variant)))
         assert all(int(lo[2][c]) % count == i for _, _, c in res.triples)
         trip.extend(map(tuple, res.triples.tolist()))
         pairs += res.telemetry.logical_pairs
-        part = tg.run_gpu_root(keys, tg.Config(shard_index=i, shard_count=count, sweep_v1=v1),
+        part = tg.run_gpu_root(keys, tg.Config(shard_index=i, shard_count=count, **vcfg(variant)),
                                cells=sub)
         sub_trip.extend(map(tuple, part.triples.tolist()))
     assert len(trip) == g["brute"]["triples"]
