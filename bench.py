@@ -48,8 +48,12 @@ UNIT = "pairs/s"
 SIZES = (3_650_689, 6_900_048, 6_896_564)
 QBITS = 69
 PLANTED = 8
-# per logical pair the sweep issues: IADD, SHF, LDS, 2x SHF.funnel
+# per logical pair the sweep issues at least: IADD, LOP (word offset), LDS, 2x SHF.funnel
 OPS_PER_PAIR = 5
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one default-variant sweep
+# launch on the default workload (the whole authentic n=108 root of seed 0x1001), from one
+# ncu capture of that launch; other workloads and variants report null
+SWEEP_DRAM_BYTES = {"k_sweep3": 2.29e9 + 240.75e6}
 
 
 def parse():
@@ -68,6 +72,18 @@ def parse():
                    help="cells of the reference's declared subsample timed on one core")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--batch", action="store_true",
+                   help="batched attempts (256 instances, n from {36,48,60,72}, 1-16 attempts): "
+                        "solves/s batched vs one at a time")
+    p.add_argument("--serve", action="store_true",
+                   help="served solve stream: Poisson arrivals, continuous batching, p50/p99")
+    p.add_argument("--requests", type=int, default=256, help="--batch / --serve request count")
+    p.add_argument("--slots", type=int, default=16, help="--batch / --serve concurrent pipelines")
+    p.add_argument("--rate", type=float, default=40.0, help="--serve arrivals per second")
+    p.add_argument("--serve-n", default="36,48,60,72,84,96",
+                   help="--serve dimensions (108 makes one attempt ~9 s; add it explicitly)")
+    p.add_argument("--max-attempts", type=int, default=0,
+                   help="attempt budgets uniform in [1, max]: 16 for --batch, 64 for --serve")
     p.add_argument("--shard-root", action="store_true",
                    help="N>1: split one root over the ranks (strong scaling) instead of replicas")
     p.add_argument("--synthetic", action="store_true",
@@ -335,6 +351,7 @@ def run_tergpu(args):
         sm_mhz = clk.get("sm_mhz") or 1965.0
         # algorithmic HBM bytes of one sweep launch: each partitioned list read once (8 B keys)
         sweep_bytes = sum(sizes) * 8
+        sweep_kernel = "k_sweep" if args.sweep_v1 else ("k_sweep2" if args.sweep_v2 else "k_sweep3")
         part_bytes = sum(sizes) * (2 * 9 + 8 + 13 + 4)  # hist read, scatter read + write
         issue_peak = 148 * 4 * 32 * sm_mhz * 1e6 / OPS_PER_PAIR
         result = {
@@ -355,12 +372,15 @@ def run_tergpu(args):
                        "filter_survivors": survivors, "full_q_triples": triples,
                        "parallelism": (f"shards{shard_count}-over-{world}" if sharded
                                        else f"replicas{world}")},
-            "roofline": {"bound": "hbm", "kernel": "k_sweep",
+            "roofline": {"bound": "hbm", "kernel": sweep_kernel,
                          "achieved": sweep_bytes / (sweep_ms / 1000.0) / 1e9, "peak": hbm,
                          "unit": "GB/s", "frac": sweep_bytes / (sweep_ms / 1000.0) / 1e9 / hbm,
-                         "peak_source": peak_src, "traffic": None,
-                         "note": "the sweep is issue-bound, not HBM-bound: see issue_roofline"},
-            "issue_roofline": {"bound": "int32-issue", "kernel": "k_sweep", "unit": "pairs/s",
+                         "peak_source": peak_src,
+                         "traffic": (SWEEP_DRAM_BYTES.get(sweep_kernel)
+                                     if not args.synthetic and args.seed == 0x1001 else None),
+                         "note": "the sweep is bound on chip (issue, shared-memory probes), not by "
+                                 "HBM: see issue_roofline"},
+            "issue_roofline": {"bound": "int32-issue", "kernel": sweep_kernel, "unit": "pairs/s",
                                "achieved": local_pairs / (sweep_ms / 1000.0), "peak": issue_peak,
                                "frac": local_pairs / (sweep_ms / 1000.0) / issue_peak,
                                "ops_per_pair": OPS_PER_PAIR, "sm_mhz": sm_mhz},
@@ -481,10 +501,89 @@ def run_reference(args):
     print(json.dumps(base), flush=True)
 
 
+def solve_requests(args, serve: bool):
+    """Seeded request mix of the batch (config 4) or served (config 5) workload."""
+    from tergpu import attempt, batch, instance
+
+    rng = np.random.default_rng(args.seed)
+    ns = [36, 48, 60, 72] if not serve else [int(v) for v in args.serve_n.split(",")]
+    max_att = args.max_attempts or (64 if serve else 16)
+    reqs, t = [], 0.0
+    for _ in range(args.requests):
+        n = int(rng.choice(ns))
+        seed = int(rng.integers(1, 1 << 62))
+        if serve:
+            t += float(rng.exponential(1000.0 / args.rate))
+        reqs.append(batch.Request(instance.build_instance(n, seed),
+                                  attempt.FullTerConfig(seed=seed,
+                                                        attempt_limit=int(rng.integers(1, max_att + 1))),
+                                  arrival_ms=t))
+    return reqs
+
+
+def run_batch_modes(args):
+    """--batch / --serve: the same requests one at a time (one pipeline, in
+    order) and through the continuous-batching engine; every result must be
+    bit-identical between the two; prints one JSON line."""
+    import torch
+
+    from tergpu import batch
+
+    torch.cuda.set_device(0)
+    serve = args.serve
+    reqs = solve_requests(args, serve)
+    # warm both paths (workspaces, module load)
+    batch.solve_batch(reqs[:4], slots=2)
+    one = batch.solve_batch(reqs, slots=1, served=serve)
+    many = batch.solve_batch(reqs, slots=args.slots, served=serve)
+    for i, (a, b) in enumerate(zip(one.results, many.results)):
+        if not batch.same_result(a, b):
+            print(f"request {i} (n={reqs[i].instance.n}, seed={reqs[i].config.seed:#x}, "
+                  f"budget {reqs[i].config.attempt_limit}): one at a time {a.status_name} "
+                  f"{[t['level1'] for t in a.attempts][:3]}, batched {b.status_name} "
+                  f"{[t['level1'] for t in b.attempts][:3]}", file=sys.stderr)
+            raise RuntimeError("a request's result differs between one-at-a-time and batched runs")
+    statuses = [r.status for r in many.results]
+    found = [i for i, s in enumerate(statuses) if s == 1]
+    admitted = [i for i, s in enumerate(statuses) if s in (1, 3)]
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if len(v) else None
+
+    def summary(res):
+        lat = res.latency_ms
+        return {"solves_per_s": len(reqs) / (res.total_ms / 1000.0),
+                "admitted_solves_per_s": len(admitted) / (res.total_ms / 1000.0),
+                "wall_ms": res.total_ms, "peak_running": res.peak_running,
+                "latency_p50_ms": pct(lat[admitted], 50), "latency_p99_ms": pct(lat[admitted], 99),
+                "time_to_found_p50_ms": pct(lat[found], 50),
+                "time_to_found_p99_ms": pct(lat[found], 99)}
+
+    s1, sb = summary(one), summary(many)
+    attempts = sum(len(r.attempts) for r in many.results)
+    line = {
+        "metric": "served solves/s" if serve else "batched solves/s",
+        "value": sb["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
+        "n_gpus": 1, "impl": "tergpu",
+        "vs_one_at_a_time": sb["solves_per_s"] / s1["solves_per_s"],
+        "config": {"workload": ("served stream" if serve else "batched attempts"),
+                   "requests": len(reqs), "slots": args.slots, "seed": args.seed,
+                   "n": sorted({r.instance.n for r in reqs}),
+                   "max_attempts": args.max_attempts or (64 if serve else 16),
+                   "arrival_rate_per_s": args.rate if serve else None,
+                   "refused": many.refused, "found": len(found), "attempts_run": attempts,
+                   "identical_results": True},
+        "batched": sb, "one_at_a_time": s1,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.batch or args.serve:
+        run_batch_modes(args)
     else:
         run_tergpu(args)
 

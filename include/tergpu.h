@@ -54,6 +54,11 @@ enum tergpu_status {
 #define TERGPU_ROOT_DEVICE_INPUTS 2u /* key_lo / key_hi / id / cells are device pointers of
                                         `device`, already resident: nothing is uploaded */
 #define TERGPU_ROOT_SWEEP_V1 4u      /* sweep variant 1: A in registers, B broadcast */
+#define TERGPU_ROOT_AUTOTUNE 16u     /* family bits, filter bits and sweep variant picked per root
+                                        shape by timing the neighbours of the size-based choice
+                                        on 1/64 of the target families (cached per shape for the
+                                        process; ignored when family_bits, filter_bits or a
+                                        variant flag is given); same results */
 #define TERGPU_ROOT_SWEEP_V2 8u      /* sweep variant 2: B in registers (families sorted by
                                         window), A broadcast.  Default (neither flag):
                                         variant 3, variant 2 with B families laid out in
@@ -118,6 +123,8 @@ typedef struct {
   uint32_t family_bits;     /* tuning the call ran with */
   uint32_t filter_bits;
   uint32_t kernel_launches; /* device kernels this call launched */
+  uint32_t sweep_variant;   /* sweep variant the join ran (1, 2 or 3) */
+  double tune_ms;           /* device time the autotuner spent (0: no tuning or cached shape) */
 } tergpu_root_out;
 
 /* Replaces: run_hash_join / run_arwlf / run_k2_wide bodies
@@ -250,13 +257,57 @@ typedef struct {
   uint64_t l1_capacity[3];
   uint32_t child_targets[3][4];/* the last attempt's L1 targets (words32) */
   uint32_t root_target[4];
-  uint64_t device_bytes;
+  uint64_t device_bytes;        /* predicted device bytes (the preflight's admission figure) */
   double total_ms;
+  uint64_t device_bytes_held;   /* device bytes the call's workspace held at its end (its peak:
+                                   buffers only grow within a call; the shared workspace keeps
+                                   buffers of earlier calls, a batch request starts empty) */
 } tergpu_attempt_out;
 
 /* Replaces: solve_full_ter's attempt loop (src/full_ter.cpp:3125-3515) and
  * stream_full_ter_root_lists (src/full_ter.cpp:3926-4195) for the L1 export. */
 int tergpu_attempt_run(const tergpu_attempt_in *in, tergpu_attempt_out *out);
+
+/*
+ * Many independent attempt ranges on one device at once: the batched and served
+ * paths (continuous batching).  No counterpart in the reference, whose solver
+ * runs one attempt at a time on one thread.
+ *
+ * Request i is jobs[i] (its device field is ignored: the batch's device is used)
+ * and its result outs[i], exactly what tergpu_attempt_run(&jobs[i], &outs[i])
+ * returns when called alone; outs[i].status carries the status.  `slots`
+ * attempt pipelines run concurrently, each a host thread with its own CUDA
+ * stream and device workspace.  A request becomes eligible at arrival_ms[i]
+ * after the call starts (NULL: all at once); eligible requests are admitted in
+ * arrival order while a slot is free and the predicted device bytes of the
+ * running requests (each request's preflight) stay within memory_budget_bytes;
+ * a request that does not fit yet waits and later requests that fit go ahead.
+ * Requests the preflight refuses (InvalidConfiguration; ResourceLimit against
+ * their own ceiling or above the whole budget) complete immediately with that
+ * status, before any device work.  admit_ms / finish_ms (optional) receive each
+ * request's start on a slot and completion, in ms after the call started.
+ * Returns TERGPU_COMPLETED when every request has a result.
+ */
+typedef struct {
+  const tergpu_attempt_in *jobs;
+  tergpu_attempt_out *outs;     /* outs[i].stats / l1_records as in tergpu_attempt_run */
+  uint64_t count;
+  const double *arrival_ms;     /* may be NULL */
+  uint32_t slots;               /* concurrent attempt pipelines; 0: 8 */
+  int32_t device;
+  uint64_t memory_budget_bytes; /* 0: 90% of the device's free memory at the start */
+  double *admit_ms;             /* may be NULL */
+  double *finish_ms;            /* may be NULL */
+} tergpu_batch_in;
+
+typedef struct {
+  double total_ms;              /* wall time from the start to the last result */
+  uint64_t peak_predicted_bytes;/* largest predicted bytes of the requests running at once */
+  uint32_t peak_running;        /* most requests running at once */
+  uint64_t refused;             /* requests completed at admission by the preflight */
+} tergpu_batch_out;
+
+int tergpu_attempt_batch(const tergpu_batch_in *in, tergpu_batch_out *out);
 
 /*
  * The root join for callers that cannot allocate device memory.  This entry

@@ -132,9 +132,9 @@ ConstEntryArrays as_const(const EntryArrays& e) {
 }
 
 template <typename T>
-void download(T* dst, const T* src, size_t n, cudaStream_t st) {
+void download(Workspace& w, T* dst, const T* src, size_t n, cudaStream_t st) {
   check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, st), "download");
-  check(cudaStreamSynchronize(st), "sync");
+  sync_stream(w, st, "sync");
 }
 
 // Canonical order of `count` entries in `raw`: radix sort + unique into `dst`.
@@ -145,7 +145,7 @@ uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, int 
   if (count == 0) return 0;
   launch_or_reduce(as_const(raw), count, acc, st);
   unsigned long long vary[2];
-  download(vary, acc, 2, st);
+  download(w, vary, acc, 2, st);
   uint32_t* scratch = ensure<uint32_t>(w, S_SORT, radix_scratch_words(count) * 4);
   uint32_t* perm = ensure<uint32_t>(w, S_PERM, (count + 16) * 4);
   radix_sort_entries(as_const(raw), count, vary[0], vary[1], perm, scratch, st);
@@ -154,7 +154,7 @@ uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, int 
   uint32_t* scan2 = ensure<uint32_t>(w, S_SCAN2, (count / 2048 + 64) * 4);
   launch_gather_unique(as_const(raw), perm, count, *dst, flags, starts, scan2, acc + 2, st);
   unsigned long long kept = 0;
-  download(&kept, acc + 2, 1, st);
+  download(w, &kept, acc + 2, 1, st);
   return kept;
 }
 
@@ -169,7 +169,11 @@ double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
 }
 
-int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
+}  // namespace
+
+// One attempt range on `own` (a private workspace of the batch engine) or, when
+// null, on the device's shared workspace.
+int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace* own) {
   const auto t_call = std::chrono::steady_clock::now();
   const uint32_t n = in->n;
   if (n == 0 || n % 36 != 0 || n > 108) {
@@ -212,10 +216,21 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
   if (w64 > 1) T |= (u128)in->target_le[1] << 64;
   T &= nmask;
 
-  Workspace& w = workspace(in->device);
+  Workspace& w = own != nullptr ? *own : workspace(in->device);
   std::lock_guard<std::mutex> lock(w.mu);
+  // on every exit: the bytes the workspace holds (grow-only within the call)
+  struct Held {
+    Workspace& w;
+    tergpu_attempt_out* o;
+    ~Held() {
+      uint64_t bytes = 0;
+      for (const auto& kv : w.buf) bytes += kv.second.bytes;
+      o->device_bytes_held = bytes;
+    }
+  } held{w, out};
   check(cudaSetDevice(w.device), "cudaSetDevice");
   cudaStream_t st = w.stream;
+  w.alloc_stream = st;
 
   // ---- level 3 (once per call): both halves, lexicographic k-subsets
   std::vector<uint64_t> weights(2 * n, 0);
@@ -258,7 +273,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
       launch_l2_count(as_const(left), l3, boff, r2, t, counts, st);
       launch_scan_u32(counts, l3, starts, scan, st);
       uint32_t total = 0;
-      download(&total, starts + l3, 1, st);
+      download(w, &total, starts + l3, 1, st);
       EntryArrays raw = entry_slot(w, S_L2RAW, total);
       launch_l2_fill(as_const(left), l3, as_const(right), boff, order, r2, t, n, starts, raw, st);
       l2n[i] = canonicalize(w, raw, total, S_L2 + 4 * i, &l2[i], st);
@@ -317,7 +332,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
       launch_l1_parents(jr.d_triples, jr.triples, as_const(l2[3 * g]), as_const(l2[3 * g + 1]),
                         as_const(l2[3 * g + 2]), n, n / 6, cand, acc + 4, st);
       unsigned long long ncand = 0;
-      download(&ncand, acc + 4, 1, st);
+      download(w, &ncand, acc + 4, 1, st);
       l1n[g] = canonicalize(w, cand, ncand, S_L1 + 4 * g, &l1[g], st);
       stat.level1_sizes[g] = l1n[g];
     }
@@ -342,7 +357,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
         out->l1_capacity[l] = l1n[l];
       }
       for (uint32_t q = 0; q < 4; ++q) out->root_target[q] = q < w32 ? (uint32_t)(T >> (32 * q)) : 0u;
-      check(cudaStreamSynchronize(st), "export");
+      sync_stream(w, st, "export");
     };
     if (in->flags & TERGPU_ATTEMPT_CAPTURE_ONLY) {
       stat.status = TERGPU_NO_WITNESS_THIS_ATTEMPT;
@@ -417,7 +432,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
       hflags.resize(jr.triples);
       check(cudaMemcpyAsync(htrip.data(), jr.d_triples, jr.triples * 12, cudaMemcpyDeviceToHost, st), "d2h");
       check(cudaMemcpyAsync(hflags.data(), dflags, jr.triples, cudaMemcpyDeviceToHost, st), "d2h");
-      check(cudaStreamSynchronize(st), "sync");
+      sync_stream(w, st, "sync");
     }
     // valid roots: parents of the flagged triples, canonical (sorted, unique)
     std::vector<std::array<uint64_t, 2>> parents;
@@ -473,7 +488,6 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
   return status;
 }
 
-}  // namespace
 }  // namespace tergpu
 
 extern "C" int tergpu_attempt_run(const tergpu_attempt_in* in, tergpu_attempt_out* out) {
@@ -484,7 +498,7 @@ extern "C" int tergpu_attempt_run(const tergpu_attempt_in* in, tergpu_attempt_ou
     return TERGPU_INVALID_INPUT;
   }
   try {
-    const int st = attempt_body(in, out);
+    const int st = attempt_body(in, out, nullptr);
     out->status = st;
     return st;
   } catch (const Failure& f) {

@@ -14,6 +14,10 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 namespace tergpu {
 
 namespace {
@@ -896,6 +900,26 @@ __global__ void k_authority(const AuthorityArgs a) {
   if (c_rule) atomicAdd(&a.counters[2], c_rule);
 }
 
+// Allows a kernel the device's whole opt-in shared memory, once per device and
+// kernel.  Setting the attribute per launch to that launch's size would race when
+// several host threads launch the same kernel with different sizes (the batch
+// engine's slots): one thread could lower the limit between another's set and
+// launch.
+void allow_max_smem(const void* kernel) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done.insert({dev, kernel}).second) return;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, kernel);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       optin - static_cast<int>(fa.sharedSizeBytes));
+}
+
 int grid_for(uint64_t n, int threads) {
   uint64_t blocks = (n + threads - 1) / threads;
   if (blocks > 148ull * 16ull) blocks = 148ull * 16ull;
@@ -936,10 +960,10 @@ void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st) {
   const size_t smem = sweep_smem_bytes(a.wb);
   const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
   if (aligned) {
-    cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_smem(reinterpret_cast<const void*>(k_sweep<true>));
     k_sweep<true><<<grid, kSweepThreads, smem, st>>>(a);
   } else {
-    cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_smem(reinterpret_cast<const void*>(k_sweep<false>));
     k_sweep<false><<<grid, kSweepThreads, smem, st>>>(a);
   }
 }
@@ -948,10 +972,10 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
   const size_t smem = sweep_smem_bytes(a.wb) + static_cast<size_t>(kSweepWarps) * 32 * 8 * 4;
   const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
   if (aligned) {
-    cudaFuncSetAttribute(k_sweep2<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_smem(reinterpret_cast<const void*>(k_sweep2<true, 8>));
     k_sweep2<true, 8><<<grid, kSweepThreads, smem, st>>>(a);
   } else {
-    cudaFuncSetAttribute(k_sweep2<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_smem(reinterpret_cast<const void*>(k_sweep2<false, 8>));
     k_sweep2<false, 8><<<grid, kSweepThreads, smem, st>>>(a);
   }
 }
@@ -959,14 +983,14 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
 void launch_sweep3(const SweepArgs& a, cudaStream_t st) {
   const size_t smem = sweep_smem_bytes(a.wb) + static_cast<size_t>(kSweepWarps) * 32 * 8 * 4;
   const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
-  cudaFuncSetAttribute(k_sweep3<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep3<8>));
   k_sweep3<8><<<grid, kSweepThreads, smem, st>>>(a);
 }
 
 void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
                            const uint32_t* cnt, uint32_t nfam, cudaStream_t st) {
   const size_t smem = static_cast<size_t>(kSortCap) * (8 + 4 + 2 + 2 + 1);
-  cudaFuncSetAttribute(k_family_arrange, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  allow_max_smem(reinterpret_cast<const void*>(k_family_arrange));
   k_family_arrange<<<nfam, 256, smem, st>>>(res, hi, id, off, cnt);
 }
 
@@ -975,10 +999,10 @@ void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t
                         cudaStream_t st) {
   const size_t smem = static_cast<size_t>(kSortCap) * (8 + 4 + 1) + (static_cast<size_t>(4) << sb) + 16;
   if (mrb < 32) {
-    cudaFuncSetAttribute(k_family_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_smem(reinterpret_cast<const void*>(k_family_sort<true>));
     k_family_sort<true><<<nfam, 256, smem, st>>>(res, hi, id, off, cnt, mrb, sb);
   } else {
-    cudaFuncSetAttribute(k_family_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_smem(reinterpret_cast<const void*>(k_family_sort<false>));
     k_family_sort<false><<<nfam, 256, smem, st>>>(res, hi, id, off, cnt, mrb, sb);
   }
 }

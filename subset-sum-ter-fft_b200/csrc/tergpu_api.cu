@@ -16,8 +16,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -51,25 +53,70 @@ Workspace& workspace(int device) {
     t_error = "no CUDA device " + std::to_string(device);
     throw Failure{TERGPU_DEVICE_ERROR};
   }
+  g_ws.push_back(make_workspace(device));
+  return *g_ws.back();
+}
+
+std::unique_ptr<Workspace> make_workspace(int device, bool blocking) {
   auto w = std::make_unique<Workspace>();
   w->device = device;
   check(cudaSetDevice(device), "cudaSetDevice");
+  // keep freed stream-ordered memory in the device pool instead of returning it
+  // at every synchronization (workspaces grow and shrink across calls)
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreate(&w->start), "cudaEventCreate");
   check(cudaEventCreate(&w->mid), "cudaEventCreate");
   check(cudaEventCreate(&w->stop), "cudaEventCreate");
-  g_ws.push_back(std::move(w));
-  return *g_ws.back();
+  if (blocking) {
+    check(cudaEventCreateWithFlags(&w->sync_event, cudaEventBlockingSync | cudaEventDisableTiming),
+          "cudaEventCreate");
+  }
+  return w;
+}
+
+void sync_stream(Workspace& w, cudaStream_t st, const char* what) {
+  if (w.sync_event != nullptr) {
+    check(cudaEventRecord(w.sync_event, st), what);
+    check(cudaEventSynchronize(w.sync_event), what);
+  } else {
+    check(cudaStreamSynchronize(st), what);
+  }
+}
+
+void release_buffers(Workspace& w) {
+  cudaSetDevice(w.device);
+  for (auto& kv : w.buf) {
+    if (kv.second.ptr != nullptr) cudaFreeAsync(kv.second.ptr, w.stream);
+  }
+  w.buf.clear();
+}
+
+void destroy_workspace(Workspace& w) {
+  release_buffers(w);
+  if (w.stream) cudaStreamSynchronize(w.stream);
+  if (w.start) cudaEventDestroy(w.start);
+  if (w.mid) cudaEventDestroy(w.mid);
+  if (w.stop) cudaEventDestroy(w.stop);
+  if (w.sync_event) cudaEventDestroy(w.sync_event);
+  if (w.stream) cudaStreamDestroy(w.stream);
+  w.start = w.mid = w.stop = w.sync_event = nullptr;
+  w.stream = nullptr;
 }
 
 void* ensure_bytes(Workspace& w, int slot, size_t bytes) {
   bytes = std::max<size_t>(bytes, 256);
   Buffer& b = w.buf[slot];
   if (b.bytes < bytes) {
-    if (b.ptr != nullptr) check(cudaFree(b.ptr), "cudaFree");
+    cudaStream_t s = w.alloc_stream != nullptr ? w.alloc_stream : w.stream;
+    if (b.ptr != nullptr) check(cudaFreeAsync(b.ptr, s), "cudaFreeAsync");
     b.ptr = nullptr;
     b.bytes = 0;
-    check(cudaMalloc(&b.ptr, bytes), "cudaMalloc");
+    check(cudaMallocAsync(&b.ptr, bytes, s), "cudaMallocAsync");
     b.bytes = bytes;
   }
   return b.ptr;
@@ -129,10 +176,13 @@ uint64_t partition_bytes(const uint64_t count[3], uint32_t fb) {
   return b;
 }
 
+bool autotune_requested(uint32_t flags) { return (flags & TERGPU_ROOT_AUTOTUNE) != 0; }
+
+// 0: the default (variant 3, or the autotuner's pick), 1 or 2 when a flag forces one.
 uint32_t sweep_variant(uint32_t flags) {
   if ((flags & TERGPU_ROOT_SWEEP_V1) != 0) return 1;
   if ((flags & TERGPU_ROOT_SWEEP_V2) != 0) return 2;
-  return 3;
+  return 0;
 }
 
 uint32_t checked_shards(uint32_t index, uint32_t count) {
@@ -144,9 +194,95 @@ uint32_t checked_shards(uint32_t index, uint32_t count) {
   return n;
 }
 
+// ---- autotuner: per root shape, the fastest (family bits, filter bits, sweep
+// variant) among the neighbours of the size-based choice, timed as device time
+// (partition + sweep) on one 64th of the root's target families (shard 0 of
+// 64: all of A and B against 1/64 of D); cached for the life of the process.
+// Replaces the reference's CPU probe dispatcher (ter2_root/frozen/ter_arwlf.cpp:612-747)
+// on the device side.  The choice changes only the time, never a result.
+struct ShapeKey {
+  uint32_t q, la, lb, ld, proj;
+  bool operator<(const ShapeKey& o) const {
+    return std::tie(q, la, lb, ld, proj) < std::tie(o.q, o.la, o.lb, o.ld, o.proj);
+  }
+};
+struct Tuned {
+  uint32_t fb = 0, filter_bits = 0, variant = 0;
+};
+std::mutex g_tune_mu;
+std::map<ShapeKey, Tuned> g_tuned;
+
+uint32_t size_bucket(uint64_t n) {
+  return n == 0 ? 0u : static_cast<uint32_t>(std::lround(4.0 * std::log2(static_cast<double>(n))));
+}
+
+Tuned autotune(Workspace& w, const JoinInput& in, uint64_t input_bytes, float* spent_ms) {
+  const uint32_t F = std::min<uint32_t>(in.quotient_bits, 64);
+  const Tuning base = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, 0, 0, 3, 1);
+  Tuned best;
+  float best_ms = 0;
+  *spent_ms = 0;
+  for (uint32_t variant : {3u, 2u}) {
+    for (int dfb = -1; dfb <= 1; ++dfb) {
+      for (int dfl = -1; dfl <= 1; ++dfl) {
+        JoinInput j = in;
+        j.autotune = false;
+        j.count_only = true;
+        j.capacity = 0;
+        j.projected_bits = 0;
+        j.shard = 0;
+        j.shards = 64;
+        j.family_bits = static_cast<uint32_t>(static_cast<int>(base.fb) + dfb);
+        j.filter_bits = static_cast<uint32_t>(static_cast<int>(base.wb) + 5 + dfl);
+        j.sweep_variant = variant;
+        if (j.family_bits < 6 || j.family_bits + 2 > F || j.filter_bits < 10 || j.filter_bits > 20) continue;
+        try {
+          const JoinResult r = run_join(w, j, input_bytes);
+          const float ms = r.partition_ms + r.sweep_ms;
+          *spent_ms += r.join_ms;
+          if (best.fb == 0 || ms < best_ms) {
+            best_ms = ms;
+            best = Tuned{j.family_bits, j.filter_bits, variant};
+          }
+        } catch (const Failure&) {
+          t_error.clear();  // a candidate outside the supported range: skip it
+        }
+      }
+    }
+  }
+  return best;
+}
+
 // Partition + sweep(s) on keys already on the device.  The only host
 // synchronization is the final download of counters and family sizes.
 JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
+  if (in.autotune && in.family_bits == 0 && in.filter_bits == 0 && in.sweep_variant == 0 &&
+      in.count[0] != 0 && in.count[1] != 0 && in.count[2] != 0) {
+    const ShapeKey key{in.quotient_bits, size_bucket(in.count[0]), size_bucket(in.count[1]),
+                       size_bucket(in.count[2]), in.projected_bits};
+    Tuned t;
+    float spent = 0;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) t = it->second;
+    }
+    if (t.fb == 0) {
+      t = autotune(w, in, input_bytes, &spent);
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      if (t.fb != 0) g_tuned[key] = t;
+    }
+    JoinInput j = in;
+    j.autotune = false;
+    if (t.fb != 0) {
+      j.family_bits = t.fb;
+      j.filter_bits = t.filter_bits;
+      j.sweep_variant = t.variant;
+    }
+    JoinResult r = run_join(w, j, input_bytes);
+    r.tune_ms = spent;
+    return r;
+  }
   JoinResult r;
   const uint32_t Q = in.quotient_bits;
   const uint32_t F = std::min<uint32_t>(Q, 64);
@@ -210,6 +346,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   // v3 needs full 32-bit windows (mrb >= 32); below that the B-in-registers
   // sweep (v2) runs, exact for any family order.
   const uint32_t main_variant = tu.variant == 3 && F - tu.fb < 32 ? 2u : tu.variant;
+  r.tuning.variant = main_variant;
   if (main_variant == 3 && in.count[1] != 0) {
     // B families in lane slots of distinct residual classes mod 32 (bank-free probes)
     launch_family_arrange(res[1], hi[1], ids[1], off[1], cnt[1], nfam, st);
@@ -267,7 +404,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     check(cudaMemcpyAsync(hcnt[l].data(), cnt[l], nfam * 4ull, cudaMemcpyDeviceToHost, st),
           "count download");
   }
-  check(cudaStreamSynchronize(st), "join");
+  sync_stream(w, st, "join");
   check(cudaEventElapsedTime(&r.join_ms, w.start, w.stop), "elapsed");
   check(cudaEventElapsedTime(&r.partition_ms, w.start, w.mid), "elapsed");
   check(cudaEventElapsedTime(&r.sweep_ms, w.mid, w.stop), "elapsed");
@@ -308,6 +445,8 @@ void fill_out(const JoinResult& j, tergpu_root_out* out) {
   out->family_bits = j.tuning.fb;
   out->filter_bits = j.tuning.wb + 5;
   out->kernel_launches = j.launches;
+  out->sweep_variant = j.tuning.variant;
+  out->tune_ms = j.tune_ms;
 }
 
 int guarded(const char* what, int (*body)(const void*, void*), const void* in, void* out) {
@@ -356,6 +495,7 @@ int root_run_body(const void* vin, void* vout) {
   std::lock_guard<std::mutex> lock(w.mu);
   check(cudaSetDevice(w.device), "cudaSetDevice");
   cudaStream_t st = in->stream != nullptr ? static_cast<cudaStream_t>(in->stream) : w.stream;
+  w.alloc_stream = st;
   uint64_t input_bytes = 0;
   if (!resident) {
     for (int l = 0; l < 3; ++l) input_bytes += in->count[l] * 13 + 64;
@@ -409,6 +549,7 @@ int root_run_body(const void* vin, void* vout) {
   j.capacity = count_only ? 0 : out->capacity;
   j.count_only = count_only;
   j.sweep_variant = sweep_variant(in->flags);
+  j.autotune = autotune_requested(in->flags) && j.sweep_variant == 0;
   j.shard = in->shard_index;
   j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);
@@ -490,6 +631,7 @@ int root_records_body(const void* vin, void* vout) {
   Workspace& w = workspace(in->device);
   std::lock_guard<std::mutex> lock(w.mu);
   check(cudaSetDevice(w.device), "cudaSetDevice");
+  w.alloc_stream = w.stream;
   uint64_t input_bytes = 0;
   for (int l = 0; l < 3; ++l) input_bytes += in->count[l] * (in->record_bytes + 9) + 64;
   if (in->memory_limit_bytes != 0 && input_bytes > in->memory_limit_bytes) {
@@ -539,6 +681,7 @@ int root_records_body(const void* vin, void* vout) {
   j.capacity = count_only ? 0 : out->root.capacity;
   j.count_only = count_only;
   j.sweep_variant = sweep_variant(in->flags);
+  j.autotune = autotune_requested(in->flags) && j.sweep_variant == 0;
   j.shard = in->shard_index;
   j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);
@@ -619,16 +762,9 @@ void tergpu_release(void) {
   std::lock_guard<std::mutex> lock(tergpu::g_mu);
   for (auto& w : tergpu::g_ws) {
     std::lock_guard<std::mutex> inner(w->mu);
-    cudaSetDevice(w->device);
-    for (auto& kv : w->buf) {
-      if (kv.second.ptr != nullptr) cudaFree(kv.second.ptr);
-      kv.second.ptr = nullptr;
-      kv.second.bytes = 0;
-    }
-    if (w->start) cudaEventDestroy(w->start);
-    if (w->mid) cudaEventDestroy(w->mid);
-    if (w->stop) cudaEventDestroy(w->stop);
-    if (w->stream) cudaStreamDestroy(w->stream);
+    tergpu::destroy_workspace(*w);
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, w->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   }
   tergpu::g_ws.clear();
 }

@@ -5,8 +5,11 @@
 
 #include <cuda_runtime.h>
 
+#include "tergpu.h"
+
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 
@@ -26,16 +29,36 @@ struct Buffer {
   size_t bytes = 0;
 };
 
+// Device buffers, a stream and timing events for one call at a time.  Buffers
+// are stream-ordered allocations (cudaMallocAsync / cudaFreeAsync on
+// alloc_stream, or on `stream` when that is null), so growing one workspace
+// never waits for work that other workspaces have in flight on the device.
 struct Workspace {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t alloc_stream = nullptr;  // the stream the current call launches on
   cudaEvent_t start = nullptr, mid = nullptr, stop = nullptr;
+  // batch slots wait on a blocking-sync event (the host thread sleeps instead of
+  // spinning: many slots share the host cores); the shared workspace spins
+  cudaEvent_t sync_event = nullptr;
   std::map<int, Buffer> buf;
   std::mutex mu;
 };
 
-// The workspace of a device (created on first use).
+// Waits until the work queued so far on `st` is done (see Workspace::sync_event).
+void sync_stream(Workspace& w, cudaStream_t st, const char* what);
+
+// The shared workspace of a device (created on first use; calls through it are
+// serialized by its mutex).
 Workspace& workspace(int device);
+
+// A workspace with its own stream and events; `blocking` makes its waits yield the
+// host thread (the batch engine's slots).
+std::unique_ptr<Workspace> make_workspace(int device, bool blocking = false);
+// Frees a workspace's buffers, stream and events (waits for its stream).
+void destroy_workspace(Workspace& w);
+// Returns a workspace's buffers to the device pool (stream-ordered, no wait).
+void release_buffers(Workspace& w);
 
 // Grow-only device buffer in slot `slot` of the workspace.
 void* ensure_bytes(Workspace& w, int slot, size_t bytes);
@@ -64,6 +87,7 @@ struct JoinInput {
   uint64_t capacity;
   bool count_only;
   uint32_t sweep_variant;  // 0: default (3), else 1, 2 or 3
+  bool autotune = false;   // pick fb / filter bits / variant by timing a sample first
   uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
   cudaStream_t stream;
 };
@@ -73,6 +97,7 @@ struct JoinResult {
   uint64_t device_bytes = 0;
   float join_ms = 0, partition_ms = 0, sweep_ms = 0;
   uint32_t launches = 0;
+  float tune_ms = 0;       // device time the autotuner spent on this shape (0: cached)
   Tuning tuning;
   uint32_t* d_triples = nullptr;  // device, capacity triples (valid until the next join)
 };
@@ -84,6 +109,10 @@ uint32_t checked_shards(uint32_t index, uint32_t count);
 
 // Partition + sweep on keys already on the device (throws Failure).
 JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes);
+
+// One attempt range (tergpu_attempt_run's body) on `own`, a private workspace,
+// or on the device's shared workspace when `own` is null.  Returns the status.
+int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace* own);
 
 // Slots 0..99 belong to the root entry points; the attempt driver uses 100+.
 constexpr int kAttemptSlotBase = 100;

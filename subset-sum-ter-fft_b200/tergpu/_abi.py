@@ -40,6 +40,7 @@ ROOT_DEVICE_INPUTS = 2
 ABI_VERSION = 2  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
 ROOT_SWEEP_V1 = 4
 ROOT_SWEEP_V2 = 8
+ROOT_AUTOTUNE = 16
 MAX_QUOTIENT_BITS = 72
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -68,6 +69,7 @@ class RootOut(ctypes.Structure):
         ("partition_ms", ctypes.c_double), ("sweep_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double), ("family_bits", ctypes.c_uint32),
         ("filter_bits", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+        ("sweep_variant", ctypes.c_uint32), ("tune_ms", ctypes.c_double),
     ]
 
 

@@ -47,7 +47,7 @@ class AttemptOut(ctypes.Structure):
         ("stats", ctypes.POINTER(AttemptStats)), ("l1_records", ctypes.POINTER(ctypes.c_uint8) * 3),
         ("l1_capacity", ctypes.c_uint64 * 3), ("child_targets", (ctypes.c_uint32 * 4) * 3),
         ("root_target", ctypes.c_uint32 * 4), ("device_bytes", ctypes.c_uint64),
-        ("total_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double), ("device_bytes_held", ctypes.c_uint64),
     ]
 
 
@@ -74,6 +74,8 @@ class FullTerResult:
     attempts: list = field(default_factory=list)
     snapshot: object | None = None
     total_ms: float = 0.0
+    device_bytes: int = 0        # the preflight's predicted bytes
+    device_bytes_held: int = 0   # bytes the workspace held at the end of the call
 
     @property
     def status_name(self) -> str:
@@ -92,15 +94,19 @@ def _stats_dict(s: AttemptStats) -> dict:
     }
 
 
-def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -> FullTerResult:
-    """Runs attempts [attempt_first, attempt_first + attempt_limit) on the device.
+def _result(st: int, out: AttemptOut, stats, n: int) -> FullTerResult:
+    res = FullTerResult(status=st, r1=int(out.r1), r2=int(out.r2), level3_size=int(out.level3_size),
+                        total_ms=float(out.total_ms), device_bytes=int(out.device_bytes),
+                        device_bytes_held=int(out.device_bytes_held),
+                        attempts=[_stats_dict(stats[i]) for i in range(int(out.attempts_run))])
+    if st == _abi.FOUND:
+        res.witness = np.array(out.witness[:n], dtype=np.uint8)
+        res.found_attempt = int(out.found_attempt)
+    return res
 
-    `cancel` may be a ctypes.c_int32 whose value the caller sets from another
-    thread; the loop stops with Cancelled at the next stage boundary."""
-    config = config or FullTerConfig()
-    lib = _abi.load()
-    lib.tergpu_attempt_run.argtypes = [ctypes.POINTER(AttemptIn), ctypes.POINTER(AttemptOut)]
-    lib.tergpu_attempt_run.restype = ctypes.c_int
+
+def make_request(instance, config: FullTerConfig, cancel=None):
+    """The C structs of one request: (AttemptIn, AttemptOut, keep-alive buffers)."""
     values = np.ascontiguousarray(instance.values_le, dtype=np.uint64).reshape(-1)
     target = np.ascontiguousarray(instance.target_le, dtype=np.uint64)
     ain = AttemptIn()
@@ -117,6 +123,19 @@ def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -
     stats = (AttemptStats * max(1, config.attempt_limit))()
     out = AttemptOut()
     out.stats = ctypes.cast(stats, ctypes.POINTER(AttemptStats))
+    return ain, out, (values, target, stats)
+
+
+def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -> FullTerResult:
+    """Runs attempts [attempt_first, attempt_first + attempt_limit) on the device.
+
+    `cancel` may be a ctypes.c_int32 whose value the caller sets from another
+    thread; the loop stops with Cancelled at the next stage boundary."""
+    config = config or FullTerConfig()
+    lib = _abi.load()
+    lib.tergpu_attempt_run.argtypes = [ctypes.POINTER(AttemptIn), ctypes.POINTER(AttemptOut)]
+    lib.tergpu_attempt_run.restype = ctypes.c_int
+    ain, out, (_values, _target, stats) = make_request(instance, config, cancel)
     w64, w32 = (instance.n + 63) // 64, (instance.n + 31) // 32
     rb = 16 * w64 + 4 * w32
     bufs = []
@@ -130,12 +149,7 @@ def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -
     if st not in (_abi.FOUND, _abi.ATTEMPT_LIMIT_REACHED, _abi.CANCELLED, _abi.RESOURCE_LIMIT,
                   _abi.INVALID_CONFIGURATION):
         raise TergpuError(st, _abi.last_error())
-    res = FullTerResult(status=st, r1=int(out.r1), r2=int(out.r2), level3_size=int(out.level3_size),
-                        total_ms=float(out.total_ms),
-                        attempts=[_stats_dict(stats[i]) for i in range(int(out.attempts_run))])
-    if st == _abi.FOUND:
-        res.witness = np.array(out.witness[: instance.n], dtype=np.uint8)
-        res.found_attempt = int(out.found_attempt)
+    res = _result(st, out, stats, instance.n)
     if bufs and out.attempts_run > 0:
         from .snapshot import Snapshot
 

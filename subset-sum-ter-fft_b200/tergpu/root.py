@@ -49,6 +49,7 @@ class Config:
     capacity: int = 1 << 16
     sweep_v1: bool = False  # sweep variant 1 (A in registers)
     sweep_v2: bool = False  # sweep variant 2 (B in registers, windows sorted); default: variant 3
+    autotune: bool = False  # pick fb / filter bits / variant per shape by timing a 1/64 sample
     shard_index: int = 0
     shard_count: int = 1  # power of two <= 64: join only D entries with key_d == index (mod count)
 
@@ -68,6 +69,8 @@ class Telemetry:
     kernel_launches: int = 0
     family_bits: int = 0
     filter_bits: int = 0
+    sweep_variant: int = 0
+    tune_ms: float = 0.0
 
 
 @dataclass
@@ -94,7 +97,8 @@ def _telemetry(out: _abi.RootOut) -> Telemetry:
         join_ms=float(out.join_ms), partition_ms=float(out.partition_ms),
         sweep_ms=float(out.sweep_ms), total_ms=float(out.total_ms),
         kernel_launches=int(out.kernel_launches),
-        family_bits=int(out.family_bits), filter_bits=int(out.filter_bits))
+        family_bits=int(out.family_bits), filter_bits=int(out.filter_bits),
+        sweep_variant=int(out.sweep_variant), tune_ms=float(out.tune_ms))
 
 
 def run_gpu_root(keys: RootKeys, config: Config | None = None,
@@ -116,7 +120,8 @@ def run_gpu_root(keys: RootKeys, config: Config | None = None,
     rin.quotient_bits = keys.quotient_bits
     rin.flags = (_abi.ROOT_COUNT_ONLY if config.count_only else 0) | \
         (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
-        (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0)
+        (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0) | \
+        (_abi.ROOT_AUTOTUNE if config.autotune else 0)
     for l in range(3):
         rin.count[l] = len(lo[l])
         rin.key_lo[l] = _p(lo[l], ctypes.c_uint64)
@@ -158,7 +163,8 @@ def run_gpu_root_records(snap, config: Config | None = None,
     rin.r1 = snap.r1
     rin.flags = (_abi.ROOT_COUNT_ONLY if config.count_only else 0) | \
         (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
-        (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0)
+        (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0) | \
+        (_abi.ROOT_AUTOTUNE if config.autotune else 0)
     rin.record_bytes = snap.record_bytes
     recs = [np.ascontiguousarray(r, dtype=np.uint8) for r in snap.records]
     targets = [np.ascontiguousarray(t, dtype=np.uint32) for t in snap.child_targets]

@@ -259,3 +259,24 @@ def test_sharded_root_in_one_process_and_bad_shard_counts(tg, oracle_mod, golden
         with pytest.raises(tg.TergpuError) as e:
             tg.run_gpu_root(keys, tg.Config(shard_index=index, shard_count=count))
         assert e.value.status == 66  # InvalidInput
+
+
+def test_autotune_is_exact_and_cached(tg, oracle_mod, golden):
+    """The autotuner times candidate tunings on 1/64 of the target families and
+    caches the pick per shape; the result is the reference's either way."""
+    from tergpu import workload
+
+    g = golden["synthetic_roots"][1]
+    _, _, keys = keys_of(oracle_mod, g["bits"], g["seed"], g["size"], g["pool"])
+    first = tg.run_gpu_root(keys, tg.Config(autotune=True))
+    second = tg.run_gpu_root(keys, tg.Config(autotune=True))
+    for res in (first, second):
+        assert_digest(workload.digest(res.triples), g["brute"])
+        assert res.telemetry.sweep_variant in (2, 3)
+    assert first.telemetry.tune_ms > 0 and second.telemetry.tune_ms == 0
+    assert (first.telemetry.family_bits, first.telemetry.filter_bits,
+            first.telemetry.sweep_variant) == (second.telemetry.family_bits,
+                                               second.telemetry.filter_bits,
+                                               second.telemetry.sweep_variant)
+    plain = tg.run_gpu_root(keys, tg.Config(sweep_v1=True))
+    assert plain.telemetry.sweep_variant == 1 and plain.telemetry.tune_ms == 0
