@@ -532,8 +532,9 @@ def run_batch_modes(args):
     torch.cuda.set_device(0)
     serve = args.serve
     reqs = solve_requests(args, serve)
-    # warm both paths (workspaces, module load)
-    batch.solve_batch(reqs[:4], slots=2)
+    # warm both paths: module load, and every slot's workspace with its captured
+    # attempt graphs (the engine keeps its slots between calls, as a server would)
+    batch.solve_batch(reqs, slots=args.slots)
     one = batch.solve_batch(reqs, slots=1, served=serve)
     many = batch.solve_batch(reqs, slots=args.slots, served=serve)
     for i, (a, b) in enumerate(zip(one.results, many.results)):

@@ -225,6 +225,10 @@ typedef struct {
 /* tergpu_attempt_in.flags */
 #define TERGPU_ATTEMPT_CAPTURE_ONLY 1u /* stop after L1 (export only): the device
                                           counterpart of stream_full_ter_root_lists */
+#define TERGPU_ATTEMPT_NO_GRAPH 4u     /* n = 36 and 72 run each attempt as one captured CUDA
+                                          graph (fixed capacities, counts kept on the device);
+                                          this flag runs the stage-by-stage path instead.
+                                          Same results */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return
@@ -275,9 +279,12 @@ int tergpu_attempt_run(const tergpu_attempt_in *in, tergpu_attempt_out *out);
  *
  * Request i is jobs[i] (its device field is ignored: the batch's device is used)
  * and its result outs[i], exactly what tergpu_attempt_run(&jobs[i], &outs[i])
- * returns when called alone; outs[i].status carries the status.  `slots`
- * attempt pipelines run concurrently, each a host thread with its own CUDA
- * stream and device workspace.  A request becomes eligible at arrival_ms[i]
+ * returns when called alone (status, attempts_run, stats, witness, found_attempt,
+ * r1, r2, level3_size); outs[i].status carries the status.  The unit of work is
+ * one attempt: `slots` attempts run concurrently, each on a host thread with its
+ * own CUDA stream and device workspace, and a request is decided by its lowest
+ * attempt that is not NoWitnessThisAttempt (attempts above it are not started);
+ * L1 exports (outs[i].l1_records) are not produced in a batch.  A request becomes eligible at arrival_ms[i]
  * after the call starts (NULL: all at once); eligible requests are admitted in
  * arrival order while a slot is free and the predicted device bytes of the
  * running requests (each request's preflight) stay within memory_budget_bytes;
@@ -290,7 +297,7 @@ int tergpu_attempt_run(const tergpu_attempt_in *in, tergpu_attempt_out *out);
  */
 typedef struct {
   const tergpu_attempt_in *jobs;
-  tergpu_attempt_out *outs;     /* outs[i].stats / l1_records as in tergpu_attempt_run */
+  tergpu_attempt_out *outs;     /* outs[i].stats (attempt_count entries) as in tergpu_attempt_run */
   uint64_t count;
   const double *arrival_ms;     /* may be NULL */
   uint32_t slots;               /* concurrent attempt pipelines; 0: 8 */

@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 namespace tergpu {
@@ -118,7 +119,7 @@ enum : int {
   S_REC = S_L1 + 12,              // +0..+2
   S_RKLO = S_REC + 3,             // +0..+2
   S_RKHI = S_RKLO + 3,            // +0..+2
-  S_AFLAGS = S_RKHI + 3, S_ACOUNT
+  S_AFLAGS = S_RKHI + 3, S_ACOUNT, S_BOUNDS, S_KEPT9
 };
 
 EntryArrays entry_slot(Workspace& w, int slot, uint64_t count) {
@@ -131,16 +132,21 @@ ConstEntryArrays as_const(const EntryArrays& e) {
   return ConstEntryArrays{e.pos0, e.pos1, e.res_lo, e.res_hi};
 }
 
+// Entries [off, ...) of a list, as a list of their own.
+EntryArrays view(const EntryArrays& e, uint64_t off) {
+  return EntryArrays{e.pos0 + off, e.pos1 + off, e.res_lo + off, e.res_hi + off};
+}
+
 template <typename T>
 void download(Workspace& w, T* dst, const T* src, size_t n, cudaStream_t st) {
   check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, st), "download");
   sync_stream(w, st, "sync");
 }
 
-// Canonical order of `count` entries in `raw`: radix sort + unique into `dst`.
-uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, int dst_slot, EntryArrays* dst,
+// Canonical order of `count` entries in `raw`: radix sort + unique into `dst`
+// (room for `count` entries).
+uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, const EntryArrays& dst,
                       cudaStream_t st) {
-  *dst = entry_slot(w, dst_slot, count);
   unsigned long long* acc = ensure<unsigned long long>(w, S_ACC, 64);
   if (count == 0) return 0;
   launch_or_reduce(as_const(raw), count, acc, st);
@@ -152,7 +158,7 @@ uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, int 
   uint32_t* flags = ensure<uint32_t>(w, S_FLAGS, (count + 16) * 4);
   uint32_t* starts = ensure<uint32_t>(w, S_STARTS, (count + 16) * 4);
   uint32_t* scan2 = ensure<uint32_t>(w, S_SCAN2, (count / 2048 + 64) * 4);
-  launch_gather_unique(as_const(raw), perm, count, *dst, flags, starts, scan2, acc + 2, st);
+  launch_gather_unique(as_const(raw), perm, count, dst, flags, starts, scan2, acc + 2, st);
   unsigned long long kept = 0;
   download(w, &kept, acc + 2, 1, st);
   return kept;
@@ -167,6 +173,381 @@ void cancelled_check(const tergpu_attempt_in* in) {
 
 double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
+// ---- graph mode: one attempt as one captured CUDA graph (n = 36 and 72) ----
+//
+// Every size-dependent step reads its counts on the device (Count) and works in
+// fixed-capacity buffers owned by the plan, so an attempt is a fixed sequence
+// of launches: captured once per workspace and shape, replayed per attempt
+// after the attempt's values (targets) are copied into a device parameter
+// block.  The kernels and their order are those of the stage-by-stage path; a
+// capacity that would overflow is flagged on the device and that attempt runs
+// again on the stage-by-stage path, so results are identical either way.
+
+struct GraphParams {
+  MergeTargets t2;        // L3 -> L2 targets mod 2^r2
+  uint64_t q[9][3];       // L2 list 3g + l of the ternary merge: {t_lo, t_hi, tau_g}
+  uint64_t rk[3][4];      // L1 list l: {child_lo, child_hi, tau_lo, tau_hi} of the root keys
+  uint64_t root[2];       // T
+};
+
+struct GraphCounts {      // device counts the host reads after an attempt
+  uint32_t bounds[10];    // raw L2 list boundaries (bounds[9]: L3 -> L2 pairs)
+  unsigned long long kept9[9];
+  unsigned long long l2_triples[3];
+  unsigned long long ncand[3];
+  unsigned long long l1[3];
+  unsigned long long root_counters[kCounters];
+  unsigned long long auth[3];
+  unsigned int overflow;  // a segment above the canonical-sort capacity
+};
+
+struct GraphPlan {
+  uint32_t n = 0, r1 = 0, r2 = 0;
+  uint64_t l3 = 0, cap_l2 = 0, cap_t = 0, cap_r = 0;
+  Tuning tu_l2{}, tu_root{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // buffers
+  EntryArrays left{}, right{}, raw{}, l2all{}, cand{}, l1[3]{};
+  uint64_t* d_weights = nullptr;
+  uint32_t *bcnt = nullptr, *boff = nullptr, *bcur = nullptr, *order = nullptr;
+  uint32_t *counts = nullptr, *starts = nullptr, *scan = nullptr;
+  uint64_t* keys[3]{};
+  JoinBuffers jb{};
+  uint32_t* sort_scratch = nullptr;
+  uint32_t *perm = nullptr, *flags = nullptr, *starts2 = nullptr, *scan2 = nullptr;
+  uint8_t* recs[3]{};
+  uint64_t* rk_lo[3]{};
+  uint8_t* rk_hi[3]{};
+  uint8_t* aflags = nullptr;
+  GraphParams* d_params = nullptr;
+  GraphParams* h_params = nullptr;  // pinned
+  GraphCounts* d_counts = nullptr;
+  GraphCounts* h_counts = nullptr;  // pinned
+  uint32_t* h_triples = nullptr;    // pinned, cap_r * 3
+  uint8_t* h_aflags = nullptr;      // pinned, cap_r
+  uint64_t bytes = 0;
+
+  char* base = nullptr;  // one device allocation holds every buffer (null: size only)
+
+  template <typename T>
+  T* alloc(uint64_t count) {
+    const uint64_t b = (std::max<uint64_t>(count * sizeof(T), 256) + 255) & ~255ull;
+    const uint64_t at = bytes;
+    bytes += b;
+    return base != nullptr ? reinterpret_cast<T*>(base + at) : nullptr;
+  }
+  EntryArrays entries(uint64_t count) {
+    return EntryArrays{alloc<uint64_t>(count + 16), alloc<uint64_t>(count + 16), alloc<uint64_t>(count + 16),
+                       alloc<uint64_t>(count + 16)};
+  }
+  ~GraphPlan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (base) cudaFree(base);
+    if (h_params) cudaFreeHost(h_params);
+    if (h_counts) cudaFreeHost(h_counts);
+    if (h_triples) cudaFreeHost(h_triples);
+    if (h_aflags) cudaFreeHost(h_aflags);
+  }
+};
+
+// Expected level sizes of the FiniteSanity shape (the preflight's means).
+double expected_l1(uint64_t l3, uint32_t r1, uint32_t r2) {
+  const double l2 = (double)l3 * l3 / std::ldexp(1.0, r2);
+  return l2 * l2 * l2 / std::ldexp(1.0, r1 - r2) * 0.3;
+}
+
+// The capture: the stage-by-stage path's launches with device counts.
+void capture_attempt(GraphPlan& g, cudaStream_t st) {
+  const uint32_t n = g.n, r1 = g.r1, r2 = g.r2;
+  const uint64_t l3 = g.l3;
+  const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
+  const uint32_t rb = 16 * w64 + 4 * w32;
+  GraphCounts* dc = g.d_counts;
+  GraphParams* dp = g.d_params;
+  MergeTargets none{};
+  uint32_t launches = 0;
+  check(cudaMemsetAsync(&dc->overflow, 0, sizeof(unsigned int), st), "memset");
+  // L3 -> L2
+  launch_l2_count_all(as_const(g.left), l3, g.boff, r2, none, g.counts, st, &dp->t2);
+  launch_scan_u32(g.counts, 9 * l3, g.starts, g.scan, st);
+  launch_l2_bounds(g.starts, l3, dc->bounds, st);
+  launch_l2_fill_all(as_const(g.left), l3, as_const(g.right), g.boff, g.order, r2, none, n, g.starts, g.raw, st,
+                     &dp->t2, 9 * g.cap_l2);
+  Segments seg{};
+  launch_canon_small(as_const(g.raw), seg, 9, g.l2all, dc->kept9, st, dc->bounds, &dc->overflow,
+                     9 * g.cap_l2);
+  // L2 -> L1: three ternary joins on the projected quotient
+  const uint32_t b1 = std::min(r1, r2 + 32);
+  const uint32_t qbits = b1 - r2;
+  const uint64_t vary0 = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+  const uint64_t vary1 = n > 64 ? ((1ull << (n - 64)) - 1ull) : 0ull;
+  for (int grp = 0; grp < 3; ++grp) {
+    JoinWork jw{};
+    for (int l = 0; l < 3; ++l) {
+      const int li = 3 * grp + l;
+      launch_l2_quotients(as_const(g.l2all), Count(g.cap_l2, &dc->kept9[li]), b1, r2, 0, 0, l == 2, 0,
+                          g.keys[l], st, &dc->bounds[li], dp->q[li]);
+      jw.key_lo[l] = g.keys[l];
+      jw.key_hi[l] = nullptr;
+      jw.id[l] = nullptr;
+      jw.count[l] = Count(g.cap_l2, &dc->kept9[li]);
+    }
+    jw.quotient_bits = qbits;
+    jw.cells = nullptr;
+    jw.shard = 0;
+    jw.shards = 1;
+    jw.cap = g.cap_t;
+    jw.main_sweep = true;
+    jw.projected_bits = 0;
+    enqueue_join(g.jb, jw, g.tu_l2, nullptr, st, &launches);
+    launch_copy_count(&g.jb.counters[kTriples], &dc->l2_triples[grp], st);
+    launch_l1_parents(g.jb.triples, Count(g.cap_t, &g.jb.counters[kTriples]), as_const(g.l2all),
+                      as_const(g.l2all), as_const(g.l2all), n, n / 6, g.cand, &dc->ncand[grp], st,
+                      &dc->bounds[3 * grp]);
+    radix_sort_entries(as_const(g.cand), Count(g.cap_t, &dc->ncand[grp]), vary0, vary1, g.perm,
+                       g.sort_scratch, st);
+    launch_gather_unique(as_const(g.cand), g.perm, Count(g.cap_t, &dc->ncand[grp]), g.l1[grp], g.flags,
+                         g.starts2, g.scan2, &dc->l1[grp], st);
+  }
+  // root: records, device keys, join, authority
+  JoinWork jr{};
+  for (int l = 0; l < 3; ++l) {
+    launch_pack_records(as_const(g.l1[l]), Count(g.cap_t, &dc->l1[l]), n, g.recs[l], st);
+    RecordKeyArgs ka{};
+    ka.records = g.recs[l];
+    ka.count = Count(g.cap_t, &dc->l1[l]);
+    ka.record_bytes = rb;
+    ka.res_offset = 16 * w64;
+    ka.words32 = w32;
+    ka.n = n;
+    ka.r1 = r1;
+    ka.qbits = n - r1;
+    ka.negate = l == 2;
+    ka.key_lo = g.rk_lo[l];
+    ka.key_hi = g.rk_hi[l];
+    ka.dvals = dp->rk[l];
+    launch_record_keys(ka, st);
+    jr.key_lo[l] = g.rk_lo[l];
+    jr.key_hi[l] = g.rk_hi[l];
+    jr.id[l] = nullptr;
+    jr.count[l] = Count(g.cap_t, &dc->l1[l]);
+  }
+  jr.quotient_bits = n - r1;
+  jr.cells = nullptr;
+  jr.shard = 0;
+  jr.shards = 1;
+  jr.cap = g.cap_r;
+  jr.main_sweep = true;
+  jr.projected_bits = 0;
+  enqueue_join(g.jb, jr, g.tu_root, nullptr, st, &launches);
+  check(cudaMemsetAsync(dc->auth, 0, sizeof dc->auth, st), "memset");
+  AuthorityArgs au{};
+  for (int l = 0; l < 3; ++l) au.records[l] = g.recs[l];
+  au.record_bytes = rb;
+  au.res_offset = 16 * w64;
+  au.words32 = w32;
+  au.words64 = w64;
+  au.n = n;
+  au.droot = dp->root;
+  au.triples = g.jb.triples;
+  au.count = Count(g.cap_r, &g.jb.counters[kTriples]);
+  au.flags = g.aflags;
+  au.counters = dc->auth;
+  launch_authority(au, st);
+  check(cudaMemcpyAsync(dc->root_counters, g.jb.counters, sizeof dc->root_counters,
+                        cudaMemcpyDeviceToDevice, st), "counters");
+  // results to the pinned host copies
+  check(cudaMemcpyAsync(g.h_counts, dc, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st), "counts");
+  check(cudaMemcpyAsync(g.h_triples, g.jb.triples, g.cap_r * 12, cudaMemcpyDeviceToHost, st), "triples");
+  check(cudaMemcpyAsync(g.h_aflags, g.aflags, g.cap_r, cudaMemcpyDeviceToHost, st), "flags");
+  check(cudaGetLastError(), "graph capture");
+}
+
+bool graph_shape(uint32_t n) { return n == 36 || n == 72; }
+
+// The plan's fixed capacities, tunings and device buffers, carved from g->base
+// (without a base: only their byte count, which the preflight adds to its
+// prediction).
+void size_plan(GraphPlan* g, uint32_t n, uint32_t r1, uint32_t r2, uint64_t l3) {
+  g->n = n;
+  g->r1 = r1;
+  g->r2 = r2;
+  g->l3 = l3;
+  g->cap_l2 = kCanonSmallCap;
+  const double l1 = expected_l1(l3, r1, r2);
+  g->cap_t = n == 36 ? 4096 : (1u << 18);
+  g->cap_r = 4096;
+  const uint32_t b1 = std::min(r1, r2 + 32);
+  const uint32_t qbits = b1 - r2;
+  const uint32_t fb_l2 = std::max<uint32_t>(6, qbits > 17 ? qbits - 17 : 6);
+  const uint32_t filt_l2 = std::clamp<uint32_t>(qbits - fb_l2, 10, 20);
+  g->tu_l2 = choose_tuning(g->cap_l2, g->cap_l2, qbits, 0, fb_l2, filt_l2, 0, 1);
+  const uint32_t qroot = n - r1;
+  g->tu_root = choose_tuning((uint64_t)l1, (uint64_t)l1, std::min<uint32_t>(qroot, 64), 0, 0, 0, 0, 1);
+  const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
+  const uint32_t rb = 16 * w64 + 4 * w32;
+  const uint32_t nbk = 1u << r2;
+  // buffers (fixed capacities)
+  g->d_weights = g->alloc<uint64_t>(2 * n);
+  g->left = g->entries(l3);
+  g->right = g->entries(l3);
+  g->bcnt = g->alloc<uint32_t>(nbk + 16);
+  g->boff = g->alloc<uint32_t>(nbk + 16);
+  g->bcur = g->alloc<uint32_t>(2ull * nbk + 64);
+  g->order = g->alloc<uint32_t>(l3 + 16);
+  g->counts = g->alloc<uint32_t>(9 * l3 + 16);
+  g->starts = g->alloc<uint32_t>(9 * l3 + 16);
+  g->scan = g->alloc<uint32_t>(9 * l3 / 2048 + 64);
+  g->raw = g->entries(9 * g->cap_l2);
+  g->l2all = g->entries(9 * g->cap_l2);
+  for (int l = 0; l < 3; ++l) g->keys[l] = g->alloc<uint64_t>(g->cap_l2 + 16);
+  const uint64_t jcap = std::max<uint64_t>(g->cap_l2, g->cap_t);
+  const uint32_t nfam = 1u << std::max(g->tu_l2.fb, g->tu_root.fb);
+  for (int l = 0; l < 3; ++l) {
+    const uint64_t slots = jcap + nfam + 16;
+    g->jb.res[l] = g->alloc<uint64_t>(slots);
+    g->jb.hi[l] = g->alloc<uint8_t>(slots);
+    g->jb.id[l] = g->alloc<uint32_t>(slots);
+    g->jb.cnt[l] = g->alloc<uint32_t>(nfam + 1);
+    g->jb.off[l] = g->alloc<uint32_t>(nfam + 1);
+    g->jb.cur[l] = g->alloc<uint32_t>(nfam + 1);
+  }
+  g->jb.counters = g->alloc<unsigned long long>(kCounters);
+  g->jb.triples = g->alloc<uint32_t>(3 * std::max(g->cap_t, g->cap_r));
+  g->cand = g->entries(g->cap_t);
+  g->sort_scratch = g->alloc<uint32_t>(radix_scratch_words(g->cap_t));
+  g->perm = g->alloc<uint32_t>(g->cap_t + 16);
+  g->flags = g->alloc<uint32_t>(g->cap_t + 16);
+  g->starts2 = g->alloc<uint32_t>(g->cap_t + 16);
+  g->scan2 = g->alloc<uint32_t>(g->cap_t / 2048 + 64);
+  for (int l = 0; l < 3; ++l) {
+    g->l1[l] = g->entries(g->cap_t);
+    g->recs[l] = g->alloc<uint8_t>((g->cap_t + 16) * rb);
+    g->rk_lo[l] = g->alloc<uint64_t>(g->cap_t + 16);
+    g->rk_hi[l] = g->alloc<uint8_t>(g->cap_t + 16);
+  }
+  g->aflags = g->alloc<uint8_t>(g->cap_r + 16);
+  g->d_params = g->alloc<GraphParams>(1);
+  g->d_counts = g->alloc<GraphCounts>(1);
+}
+
+uint64_t plan_bytes(uint32_t n, uint32_t r1, uint32_t r2, uint64_t l3) {
+  GraphPlan g;
+  size_plan(&g, n, r1, r2, l3);
+  return g.bytes;
+}
+
+// The plan of workspace `w` for shape n (built and captured on first use), or
+// null when the shape runs stage by stage.
+GraphPlan* graph_plan(Workspace& w, uint32_t n, uint32_t r1, uint32_t r2, uint64_t l3, cudaStream_t st) {
+  if (!graph_shape(n)) return nullptr;
+  auto it = w.plans.find(n);
+  if (it != w.plans.end()) return static_cast<GraphPlan*>(it->second.get());
+  auto g = std::make_shared<GraphPlan>();
+  const uint64_t total = plan_bytes(n, r1, r2, l3);
+  check(cudaMalloc(&g->base, total), "cudaMalloc");
+  size_plan(g.get(), n, r1, r2, l3);
+  check(cudaMallocHost(&g->h_params, sizeof(GraphParams)), "cudaMallocHost");
+  check(cudaMallocHost(&g->h_counts, sizeof(GraphCounts)), "cudaMallocHost");
+  check(cudaMallocHost(&g->h_triples, g->cap_r * 12), "cudaMallocHost");
+  check(cudaMallocHost(&g->h_aflags, g->cap_r), "cudaMallocHost");
+  // capture (the kernels' shared-memory limits are set before, outside the capture)
+  prepare_root_kernels();
+  prepare_attempt_kernels();
+  check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+  try {
+    capture_attempt(*g, st);
+  } catch (...) {
+    cudaGraph_t dropped = nullptr;
+    cudaStreamEndCapture(st, &dropped);
+    if (dropped) cudaGraphDestroy(dropped);
+    throw;
+  }
+  check(cudaStreamEndCapture(st, &g->graph), "capture");
+  check(cudaGraphInstantiate(&g->exec, g->graph, 0), "graph instantiate");
+  w.plans[n] = g;
+  return g.get();
+}
+
+// Level 3 of the call's instance into the plan's buffers (direct launches).
+void graph_level3(GraphPlan& g, const std::vector<uint64_t>& weights, cudaStream_t st) {
+  check(cudaMemcpyAsync(g.d_weights, weights.data(), weights.size() * 8, cudaMemcpyHostToDevice, st), "weights");
+  launch_enumerate_half(g.d_weights, g.n, 0, g.l3, g.left, st);
+  launch_enumerate_half(g.d_weights, g.n, 1, g.l3, g.right, st);
+  launch_bucket_right(as_const(g.right), g.l3, g.r2, g.bcnt, g.boff, g.bcur, g.order, st);
+  check(cudaGetLastError(), "level 3");
+}
+
+// One attempt through the graph.  False when a capacity overflowed (the
+// attempt then runs stage by stage); else stats and the valid parents.
+bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, tergpu_attempt_stats* stat,
+                   std::vector<std::array<uint64_t, 2>>* parents, cudaStream_t st) {
+  const uint32_t n = g.n, r1 = g.r1, r2 = g.r2;
+  const uint32_t b1 = std::min(r1, r2 + 32);
+  const u128 m1 = mask128(b1), m2 = mask128(r2), nmask = mask128(n);
+  GraphParams& hp = *g.h_params;
+  std::memset(&hp, 0, sizeof hp);
+  for (int i = 0; i < 9; ++i) hp.t2.t[i] = (uint64_t)(tg.t2[i] & m2);
+  for (int grp = 0; grp < 3; ++grp) {
+    const u128 ta = tg.t2[3 * grp] & m2, tb = tg.t2[3 * grp + 1] & m2, t1 = tg.t1[grp] & m1;
+    const u128 tc = (t1 - ta - tb) & m2;
+    if (tc != (tg.t2[3 * grp + 2] & m2)) {
+      t_error = "derived third L2 target disagrees with the stored target";
+      throw Failure{TERGPU_INVARIANT_VIOLATION};
+    }
+    const uint64_t tau = (uint64_t)((((t1 - ta - tb - tc) & m1) >> r2));
+    const u128 tt[3] = {ta, tb, tc};
+    for (int l = 0; l < 3; ++l) {
+      hp.q[3 * grp + l][0] = (uint64_t)tt[l];
+      hp.q[3 * grp + l][1] = (uint64_t)(tt[l] >> 64);
+      hp.q[3 * grp + l][2] = tau;
+    }
+  }
+  u128 tau_res = T;
+  for (int l = 0; l < 3; ++l) tau_res = (tau_res - tg.t1[l]) & nmask;
+  const uint32_t Q = n - r1;
+  const u128 tau = (tau_res >> r1) & mask128(Q);
+  for (int l = 0; l < 3; ++l) {
+    hp.rk[l][0] = (uint64_t)tg.t1[l];
+    hp.rk[l][1] = (uint64_t)(tg.t1[l] >> 64);
+    hp.rk[l][2] = (uint64_t)tau;
+    hp.rk[l][3] = (uint64_t)(tau >> 64);
+  }
+  hp.root[0] = (uint64_t)T;
+  hp.root[1] = (uint64_t)(T >> 64);
+  check(cudaMemcpyAsync(g.d_params, g.h_params, sizeof(GraphParams), cudaMemcpyHostToDevice, st), "params");
+  check(cudaGraphLaunch(g.exec, st), "graph launch");
+  sync_stream(w, st, "graph");
+  const GraphCounts& c = *g.h_counts;
+  bool overflow = c.overflow != 0 || c.root_counters[kTriples] > g.cap_r;
+  for (int grp = 0; grp < 3; ++grp) overflow = overflow || c.l2_triples[grp] > g.cap_t;
+  if (overflow) return false;
+  for (int i = 0; i < 9; ++i) stat->level2_sizes[i] = c.kept9[i];
+  stat->l3_modular = c.bounds[9];
+  stat->l2_modular = c.l2_triples[0] + c.l2_triples[1] + c.l2_triples[2];
+  for (int l = 0; l < 3; ++l) stat->level1_sizes[l] = c.l1[l];
+  stat->root_pairs = c.l1[0] * c.l1[1];
+  stat->root_modular = c.root_counters[kTriples];
+  const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
+  const uint32_t rb = 16 * w64 + 4 * w32;
+  for (uint64_t i = 0; i < c.root_counters[kTriples]; ++i) {
+    if ((g.h_aflags[i] & 4) == 0) continue;
+    ++stat->valid_roots;
+    std::array<uint64_t, 2> p{0, 0};
+    for (int l = 0; l < 3; ++l) {
+      uint32_t wds[4] = {0, 0, 0, 0};  // the record's pos words (w64 <= 2)
+      check(cudaMemcpy(wds, g.recs[l] + (uint64_t)g.h_triples[3 * i + l] * rb, w64 * 8,
+                       cudaMemcpyDeviceToHost), "record download");
+      p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
+      if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
+    }
+    parents->push_back(p);
+  }
+  return true;
 }
 
 }  // namespace
@@ -204,8 +585,10 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   const double cand_est = std::pow(l2_est, 3) / std::ldexp(1.0, r1 - r2) * 1.3 + 64;
   const double l1_est = cand_est * 0.6;
   const double rec = 16.0 * w64 + 4.0 * w32;
-  const double predicted = 2.0 * (2 * l3 * 32.0 + 9 * l2_est * 32 + l2_est * 120 + cand_est * (32 + 12 + 60) +
-                                  3 * l1_est * (32 + rec + 40));
+  double predicted = 2.0 * (2 * l3 * 32.0 + 9 * l2_est * 32 + l2_est * 120 + cand_est * (32 + 12 + 60) +
+                            3 * l1_est * (32 + rec + 40));
+  // the graph plan's fixed buffers sit beside the stage-by-stage ones (its fallback)
+  if (graph_shape(n) && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) predicted += (double)plan_bytes(n, r1, r2, l3);
   out->device_bytes = (uint64_t)predicted;
   if (in->memory_limit_bytes != 0 && predicted > (double)in->memory_limit_bytes) {
     t_error = "predicted device bytes exceed the declared ceiling";
@@ -218,12 +601,14 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
 
   Workspace& w = own != nullptr ? *own : workspace(in->device);
   std::lock_guard<std::mutex> lock(w.mu);
-  // on every exit: the bytes the workspace holds (grow-only within the call)
+  // on every exit: the bytes the workspace holds for this call (grow-only
+  // within it): its stage buffers and the graph plan the call used
   struct Held {
     Workspace& w;
     tergpu_attempt_out* o;
+    const GraphPlan* plan = nullptr;
     ~Held() {
-      uint64_t bytes = 0;
+      uint64_t bytes = plan != nullptr ? plan->bytes : 0;
       for (const auto& kv : w.buf) bytes += kv.second.bytes;
       o->device_bytes_held = bytes;
     }
@@ -238,18 +623,37 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     weights[2 * i] = in->values_le[i * w64];
     weights[2 * i + 1] = w64 > 1 ? in->values_le[i * w64 + 1] : 0;
   }
-  uint64_t* d_weights = ensure<uint64_t>(w, S_WEIGHTS, weights.size() * 8);
-  check(cudaMemcpyAsync(d_weights, weights.data(), weights.size() * 8, cudaMemcpyHostToDevice, st), "weights");
-  EntryArrays left = entry_slot(w, S_L3, l3), right = entry_slot(w, S_L3 + 4, l3);
-  launch_enumerate_half(d_weights, n, 0, l3, left, st);
-  launch_enumerate_half(d_weights, n, 1, l3, right, st);
-  const uint32_t nbk = 1u << r2;
-  uint32_t* bcnt = ensure<uint32_t>(w, S_BCNT, (nbk + 16) * 4ull);
-  uint32_t* boff = ensure<uint32_t>(w, S_BOFF, (nbk + 16) * 4ull);
-  uint32_t* bcur = ensure<uint32_t>(w, S_BCUR, (2ull * nbk + 64) * 4);
-  uint32_t* order = ensure<uint32_t>(w, S_ORDER, (l3 + 16) * 4);
-  launch_bucket_right(as_const(right), l3, r2, bcnt, boff, bcur, order, st);
-  check(cudaGetLastError(), "level 3");
+  // n = 36 and 72: each attempt as one captured graph (not for L1 exports)
+  const bool exporting = (in->flags & TERGPU_ATTEMPT_CAPTURE_ONLY) != 0 || out->l1_records[0] != nullptr ||
+                         out->l1_records[1] != nullptr || out->l1_records[2] != nullptr;
+  GraphPlan* plan = nullptr;
+  if (!exporting && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
+    plan = graph_plan(w, n, r1, r2, l3, st);
+    held.plan = plan;
+    if (plan != nullptr) graph_level3(*plan, weights, st);
+  }
+  // the stage-by-stage path's level 3 (at once without a graph, else on the
+  // first attempt that overflows a graph capacity)
+  EntryArrays left{}, right{};
+  uint32_t *boff = nullptr, *order = nullptr;
+  auto dynamic_level3 = [&]() {
+    if (boff != nullptr) return;
+    uint64_t* d_weights = ensure<uint64_t>(w, S_WEIGHTS, weights.size() * 8);
+    check(cudaMemcpyAsync(d_weights, weights.data(), weights.size() * 8, cudaMemcpyHostToDevice, st),
+          "weights");
+    left = entry_slot(w, S_L3, l3);
+    right = entry_slot(w, S_L3 + 4, l3);
+    launch_enumerate_half(d_weights, n, 0, l3, left, st);
+    launch_enumerate_half(d_weights, n, 1, l3, right, st);
+    const uint32_t nbk = 1u << r2;
+    uint32_t* bcnt = ensure<uint32_t>(w, S_BCNT, (nbk + 16) * 4ull);
+    boff = ensure<uint32_t>(w, S_BOFF, (nbk + 16) * 4ull);
+    uint32_t* bcur = ensure<uint32_t>(w, S_BCUR, (2ull * nbk + 64) * 4);
+    order = ensure<uint32_t>(w, S_ORDER, (l3 + 16) * 4);
+    launch_bucket_right(as_const(right), l3, r2, bcnt, boff, bcur, order, st);
+    check(cudaGetLastError(), "level 3");
+  };
+  if (plan == nullptr) dynamic_level3();
 
   int status = TERGPU_ATTEMPT_LIMIT_REACHED;
   out->attempts_run = 0;
@@ -261,25 +665,57 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     std::memset(&stat, 0, sizeof stat);
     stat.attempt = attempt;
     const Targets tg = random_targets(in->seed + attempt, r1, r2, T);
-
-    // ---- L3 -> L2: nine binary merges, each in canonical order
+    std::vector<std::array<uint64_t, 2>> parents;
+    bool graphed = false;
+    if (plan != nullptr) {
+      graphed = graph_attempt(*plan, w, tg, T, &stat, &parents, st);
+      if (!graphed) {  // a capacity overflowed: this attempt runs stage by stage
+        parents.clear();
+        std::memset(&stat, 0, sizeof stat);
+        stat.attempt = attempt;
+        dynamic_level3();
+      }
+    }
+    if (!graphed) {
+    // ---- L3 -> L2: the nine binary merges in single launches (count, scan,
+    // fill), the raw lists back to back, then each list in canonical order
+    // (one CTA per list in shared memory when every list is small)
     std::array<EntryArrays, 9> l2;
     std::array<uint64_t, 9> l2n{};
-    uint32_t* counts = ensure<uint32_t>(w, S_L2CNT, (l3 + 16) * 4);
-    uint32_t* starts = ensure<uint32_t>(w, S_L2START, (l3 + 16) * 4);
-    uint32_t* scan = ensure<uint32_t>(w, S_SCAN, (l3 / 2048 + 64) * 4);
+    MergeTargets mt{};
+    for (int i = 0; i < 9; ++i) mt.t[i] = (uint64_t)(tg.t2[i] & mask128(r2));
+    uint32_t* counts = ensure<uint32_t>(w, S_L2CNT, (9 * l3 + 16) * 4);
+    uint32_t* starts = ensure<uint32_t>(w, S_L2START, (9 * l3 + 16) * 4);
+    uint32_t* scan = ensure<uint32_t>(w, S_SCAN, (9 * l3 / 2048 + 64) * 4);
+    uint32_t* bounds = ensure<uint32_t>(w, S_BOUNDS, 64);
+    launch_l2_count_all(as_const(left), l3, boff, r2, mt, counts, st);
+    launch_scan_u32(counts, 9 * l3, starts, scan, st);
+    launch_l2_bounds(starts, l3, bounds, st);
+    uint32_t hb[10];
+    download(w, hb, bounds, 10, st);
+    const uint64_t total_raw = hb[9];
+    EntryArrays raw = entry_slot(w, S_L2RAW, total_raw);
+    launch_l2_fill_all(as_const(left), l3, as_const(right), boff, order, r2, mt, n, starts, raw, st);
+    EntryArrays l2all = entry_slot(w, S_L2, total_raw);
+    Segments sg{};
+    uint32_t maxseg = 0;
     for (int i = 0; i < 9; ++i) {
-      const uint64_t t = (uint64_t)(tg.t2[i] & mask128(r2));
-      launch_l2_count(as_const(left), l3, boff, r2, t, counts, st);
-      launch_scan_u32(counts, l3, starts, scan, st);
-      uint32_t total = 0;
-      download(w, &total, starts + l3, 1, st);
-      EntryArrays raw = entry_slot(w, S_L2RAW, total);
-      launch_l2_fill(as_const(left), l3, as_const(right), boff, order, r2, t, n, starts, raw, st);
-      l2n[i] = canonicalize(w, raw, total, S_L2 + 4 * i, &l2[i], st);
-      stat.level2_sizes[i] = l2n[i];
-      stat.l3_modular += total;
+      sg.off[i] = hb[i];
+      sg.cnt[i] = hb[i + 1] - hb[i];
+      maxseg = std::max(maxseg, sg.cnt[i]);
+      stat.l3_modular += sg.cnt[i];
+      l2[i] = view(l2all, hb[i]);
     }
+    if (maxseg <= kCanonSmallCap) {
+      unsigned long long* kept = ensure<unsigned long long>(w, S_KEPT9, 16 * 8);
+      launch_canon_small(as_const(raw), sg, 9, l2all, kept, st);
+      unsigned long long hk[9];
+      download(w, hk, kept, 9, st);
+      for (int i = 0; i < 9; ++i) l2n[i] = hk[i];
+    } else {
+      for (int i = 0; i < 9; ++i) l2n[i] = canonicalize(w, view(raw, hb[i]), sg.cnt[i], l2[i], st);
+    }
+    for (int i = 0; i < 9; ++i) stat.level2_sizes[i] = l2n[i];
     check(cudaGetLastError(), "L3 -> L2");
     stat.l2_ms = ms_since(t_att);
     cancelled_check(in);
@@ -333,7 +769,8 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
                         as_const(l2[3 * g + 2]), n, n / 6, cand, acc + 4, st);
       unsigned long long ncand = 0;
       download(w, &ncand, acc + 4, 1, st);
-      l1n[g] = canonicalize(w, cand, ncand, S_L1 + 4 * g, &l1[g], st);
+      l1[g] = entry_slot(w, S_L1 + 4 * g, ncand);
+      l1n[g] = canonicalize(w, cand, ncand, l1[g], st);
       stat.level1_sizes[g] = l1n[g];
     }
     check(cudaGetLastError(), "L2 -> L1");
@@ -434,32 +871,32 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       check(cudaMemcpyAsync(hflags.data(), dflags, jr.triples, cudaMemcpyDeviceToHost, st), "d2h");
       sync_stream(w, st, "sync");
     }
-    // valid roots: parents of the flagged triples, canonical (sorted, unique)
-    std::vector<std::array<uint64_t, 2>> parents;
+    // valid roots: parents of the flagged triples
     for (uint64_t i = 0; i < jr.triples; ++i) {
       if ((hflags[i] & 4) == 0) continue;
       ++stat.valid_roots;
       std::array<uint64_t, 2> p{0, 0};
       for (int l = 0; l < 3; ++l) {
-        uint32_t wds[4];
-        check(cudaMemcpy(wds, recs[l] + (uint64_t)htrip[3 * i + l] * rb, 4 * w64 * 4, cudaMemcpyDeviceToHost),
+        uint32_t wds[4] = {0, 0, 0, 0};  // the record's pos words (w64 <= 2)
+        check(cudaMemcpy(wds, recs[l] + (uint64_t)htrip[3 * i + l] * rb, w64 * 8, cudaMemcpyDeviceToHost),
               "record download");
         p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
         if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
       }
       parents.push_back(p);
     }
+    stat.root_ms = ms_since(t_root);
+    // L1 export of the attempt (records + targets), when the caller asked for it
+    export_l1();
+    }  // stage by stage
+    // the valid roots' distinct parents in canonical order (sorted, unique)
     std::sort(parents.begin(), parents.end());
     parents.erase(std::unique(parents.begin(), parents.end()), parents.end());
     stat.level0_size = parents.size();
-    stat.root_ms = ms_since(t_root);
     stat.total_ms = ms_since(t_att);
     stat.status = parents.empty() ? TERGPU_NO_WITNESS_THIS_ATTEMPT : TERGPU_FOUND;
     if (out->stats != nullptr) out->stats[k] = stat;
     out->attempts_run = k + 1;
-
-    // L1 export of the attempt (records + targets), when the caller asked for it
-    export_l1();
 
     if (!parents.empty()) {
       // verify the lowest parent: binary digits, weight n/2, weights sum to the target
@@ -508,5 +945,13 @@ extern "C" int tergpu_attempt_run(const tergpu_attempt_in* in, tergpu_attempt_ou
     t_error = "host allocation failed";
     out->status = TERGPU_RESOURCE_LIMIT;
     return TERGPU_RESOURCE_LIMIT;
+  } catch (const std::exception& e) {
+    t_error = std::string("unexpected exception: ") + e.what();
+    out->status = TERGPU_DEVICE_ERROR;
+    return TERGPU_DEVICE_ERROR;
+  } catch (...) {
+    t_error = "unexpected exception";
+    out->status = TERGPU_DEVICE_ERROR;
+    return TERGPU_DEVICE_ERROR;
   }
 }

@@ -8,6 +8,7 @@
 //   canonical order ............ src/full_ter.cpp:320-326 (packed_less), 624-633
 
 #include "attempt_kernels.cuh"
+#include "root_kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -36,6 +37,10 @@ int blocks_for(uint64_t n, int threads, int cap = 148 * 16) {
   uint64_t b = (n + threads - 1) / threads;
   if (b > (uint64_t)cap) b = cap;
   return b == 0 ? 1 : (int)b;
+}
+
+__device__ __forceinline__ ConstEntryArrays offset_view(ConstEntryArrays e, uint64_t off) {
+  return ConstEntryArrays{e.pos0 + off, e.pos1 + off, e.res_lo + off, e.res_hi + off};
 }
 
 __global__ void k_enumerate_half(const uint64_t* __restrict__ weights, uint32_t n, uint32_t second,
@@ -117,6 +122,179 @@ __global__ void k_l2_fill(ConstEntryArrays left, uint64_t nl, ConstEntryArrays r
       out.res_hi[at] = (uint64_t)(sum >> 64);
     }
   }
+}
+
+__global__ void k_l2_count_all(ConstEntryArrays left, uint64_t nl, const uint32_t* __restrict__ off,
+                               uint32_t mask, MergeTargets t, const MergeTargets* __restrict__ dt,
+                               uint32_t* __restrict__ counts) {
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < 9 * nl;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t m = (uint32_t)(x / nl);
+    const uint64_t l = x - (uint64_t)m * nl;
+    const uint64_t tm = dt != nullptr ? dt->t[m] : t.t[m];
+    const uint32_t b = (uint32_t)(tm - left.res_lo[l]) & mask;
+    counts[x] = off[b + 1] - off[b];
+  }
+}
+
+__global__ void k_l2_bounds(const uint32_t* __restrict__ starts, uint64_t nl, uint32_t* __restrict__ bounds) {
+  if (threadIdx.x < 10) bounds[threadIdx.x] = starts[(uint64_t)threadIdx.x * nl];
+}
+
+__global__ void k_l2_fill_all(ConstEntryArrays left, uint64_t nl, ConstEntryArrays right,
+                              const uint32_t* __restrict__ off, const uint32_t* __restrict__ order,
+                              uint32_t mask, MergeTargets t, const MergeTargets* __restrict__ dt,
+                              uint32_t n, const uint32_t* __restrict__ starts, uint64_t cap,
+                              EntryArrays out) {
+  const u128 nm = nmask128(n);
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < 9 * nl;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t m = (uint32_t)(x / nl);
+    const uint64_t l = x - (uint64_t)m * nl;
+    const uint64_t tm = dt != nullptr ? dt->t[m] : t.t[m];
+    const uint32_t b = (uint32_t)(tm - left.res_lo[l]) & mask;
+    const u128 rl = ((u128)left.res_hi[l] << 64) | left.res_lo[l];
+    uint32_t at = starts[x];
+    for (uint32_t k = off[b]; k < off[b + 1] && at < cap; ++k, ++at) {
+      const uint32_t r = order[k];
+      const u128 rr = ((u128)right.res_hi[r] << 64) | right.res_lo[r];
+      const u128 sum = (rl + rr) & nm;
+      out.pos0[at] = left.pos0[l] | right.pos0[r];
+      out.pos1[at] = left.pos1[l] | right.pos1[r];
+      out.res_lo[at] = (uint64_t)sum;
+      out.res_hi[at] = (uint64_t)(sum >> 64);
+    }
+  }
+}
+
+// One CTA of 1024 threads per segment: bitonic sort of (pos0, pos1, index) in
+// shared memory (ties are identical digit vectors, so the order among them does
+// not matter), then the first of every run of equal keys is kept, compacted in
+// order.  Padding keys (all ones) sort last; no entry has all 64 bits of pos0 set.
+__global__ void __launch_bounds__(1024) k_canon_small(ConstEntryArrays raw, Segments seg,
+                                                      const uint32_t* __restrict__ dbounds, uint64_t cap,
+                                                      EntryArrays out, unsigned long long* __restrict__ kept,
+                                                      unsigned int* __restrict__ overflow) {
+  extern __shared__ __align__(16) uint64_t csm[];
+  uint64_t* k0 = csm;
+  uint64_t* k1 = k0 + kCanonSmallCap;
+  uint16_t* ix = reinterpret_cast<uint16_t*>(k1 + kCanonSmallCap);
+  uint32_t* pos = reinterpret_cast<uint32_t*>(ix + kCanonSmallCap);
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t s = blockIdx.x;
+  const uint32_t m = dbounds != nullptr ? dbounds[s + 1] - dbounds[s] : seg.cnt[s];
+  const uint32_t base = dbounds != nullptr ? dbounds[s] : seg.off[s];
+  if (m > kCanonSmallCap || (uint64_t)base + m > cap) {  // only with device bounds: the caller falls back
+    if (threadIdx.x == 0) {
+      kept[s] = 0;
+      if (overflow != nullptr) atomicOr(overflow, 1u);
+    }
+    return;
+  }
+  uint32_t p = 1;
+  while (p < m) p <<= 1;
+  for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
+    const bool ok = i < m;
+    k0[i] = ok ? raw.pos0[base + i] : ~0ull;
+    k1[i] = ok ? raw.pos1[base + i] : ~0ull;
+    ix[i] = (uint16_t)i;
+  }
+  __syncthreads();
+  for (uint32_t k = 2; k <= p; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
+        const uint32_t o = i ^ j;
+        if (o > i) {
+          const bool up = (i & k) == 0;
+          const bool greater = k0[i] > k0[o] || (k0[i] == k0[o] && k1[i] > k1[o]);
+          const bool less = k0[i] < k0[o] || (k0[i] == k0[o] && k1[i] < k1[o]);
+          if (up ? greater : less) {
+            const uint64_t a0 = k0[i], a1 = k1[i];
+            const uint16_t ai = ix[i];
+            k0[i] = k0[o];
+            k1[i] = k1[o];
+            ix[i] = ix[o];
+            k0[o] = a0;
+            k1[o] = a1;
+            ix[o] = ai;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // keep flags and their exclusive scan (four items per thread, in order)
+  const uint32_t per = (kCanonSmallCap + blockDim.x - 1) / blockDim.x;
+  const uint32_t begin = threadIdx.x * per;
+  uint32_t local = 0;
+  for (uint32_t i = begin; i < begin + per && i < m; ++i) {
+    local += (i == 0 || k0[i] != k0[i - 1] || k1[i] != k1[i - 1]) ? 1u : 0u;
+  }
+  uint32_t v = local;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  if (lane == 31) warp_tot[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < blockDim.x / 32 ? warp_tot[lane] : 0;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, w, d);
+      if (lane >= (uint32_t)d) w += o;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = v - local + (warp > 0 ? warp_tot[warp - 1] : 0);
+  for (uint32_t i = begin; i < begin + per && i < m; ++i) {
+    if (i == 0 || k0[i] != k0[i - 1] || k1[i] != k1[i - 1]) pos[run++] = ix[i];
+  }
+  __syncthreads();
+  const uint32_t total = warp_tot[(blockDim.x / 32) - 1];
+  for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+    const uint32_t src = base + pos[i];
+    out.pos0[base + i] = raw.pos0[src];
+    out.pos1[base + i] = raw.pos1[src];
+    out.res_lo[base + i] = raw.res_lo[src];
+    out.res_hi[base + i] = raw.res_hi[src];
+  }
+  if (threadIdx.x == 0) kept[s] = total;
+}
+
+// One CTA of 1024 threads: exclusive scan of n <= 65536 values; out[n] = total.
+__global__ void __launch_bounds__(1024) k_scan_small(const uint32_t* __restrict__ in, uint32_t n,
+                                                     uint32_t* __restrict__ out) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+  const uint32_t begin = threadIdx.x * per, end = min(n, begin + per);
+  uint32_t local = 0;
+  for (uint32_t i = begin; i < end; ++i) local += in[i];
+  uint32_t v = local;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(kFull, v, d);
+    if (lane >= (uint32_t)d) v += o;
+  }
+  if (lane == 31) warp_tot[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < blockDim.x / 32 ? warp_tot[lane] : 0;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, w, d);
+      if (lane >= (uint32_t)d) w += o;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = v - local + (warp > 0 ? warp_tot[warp - 1] : 0);
+  for (uint32_t i = begin; i < end; ++i) {
+    const uint32_t c = in[i];
+    out[i] = run;
+    run += c;
+  }
+  if (threadIdx.x == blockDim.x - 1) out[n] = run;
 }
 
 // ---- generic exclusive scan of uint32 (three kernels) ----------------------
@@ -201,12 +379,20 @@ __global__ void k_chunk_scan(const uint32_t* __restrict__ in, uint64_t n, const 
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = sums[nb];
 }
 
-__global__ void k_l2_quotients(ConstEntryArrays l, uint64_t count, uint32_t b1, uint32_t r2,
-                               uint64_t t_lo, uint64_t t_hi, int negate, uint64_t tau,
+__global__ void k_l2_quotients(ConstEntryArrays l, Count cnt, const uint32_t* __restrict__ doff,
+                               uint32_t b1, uint32_t r2, uint64_t t_lo, uint64_t t_hi, int negate,
+                               uint64_t tau, const uint64_t* __restrict__ dvals,
                                uint64_t* __restrict__ key) {
+  if (doff != nullptr) l = offset_view(l, *doff);
+  if (dvals != nullptr) {
+    t_lo = dvals[0];
+    t_hi = dvals[1];
+    tau = dvals[2];
+  }
   const u128 m1 = nmask128(b1);
   const u128 t = (((u128)t_hi << 64) | t_lo) & m1;
   const uint64_t qmask = (b1 - r2) >= 64 ? ~0ull : ((1ull << (b1 - r2)) - 1ull);
+  const uint64_t count = cnt.get();
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const u128 r = (((u128)l.res_hi[i] << 64) | l.res_lo[i]) & m1;
@@ -216,10 +402,17 @@ __global__ void k_l2_quotients(ConstEntryArrays l, uint64_t count, uint32_t b1, 
   }
 }
 
-__global__ void k_l1_parents(const uint32_t* __restrict__ triples, uint64_t nt, ConstEntryArrays x,
-                             ConstEntryArrays y, ConstEntryArrays z, uint32_t n, uint32_t ones,
-                             EntryArrays out, unsigned long long* __restrict__ count) {
+__global__ void k_l1_parents(const uint32_t* __restrict__ triples, Count ntc, ConstEntryArrays x,
+                             ConstEntryArrays y, ConstEntryArrays z, const uint32_t* __restrict__ doff,
+                             uint32_t n, uint32_t ones, EntryArrays out,
+                             unsigned long long* __restrict__ count) {
+  if (doff != nullptr) {
+    x = offset_view(x, doff[0]);
+    y = offset_view(y, doff[1]);
+    z = offset_view(z, doff[2]);
+  }
   const u128 nm = nmask128(n);
+  const uint64_t nt = ntc.get();
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nt;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t a = triples[3 * i], b = triples[3 * i + 1], c = triples[3 * i + 2];
@@ -241,7 +434,8 @@ __global__ void k_l1_parents(const uint32_t* __restrict__ triples, uint64_t nt, 
 }
 
 // ---- stable LSD radix sort on (pos0, pos1) ---------------------------------
-__global__ void k_radix_init(ConstEntryArrays in, uint64_t n, uint64_t* khi, uint64_t* klo, uint32_t* idx) {
+__global__ void k_radix_init(ConstEntryArrays in, Count cnt, uint64_t* khi, uint64_t* klo, uint32_t* idx) {
+  const uint64_t n = cnt.get();
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     khi[i] = in.pos0[i];
@@ -256,10 +450,11 @@ __device__ __forceinline__ uint32_t digit_of(uint64_t hi, uint64_t lo, uint32_t 
 
 // counts[d * nb + b]: items of digit d in tile b
 __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint64_t* __restrict__ khi,
-                                                              const uint64_t* __restrict__ klo, uint64_t n,
+                                                              const uint64_t* __restrict__ klo, Count cnt,
                                                               uint32_t word, uint32_t shift, uint32_t nb,
                                                               uint32_t* __restrict__ counts) {
   __shared__ uint32_t hist[256];
+  const uint64_t n = cnt.get();
   hist[threadIdx.x] = 0;
   __syncthreads();
   const uint64_t base = (uint64_t)blockIdx.x * kTile;
@@ -275,8 +470,9 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint64_t* __
 // __match_any_sync, per-warp digit counts give the offsets between warps.
 __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(
     const uint64_t* __restrict__ khi, const uint64_t* __restrict__ klo, const uint32_t* __restrict__ idx,
-    uint64_t n, uint32_t word, uint32_t shift, uint32_t nb, const uint32_t* __restrict__ offsets,
+    Count cnt, uint32_t word, uint32_t shift, uint32_t nb, const uint32_t* __restrict__ offsets,
     uint64_t* __restrict__ ohi, uint64_t* __restrict__ olo, uint32_t* __restrict__ oidx) {
+  const uint64_t n = cnt.get();
   __shared__ uint32_t wcnt[kRadixThreads / 32][256];
   __shared__ uint32_t goff[256];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -323,10 +519,15 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(
   }
 }
 
-__global__ void k_unique_flags(ConstEntryArrays in, const uint32_t* __restrict__ perm, uint64_t n,
+__global__ void k_unique_flags(ConstEntryArrays in, const uint32_t* __restrict__ perm, Count cnt,
                                uint32_t* __restrict__ flags) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+  const uint64_t n = cnt.get();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cnt.cap;
        i += (uint64_t)gridDim.x * blockDim.x) {
+    if (i >= n) {  // beyond a device count: nothing to keep (the scan runs to the bound)
+      flags[i] = 0;
+      continue;
+    }
     const uint32_t p = perm[i];
     uint32_t keep = 1;
     if (i > 0) {
@@ -337,9 +538,10 @@ __global__ void k_unique_flags(ConstEntryArrays in, const uint32_t* __restrict__
   }
 }
 
-__global__ void k_gather_kept(ConstEntryArrays in, const uint32_t* __restrict__ perm, uint64_t n,
+__global__ void k_gather_kept(ConstEntryArrays in, const uint32_t* __restrict__ perm, Count cnt,
                               const uint32_t* __restrict__ flags, const uint32_t* __restrict__ starts,
                               EntryArrays out, unsigned long long* kept) {
+  const uint64_t n = cnt.get();
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     if (!flags[i]) continue;
@@ -349,7 +551,7 @@ __global__ void k_gather_kept(ConstEntryArrays in, const uint32_t* __restrict__ 
     out.res_lo[at] = in.res_lo[p];
     out.res_hi[at] = in.res_hi[p];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *kept = starts[n];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *kept = starts[cnt.cap];
 }
 
 __global__ void k_or_reduce(ConstEntryArrays in, uint64_t n, unsigned long long* acc) {
@@ -369,7 +571,12 @@ __global__ void k_or_reduce(ConstEntryArrays in, uint64_t n, unsigned long long*
   }
 }
 
-__global__ void k_pack_records(ConstEntryArrays in, uint64_t n, uint32_t nbits, uint8_t* __restrict__ rec) {
+__global__ void k_copy_count(const unsigned long long* __restrict__ src, unsigned long long* __restrict__ dst) {
+  *dst = *src;
+}
+
+__global__ void k_pack_records(ConstEntryArrays in, Count cnt, uint32_t nbits, uint8_t* __restrict__ rec) {
+  const uint64_t n = cnt.get();
   const uint32_t w64 = (nbits + 63) / 64, w32 = (nbits + 31) / 32;
   const uint32_t rb = 16 * w64 + 4 * w32;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -423,24 +630,62 @@ void launch_scan_u32(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* sc
     cudaMemsetAsync(out, 0, 4, st);
     return;
   }
+  if (n <= 65536) {
+    k_scan_small<<<1, 1024, 0, st>>>(in, (uint32_t)n, out);
+    return;
+  }
   k_chunk_sums<<<nb, 256, 0, st>>>(in, n, scratch);
   k_scan_sums<<<1, 1024, 0, st>>>(scratch, nb);
   k_chunk_scan<<<nb, 1024, 0, st>>>(in, n, scratch, nb, out);
 }
 
-void launch_l2_quotients(ConstEntryArrays l, uint64_t count, uint32_t b1, uint32_t r2, uint64_t t_lo,
-                         uint64_t t_hi, int negate, uint64_t tau, uint64_t* key, cudaStream_t st) {
-  if (count == 0) return;
-  k_l2_quotients<<<blocks_for(count, 256), 256, 0, st>>>(l, count, b1, r2, t_lo, t_hi, negate, tau, key);
+void launch_l2_count_all(ConstEntryArrays left, uint64_t nl, const uint32_t* bucket_off, uint32_t r2,
+                         const MergeTargets& t, uint32_t* counts, cudaStream_t st,
+                         const MergeTargets* dt) {
+  k_l2_count_all<<<blocks_for(9 * nl, 256), 256, 0, st>>>(left, nl, bucket_off, (1u << r2) - 1u, t, dt,
+                                                          counts);
 }
 
-void launch_l1_parents(const uint32_t* triples, uint64_t ntriples, ConstEntryArrays x, ConstEntryArrays y,
+void launch_l2_bounds(const uint32_t* starts, uint64_t nl, uint32_t* bounds, cudaStream_t st) {
+  k_l2_bounds<<<1, 32, 0, st>>>(starts, nl, bounds);
+}
+
+void launch_l2_fill_all(ConstEntryArrays left, uint64_t nl, ConstEntryArrays right,
+                        const uint32_t* bucket_off, const uint32_t* order, uint32_t r2,
+                        const MergeTargets& t, uint32_t n, const uint32_t* starts, EntryArrays out,
+                        cudaStream_t st, const MergeTargets* dt, uint64_t cap) {
+  k_l2_fill_all<<<blocks_for(9 * nl, 128), 128, 0, st>>>(left, nl, right, bucket_off, order,
+                                                        (1u << r2) - 1u, t, dt, n, starts, cap, out);
+}
+
+void launch_canon_small(ConstEntryArrays raw, const Segments& seg, uint32_t nseg, EntryArrays out,
+                        unsigned long long* kept, cudaStream_t st, const uint32_t* dbounds,
+                        unsigned int* overflow, uint64_t cap) {
+  if (nseg == 0) return;
+  const size_t smem = kCanonSmallCap * (8 + 8 + 2 + 4);
+  allow_max_smem(reinterpret_cast<const void*>(k_canon_small));
+  k_canon_small<<<nseg, 1024, smem, st>>>(raw, seg, dbounds, cap, out, kept, overflow);
+}
+
+void prepare_attempt_kernels() {
+  allow_max_smem(reinterpret_cast<const void*>(k_canon_small));
+}
+
+void launch_l2_quotients(ConstEntryArrays l, Count count, uint32_t b1, uint32_t r2, uint64_t t_lo,
+                         uint64_t t_hi, int negate, uint64_t tau, uint64_t* key, cudaStream_t st,
+                         const uint32_t* doff, const uint64_t* dvals) {
+  if (count.cap == 0) return;
+  k_l2_quotients<<<blocks_for(count.cap, 256), 256, 0, st>>>(l, count, doff, b1, r2, t_lo, t_hi, negate,
+                                                             tau, dvals, key);
+}
+
+void launch_l1_parents(const uint32_t* triples, Count ntriples, ConstEntryArrays x, ConstEntryArrays y,
                        ConstEntryArrays z, uint32_t n, uint32_t expected_ones, EntryArrays out,
-                       unsigned long long* count, cudaStream_t st) {
+                       unsigned long long* count, cudaStream_t st, const uint32_t* doff) {
   cudaMemsetAsync(count, 0, 8, st);
-  if (ntriples == 0) return;
-  k_l1_parents<<<blocks_for(ntriples, 256), 256, 0, st>>>(triples, ntriples, x, y, z, n, expected_ones, out,
-                                                          count);
+  if (ntriples.cap == 0) return;
+  k_l1_parents<<<blocks_for(ntriples.cap, 256), 256, 0, st>>>(triples, ntriples, x, y, z, doff, n,
+                                                              expected_ones, out, count);
 }
 
 uint64_t radix_scratch_words(uint64_t count) {
@@ -451,8 +696,9 @@ uint64_t radix_scratch_words(uint64_t count) {
   return count * 10 + 2 * (cells + 1) + cells / kScanChunk + 64;
 }
 
-void radix_sort_entries(ConstEntryArrays in, uint64_t count, uint64_t vary_pos0, uint64_t vary_pos1,
+void radix_sort_entries(ConstEntryArrays in, Count cnt, uint64_t vary_pos0, uint64_t vary_pos1,
                         uint32_t* perm_out, uint32_t* scratch, cudaStream_t st) {
+  const uint64_t count = cnt.cap;
   if (count == 0) return;
   const uint32_t nb = (uint32_t)((count + kTile - 1) / kTile);
   const uint64_t cells = 256ull * nb;
@@ -470,15 +716,15 @@ void radix_sort_entries(ConstEntryArrays in, uint64_t count, uint64_t vary_pos0,
   uint32_t* counts = w32 + 2 * count;
   uint32_t* offsets = counts + cells + 1;
   uint32_t* scan_scratch = offsets + cells + 1;
-  k_radix_init<<<blocks_for(count, 256), 256, 0, st>>>(in, count, khi[0], klo[0], idx[0]);
+  k_radix_init<<<blocks_for(count, 256), 256, 0, st>>>(in, cnt, khi[0], klo[0], idx[0]);
   int cur = 0;
   for (uint32_t word = 0; word < 2; ++word) {  // word 0: pos1 (less significant), word 1: pos0
     const uint64_t vary = word == 0 ? vary_pos1 : vary_pos0;
     for (uint32_t shift = 0; shift < 64; shift += 8) {
       if (((vary >> shift) & 255u) == 0) continue;  // digit constant (zero) in every key
-      k_radix_hist<<<nb, kRadixThreads, 0, st>>>(khi[cur], klo[cur], count, word, shift, nb, counts);
+      k_radix_hist<<<nb, kRadixThreads, 0, st>>>(khi[cur], klo[cur], cnt, word, shift, nb, counts);
       launch_scan_u32(counts, cells, offsets, scan_scratch, st);
-      k_radix_scatter<<<nb, kRadixThreads, 0, st>>>(khi[cur], klo[cur], idx[cur], count, word, shift, nb,
+      k_radix_scatter<<<nb, kRadixThreads, 0, st>>>(khi[cur], klo[cur], idx[cur], cnt, word, shift, nb,
                                                     offsets, khi[1 - cur], klo[1 - cur], idx[1 - cur]);
       cur = 1 - cur;
     }
@@ -486,16 +732,17 @@ void radix_sort_entries(ConstEntryArrays in, uint64_t count, uint64_t vary_pos0,
   cudaMemcpyAsync(perm_out, idx[cur], count * 4, cudaMemcpyDeviceToDevice, st);
 }
 
-void launch_gather_unique(ConstEntryArrays in, const uint32_t* perm, uint64_t count, EntryArrays out,
+void launch_gather_unique(ConstEntryArrays in, const uint32_t* perm, Count cnt, EntryArrays out,
                           uint32_t* flags, uint32_t* starts, uint32_t* scratch, unsigned long long* kept,
                           cudaStream_t st) {
+  const uint64_t count = cnt.cap;
   if (count == 0) {
     cudaMemsetAsync(kept, 0, 8, st);
     return;
   }
-  k_unique_flags<<<blocks_for(count, 256), 256, 0, st>>>(in, perm, count, flags);
+  k_unique_flags<<<blocks_for(count, 256), 256, 0, st>>>(in, perm, cnt, flags);
   launch_scan_u32(flags, count, starts, scratch, st);
-  k_gather_kept<<<blocks_for(count, 256), 256, 0, st>>>(in, perm, count, flags, starts, out, kept);
+  k_gather_kept<<<blocks_for(count, 256), 256, 0, st>>>(in, perm, cnt, flags, starts, out, kept);
 }
 
 void launch_or_reduce(ConstEntryArrays in, uint64_t count, unsigned long long* acc, cudaStream_t st) {
@@ -504,9 +751,13 @@ void launch_or_reduce(ConstEntryArrays in, uint64_t count, unsigned long long* a
   k_or_reduce<<<blocks_for(count, 256), 256, 0, st>>>(in, count, acc);
 }
 
-void launch_pack_records(ConstEntryArrays in, uint64_t count, uint32_t n, uint8_t* records, cudaStream_t st) {
-  if (count == 0) return;
-  k_pack_records<<<blocks_for(count, 256), 256, 0, st>>>(in, count, n, records);
+void launch_copy_count(const unsigned long long* src, unsigned long long* dst, cudaStream_t st) {
+  k_copy_count<<<1, 1, 0, st>>>(src, dst);
+}
+
+void launch_pack_records(ConstEntryArrays in, Count count, uint32_t n, uint8_t* records, cudaStream_t st) {
+  if (count.cap == 0) return;
+  k_pack_records<<<blocks_for(count.cap, 256), 256, 0, st>>>(in, count, n, records);
 }
 
 }  // namespace tergpu

@@ -24,7 +24,8 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-__device__ __forceinline__ uint32_t yhash_of(uint32_t w) { return (w * 0x9E3779B1u) >> (32 - kYHashBits); }
+template <uint32_t BITS = kYHashBits>
+__device__ __forceinline__ uint32_t yhash_of(uint32_t w) { return (w * 0x9E3779B1u) >> (32 - BITS); }
 
 template <bool ALIGNED>
 __device__ __forceinline__ uint32_t window_of(uint64_t r, uint32_t mrb) {
@@ -34,8 +35,9 @@ __device__ __forceinline__ uint32_t window_of(uint64_t r, uint32_t mrb) {
   return static_cast<uint32_t>(r);
 }
 
-__global__ void k_hist(const uint64_t* __restrict__ key, uint64_t n, uint32_t fmask,
+__global__ void k_hist(const uint64_t* __restrict__ key, Count count, uint32_t fmask,
                        uint32_t* __restrict__ cnt) {
+  const uint64_t n = count.get();
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     atomicAdd(&cnt[static_cast<uint32_t>(key[i]) & fmask], 1u);
@@ -79,10 +81,11 @@ __global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t nfam, uint32_t
 }
 
 __global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __restrict__ key_hi,
-                          const uint32_t* __restrict__ id, uint64_t n, uint32_t fb,
+                          const uint32_t* __restrict__ id, Count count, uint32_t fb,
                           uint64_t fast_mask, uint32_t hi_mask, uint32_t* __restrict__ cursor,
                           uint64_t* __restrict__ res, uint8_t* __restrict__ hi,
                           uint32_t* __restrict__ out_id) {
+  const uint64_t n = count.get();
   const uint32_t fmask = (1u << fb) - 1u;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -476,7 +479,7 @@ __device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff,
                                               bool yshared) {
   const uint32_t wb = a.wb;
   for (uint32_t i = threadIdx.x; i < (1u << wb); i += blockDim.x) bm[i] = 0u;
-  for (uint32_t i = threadIdx.x; i < (1u << kYHashBits); i += blockDim.x) yhash[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < (1u << kY3HashBits); i += blockDim.x) yhash[i] = 0u;
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
     const uint32_t w = static_cast<uint32_t>(a.y.res[yoff + i]);  // mrb >= 32: the low 32 bits
@@ -484,10 +487,11 @@ __device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff,
     atomicOr(&bm[T & ((1u << wb) - 1u)], 1u << (31u - ((T >> 25) & 31u)));
     if (yshared) {
       ywin[i] = w;
-      uint32_t h = yhash_of(w);
+      uint32_t h = yhash_of<kY3HashBits>(w);
+      // at most kY3Cap entries in 2 * kY3Cap slots: an empty slot always exists
       while (atomicCAS(reinterpret_cast<unsigned short*>(&yhash[h]), (unsigned short)0,
                        static_cast<unsigned short>(i + 1u)) != 0) {
-        h = (h + 1u) & ((1u << kYHashBits) - 1u);
+        h = (h + 1u) & ((1u << kY3HashBits) - 1u);
       }
     }
   }
@@ -495,7 +499,7 @@ __device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff,
 }
 
 template <int R>
-__global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) {
+__global__ void __launch_bounds__(kSweep3Threads, 2) k_sweep3(const SweepArgs a) {
   static_assert(R == 4 || R == 8, "32 tests per mask");
   constexpr int QPC = 32 / R;  // A entries per 32-test mask
   extern __shared__ __align__(16) uint32_t smem[];
@@ -505,9 +509,9 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) 
   const uint32_t wb = a.wb;
   uint32_t* bm = smem;
   uint32_t* ywin = bm + (1u << wb);
-  uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kYCap);
-  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kYHashBits));
-  uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweepWarps * kQueueCap);
+  uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kY3Cap);
+  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kY3HashBits));
+  uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweep3Warps * kQueueCap);
 
   const uint32_t nloc = nfam / a.shards;
   const uint32_t u = a.shard + a.shards * (blockIdx.x % nloc);
@@ -519,7 +523,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) 
   if (s0 >= s1 || ny == 0u) return;  // uniform across the block
   const uint32_t yoff = a.y.off[u];
   const uint64_t mmask = a.mrb >= 64 ? ~0ull : ((1ull << a.mrb) - 1ull);
-  const bool yshared = ny <= kYCap;
+  const bool yshared = ny <= kY3Cap;
   if (threadIdx.x == 0) item_counter = 0u;
   build_target3(a, yoff, ny, bm, ywin, yhash, yshared);
 
@@ -552,12 +556,12 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) 
     const uint32_t qoff = a.q.off[s];
     const uint32_t xoff = a.x.off[t];
 
-    uint32_t x4[R];  // 4 * w_x
+    uint32_t nx4[R];  // -4 * w_x
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const uint32_t xi = xbase + r * 32u + lane;
       const uint32_t wx = xi < nx ? static_cast<uint32_t>(a.x.res[xoff + xi]) : 0u;
-      x4[r] = wx << 2;
+      nx4[r] = 0u - (wx << 2);
       xs[r * 32u + lane] = wx;
     }
     const uint32_t cadd = 0u - 4u * kap - 4u;  // 4 * ~(w + kap) = -4 w - 4 kap - 4
@@ -601,10 +605,10 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) 
             }
           };
           if (yshared) {
-            uint32_t h = yhash_of(w);
+            uint32_t h = yhash_of<kY3HashBits>(w);
             for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
               if (ywin[v - 1u] == w) check(v - 1u);
-              h = (h + 1u) & ((1u << kYHashBits) - 1u);
+              h = (h + 1u) & ((1u << kY3HashBits) - 1u);
             }
           } else {
             ++c_fall;
@@ -627,7 +631,10 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep3(const SweepArgs a) 
           const uint32_t c4 = static_cast<uint32_t>(e ? qq.y : qq.x) * 0xFFFFFFFCu + cadd;
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            const uint32_t t4 = c4 - x4[r];
+            // t4 = c4 - 4 w_x as an IMAD (multiplier `one` is 1 but opaque to the
+            // compiler), so the add runs on the FMA pipe beside the integer ALU work
+            uint32_t t4;
+            asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(t4) : "r"(nx4[r]), "r"(a.one), "r"(c4));
             const uint32_t w = *reinterpret_cast<const uint32_t*>(bmb + (t4 & amask));
             m = __funnelshift_l(__funnelshift_l(w, w, __umulhi(t4, 32u)), m, 1);
           }
@@ -831,9 +838,11 @@ __global__ void k_record_keys(const RecordKeyArgs a) {
   typedef unsigned __int128 u128;
   const u128 nmask = a.n >= 128 ? ~(u128)0 : ((((u128)1) << a.n) - 1);
   const u128 qmask = a.qbits >= 128 ? ~(u128)0 : ((((u128)1) << a.qbits) - 1);
-  const u128 child = ((u128)a.child_hi << 64) | a.child_lo;
-  const u128 tau = ((u128)a.tau_hi << 64) | a.tau_lo;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.count;
+  const uint64_t* v = a.dvals;
+  const u128 child = v != nullptr ? (((u128)v[1] << 64) | v[0]) : (((u128)a.child_hi << 64) | a.child_lo);
+  const u128 tau = v != nullptr ? (((u128)v[3] << 64) | v[2]) : (((u128)a.tau_hi << 64) | a.tau_lo);
+  const uint64_t count = a.count.get();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(a.records + i * a.record_bytes + a.res_offset);
     u128 r = 0;
@@ -848,9 +857,11 @@ __global__ void k_record_keys(const RecordKeyArgs a) {
 __global__ void k_authority(const AuthorityArgs a) {
   typedef unsigned __int128 u128;
   const u128 nmask = a.n >= 128 ? ~(u128)0 : ((((u128)1) << a.n) - 1);
-  const u128 root = ((u128)a.root_hi << 64) | a.root_lo;
+  const u128 root = a.droot != nullptr ? (((u128)a.droot[1] << 64) | a.droot[0])
+                                         : (((u128)a.root_hi << 64) | a.root_lo);
   unsigned long long c_res = 0, c_struct = 0, c_rule = 0;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.count;
+  const uint64_t count = a.count.get();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
        i += (uint64_t)gridDim.x * blockDim.x) {
     u128 sum = 0;
     uint64_t pos[3][2] = {{0, 0}, {0, 0}, {0, 0}}, neg[3][2] = {{0, 0}, {0, 0}, {0, 0}};
@@ -900,6 +911,14 @@ __global__ void k_authority(const AuthorityArgs a) {
   if (c_rule) atomicAdd(&a.counters[2], c_rule);
 }
 
+int grid_for(uint64_t n, int threads) {
+  uint64_t blocks = (n + threads - 1) / threads;
+  if (blocks > 148ull * 16ull) blocks = 148ull * 16ull;
+  return blocks == 0 ? 1 : static_cast<int>(blocks);
+}
+
+}  // namespace
+
 // Allows a kernel the device's whole opt-in shared memory, once per device and
 // kernel.  Setting the attribute per launch to that launch's size would race when
 // several host threads launch the same kernel with different sizes (the batch
@@ -920,17 +939,20 @@ void allow_max_smem(const void* kernel) {
                        optin - static_cast<int>(fa.sharedSizeBytes));
 }
 
-int grid_for(uint64_t n, int threads) {
-  uint64_t blocks = (n + threads - 1) / threads;
-  if (blocks > 148ull * 16ull) blocks = 148ull * 16ull;
-  return blocks == 0 ? 1 : static_cast<int>(blocks);
+void prepare_root_kernels() {
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep<true>));
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep<false>));
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep2<true, 8>));
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep2<false, 8>));
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep3<8>));
+  allow_max_smem(reinterpret_cast<const void*>(k_family_arrange));
+  allow_max_smem(reinterpret_cast<const void*>(k_family_sort<true>));
+  allow_max_smem(reinterpret_cast<const void*>(k_family_sort<false>));
 }
 
-}  // namespace
-
-void launch_hist(const uint64_t* key, uint64_t n, uint32_t fmask, uint32_t* cnt, cudaStream_t st) {
-  if (n == 0) return;
-  k_hist<<<grid_for(n, 256), 256, 0, st>>>(key, n, fmask, cnt);
+void launch_hist(const uint64_t* key, Count n, uint32_t fmask, uint32_t* cnt, cudaStream_t st) {
+  if (n.cap == 0) return;
+  k_hist<<<grid_for(n.cap, 256), 256, 0, st>>>(key, n, fmask, cnt);
 }
 
 void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor,
@@ -938,11 +960,11 @@ void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cu
   k_scan<<<1, 1024, 0, st>>>(cnt, nfam, off, cursor);
 }
 
-void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, uint64_t n,
+void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, Count n,
                     uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
                     uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st) {
-  if (n == 0) return;
-  k_scatter<<<grid_for(n, 256), 256, 0, st>>>(key_lo, key_hi, id, n, fb, fast_mask, hi_mask, cursor,
+  if (n.cap == 0) return;
+  k_scatter<<<grid_for(n.cap, 256), 256, 0, st>>>(key_lo, key_hi, id, n, fb, fast_mask, hi_mask, cursor,
                                              res, hi, out_id);
 }
 
@@ -981,10 +1003,13 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
 }
 
 void launch_sweep3(const SweepArgs& a, cudaStream_t st) {
-  const size_t smem = sweep_smem_bytes(a.wb) + static_cast<size_t>(kSweepWarps) * 32 * 8 * 4;
+  const size_t smem = (static_cast<size_t>(1) << a.wb) * 4 + kY3Cap * 4 +
+                      (static_cast<size_t>(1) << kY3HashBits) * 2 +
+                      static_cast<size_t>(kSweep3Warps) * kQueueCap * sizeof(uint2) +
+                      static_cast<size_t>(kSweep3Warps) * 32 * 8 * 4;
   const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
   allow_max_smem(reinterpret_cast<const void*>(k_sweep3<8>));
-  k_sweep3<8><<<grid, kSweepThreads, smem, st>>>(a);
+  k_sweep3<8><<<grid, kSweep3Threads, smem, st>>>(a);
 }
 
 void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
@@ -1008,13 +1033,13 @@ void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t
 }
 
 void launch_record_keys(const RecordKeyArgs& a, cudaStream_t st) {
-  if (a.count == 0) return;
-  k_record_keys<<<grid_for(a.count, 256), 256, 0, st>>>(a);
+  if (a.count.cap == 0) return;
+  k_record_keys<<<grid_for(a.count.cap, 256), 256, 0, st>>>(a);
 }
 
 void launch_authority(const AuthorityArgs& a, cudaStream_t st) {
-  if (a.count == 0) return;
-  k_authority<<<grid_for(a.count, 128), 128, 0, st>>>(a);
+  if (a.count.cap == 0) return;
+  k_authority<<<grid_for(a.count.cap, 128), 128, 0, st>>>(a);
 }
 
 }  // namespace tergpu

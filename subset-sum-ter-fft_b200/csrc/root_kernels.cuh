@@ -16,6 +16,8 @@
 
 #include <cstdint>
 
+#include "count.cuh"
+
 namespace tergpu {
 
 constexpr int kSweepThreads = 256;
@@ -24,6 +26,13 @@ constexpr int kQueueCap = 128;         // survivor slots per warp
 constexpr uint32_t kYHashBits = 13;    // shared exact-lookup table: 8192 slots of 16 bits
 constexpr uint32_t kYCap = 4096;       // D-family entries the shared table takes
 constexpr uint32_t kSortCap = 4096;    // B-family entries the in-family sort takes
+// v3: 12 warps per CTA (two CTAs per SM at 19 filter bits: 24 warps) and a
+// 4096-slot exact-lookup table (D families of up to 2048 entries; the tuning
+// aims at about 1,700, larger families fall back to a scan of the family)
+constexpr int kSweep3Threads = 384;
+constexpr int kSweep3Warps = kSweep3Threads / 32;
+constexpr uint32_t kY3HashBits = 12;
+constexpr uint32_t kY3Cap = 2048;
 
 struct ListView {
   const uint64_t* res;
@@ -38,6 +47,7 @@ struct SweepArgs {
   const uint8_t* cells;     // 4096 bytes over the low 6 key bits, or null
   uint32_t fb;              // family bits
   uint32_t s_split;         // CTAs per target family
+  uint32_t one;             // 1 (an IMAD multiplier the compiler cannot fold)
   uint32_t shard;           // this call joins the target families u == shard (mod shards)
   uint32_t shards;          // power of two, 1..64 (1: the whole root)
   uint32_t wb;              // log2 of filter words (filter bits = wb + 5)
@@ -57,11 +67,18 @@ enum Counter {
   kCounters = 8
 };
 
+// Allows a kernel the device's whole opt-in dynamic shared memory, once per
+// device and kernel (root_kernels.cu); launchers call it before a launch that
+// needs more than the default 48 KB.
+void allow_max_smem(const void* kernel);
+// allow_max_smem for every root kernel that needs it (before a graph capture).
+void prepare_root_kernels();
+
 // Host-callable launchers (root_kernels.cu).
-void launch_hist(const uint64_t* key, uint64_t n, uint32_t fmask, uint32_t* cnt, cudaStream_t st);
+void launch_hist(const uint64_t* key, Count n, uint32_t fmask, uint32_t* cnt, cudaStream_t st);
 void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor,
                  cudaStream_t st);
-void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, uint64_t n,
+void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, Count n,
                     uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
                     uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st);
 void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters, int slot,
@@ -91,7 +108,7 @@ void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t
 // list 2 turned into d = tau - q_C.
 struct RecordKeyArgs {
   const uint8_t* records;
-  uint64_t count;
+  Count count;
   uint32_t record_bytes;
   uint32_t res_offset;     // 16 * W64
   uint32_t words32;
@@ -101,6 +118,8 @@ struct RecordKeyArgs {
   int negate;              // list 2
   uint64_t* key_lo;
   uint8_t* key_hi;
+  const uint64_t* dvals;   // device {child_lo, child_hi, tau_lo, tau_hi} replacing the fields
+                           // above when not null (a captured graph's per-attempt values)
 };
 void launch_record_keys(const RecordKeyArgs& a, cudaStream_t st);
 
@@ -110,8 +129,9 @@ struct AuthorityArgs {
   const uint8_t* records[3];
   uint32_t record_bytes, res_offset, words32, words64, n;
   uint64_t root_lo, root_hi;
+  const uint64_t* droot;   // device {lo, hi} replacing root_lo / root_hi when not null
   const uint32_t* triples;
-  uint64_t count;
+  Count count;
   uint8_t* flags;
   unsigned long long* counters;  // [0] residue [1] structural [2] root rule
 };

@@ -99,6 +99,7 @@ void release_buffers(Workspace& w) {
 void destroy_workspace(Workspace& w) {
   release_buffers(w);
   if (w.stream) cudaStreamSynchronize(w.stream);
+  w.plans.clear();
   if (w.start) cudaEventDestroy(w.start);
   if (w.mid) cudaEventDestroy(w.mid);
   if (w.stop) cudaEventDestroy(w.stop);
@@ -194,6 +195,81 @@ uint32_t checked_shards(uint32_t index, uint32_t count) {
   return n;
 }
 
+uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu, cudaEvent_t mid,
+                      cudaStream_t st, uint32_t* launches) {
+  const uint32_t Q = j.quotient_bits;
+  const uint32_t F = std::min<uint32_t>(Q, 64);
+  const uint32_t hi_bits = Q - F;
+  const uint32_t nfam = 1u << tu.fb;
+  const uint64_t fast_mask = F >= 64 ? ~0ull : ((1ull << F) - 1ull);
+  ListView views[3];
+  check(cudaMemsetAsync(b.counters, 0, kCounters * 8, st), "memset");
+  for (int l = 0; l < 3; ++l) {
+    check(cudaMemsetAsync(b.cnt[l], 0, nfam * 4ull, st), "memset");
+    launch_hist(j.key_lo[l], j.count[l], nfam - 1, b.cnt[l], st);
+    launch_scan(b.cnt[l], nfam, b.off[l], b.cur[l], st);
+    launch_scatter(j.key_lo[l], j.key_hi[l], j.id[l], j.count[l], tu.fb, fast_mask,
+                   hi_bits ? ((1u << hi_bits) - 1u) : 0u, b.cur[l], b.res[l], b.hi[l], b.id[l], st);
+    views[l] = ListView{b.res[l], b.hi[l], b.id[l], b.off[l], b.cnt[l]};
+    *launches += (j.count[l].cap != 0 ? 2 : 0) + 1;
+  }
+  launch_max_family(b.cnt[0], nfam, b.counters, kMaxQ, st);
+  launch_max_family(b.cnt[1], nfam, b.counters, kMaxX, st);
+  *launches += 2;
+  // v3 needs full 32-bit windows (mrb >= 32); below that the B-in-registers
+  // sweep (v2) runs, exact for any family order.
+  const uint32_t main_variant = tu.variant == 3 && F - tu.fb < 32 ? 2u : tu.variant;
+  if (main_variant == 3 && j.count[1].cap != 0) {
+    // B families in lane slots of distinct residual classes mod 32 (bank-free probes)
+    launch_family_arrange(b.res[1], b.hi[1], b.id[1], b.off[1], b.cnt[1], nfam, st);
+    *launches += 1;
+  } else if (main_variant == 2 && j.count[1].cap != 0) {
+    // B families sorted by the top filter-word bits of the full-width window
+    launch_family_sort(b.res[1], b.hi[1], b.id[1], b.off[1], b.cnt[1], nfam, F - tu.fb, tu.sort_bits, st);
+    *launches += 1;
+  }
+  auto sweep = [&](const SweepArgs& sa) {
+    if (main_variant == 3 && sa.mrb >= 32) {
+      launch_sweep3(sa, st);
+    } else if (main_variant == 1) {
+      launch_sweep(sa, sa.mrb < 32, st);
+    } else {
+      launch_sweep2(sa, sa.mrb < 32, st);
+    }
+  };
+  check(cudaGetLastError(), "partition launch");
+  if (mid != nullptr) check(cudaEventRecord(mid, st), "event");
+  SweepArgs a{};
+  a.q = views[0];
+  a.x = views[1];
+  a.y = views[2];
+  a.cells = j.cells;
+  a.fb = tu.fb;
+  a.s_split = tu.s_split;
+  a.one = 1;
+  a.shard = j.shard;
+  a.shards = j.shards;
+  a.wb = tu.wb;
+  a.rb = F - tu.fb;
+  a.hi_bits = hi_bits;
+  a.triples = b.triples;
+  a.cap = j.cap;
+  a.counters = b.counters;
+  if (j.main_sweep) {
+    a.project = 0;
+    a.mrb = F - tu.fb;
+    sweep(a);
+    *launches += 1;
+  }
+  if (j.projected_bits != 0) {
+    a.project = 1;
+    a.mrb = j.projected_bits - tu.fb;
+    sweep(a);
+    *launches += 1;
+  }
+  return main_variant;
+}
+
 // ---- autotuner: per root shape, the fastest (family bits, filter bits, sweep
 // variant) among the neighbours of the size-based choice, timed as device time
 // (partition + sweep) on one 64th of the root's target families (shard 0 of
@@ -286,7 +362,6 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   JoinResult r;
   const uint32_t Q = in.quotient_bits;
   const uint32_t F = std::min<uint32_t>(Q, 64);
-  const uint32_t hi_bits = Q - F;
   r.tuning = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, in.family_bits,
                            in.filter_bits, in.sweep_variant, in.shards);
   const Tuning& tu = r.tuning;
@@ -297,7 +372,6 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     throw Failure{TERGPU_INVALID_INPUT};
   }
   const uint32_t nfam = 1u << tu.fb;
-  const uint64_t fast_mask = F >= 64 ? ~0ull : ((1ull << F) - 1ull);
   const uint64_t need = input_bytes + partition_bytes(in.count, tu.fb) +
                         (in.count_only ? 0 : in.capacity * 12) + 4096 + 64;
   r.device_bytes = need;
@@ -307,7 +381,6 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     throw Failure{TERGPU_RESOURCE_LIMIT};
   }
   cudaStream_t st = in.stream;
-  ListView views[3];
   uint64_t* res[3];
   uint8_t* hi[3];
   uint32_t* ids[3];
@@ -330,70 +403,32 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     d_cells = c;
   }
   check(cudaEventRecord(w.start, st), "event");
-  check(cudaMemsetAsync(counters, 0, kCounters * 8, st), "memset");
+  JoinBuffers jb{};
   for (int l = 0; l < 3; ++l) {
-    check(cudaMemsetAsync(cnt[l], 0, nfam * 4ull, st), "memset");
-    launch_hist(in.key_lo[l], in.count[l], nfam - 1, cnt[l], st);
-    launch_scan(cnt[l], nfam, off[l], cur[l], st);
-    launch_scatter(in.key_lo[l], in.key_hi[l], in.id[l], in.count[l], tu.fb, fast_mask,
-                   hi_bits ? ((1u << hi_bits) - 1u) : 0u, cur[l], res[l], hi[l], ids[l], st);
-    views[l] = ListView{res[l], hi[l], ids[l], off[l], cnt[l]};
-    r.launches += (in.count[l] != 0 ? 2 : 0) + 1;
+    jb.res[l] = res[l];
+    jb.hi[l] = hi[l];
+    jb.id[l] = ids[l];
+    jb.cnt[l] = cnt[l];
+    jb.off[l] = off[l];
+    jb.cur[l] = cur[l];
   }
-  launch_max_family(cnt[0], nfam, counters, kMaxQ, st);
-  launch_max_family(cnt[1], nfam, counters, kMaxX, st);
-  r.launches += 2;
-  // v3 needs full 32-bit windows (mrb >= 32); below that the B-in-registers
-  // sweep (v2) runs, exact for any family order.
-  const uint32_t main_variant = tu.variant == 3 && F - tu.fb < 32 ? 2u : tu.variant;
-  r.tuning.variant = main_variant;
-  if (main_variant == 3 && in.count[1] != 0) {
-    // B families in lane slots of distinct residual classes mod 32 (bank-free probes)
-    launch_family_arrange(res[1], hi[1], ids[1], off[1], cnt[1], nfam, st);
-    r.launches += 1;
-  } else if (main_variant == 2 && in.count[1] != 0) {
-    // B families sorted by the top filter-word bits of the full-width window
-    launch_family_sort(res[1], hi[1], ids[1], off[1], cnt[1], nfam, F - tu.fb, tu.sort_bits, st);
-    r.launches += 1;
+  jb.counters = counters;
+  jb.triples = d_triples;
+  JoinWork jw{};
+  for (int l = 0; l < 3; ++l) {
+    jw.key_lo[l] = in.key_lo[l];
+    jw.key_hi[l] = in.key_hi[l];
+    jw.id[l] = in.id[l];
+    jw.count[l] = Count(in.count[l]);
   }
-  auto sweep = [&](const SweepArgs& sa) {
-    if (main_variant == 3 && sa.mrb >= 32) {
-      launch_sweep3(sa, st);
-    } else if (main_variant == 1) {
-      launch_sweep(sa, sa.mrb < 32, st);
-    } else {
-      launch_sweep2(sa, sa.mrb < 32, st);
-    }
-  };
-  check(cudaGetLastError(), "partition launch");
-  check(cudaEventRecord(w.mid, st), "event");
-  SweepArgs a{};
-  a.q = views[0];
-  a.x = views[1];
-  a.y = views[2];
-  a.cells = d_cells;
-  a.fb = tu.fb;
-  a.s_split = tu.s_split;
-  a.shard = in.shard;
-  a.shards = in.shards;
-  a.wb = tu.wb;
-  a.rb = F - tu.fb;
-  a.hi_bits = hi_bits;
-  a.triples = d_triples;
-  a.cap = in.count_only ? 0 : in.capacity;
-  a.counters = counters;
-  if (!in.count_only || in.projected_bits == 0) {
-    a.project = 0;
-    a.mrb = F - tu.fb;
-    sweep(a);
-    r.launches += 1;
-  }
-  if (in.projected_bits != 0) {
-    a.project = 1;
-    a.mrb = in.projected_bits - tu.fb;
-    sweep(a);
-    r.launches += 1;
-  }
+  jw.quotient_bits = Q;
+  jw.cells = d_cells;
+  jw.shard = in.shard;
+  jw.shards = in.shards;
+  jw.cap = in.count_only ? 0 : in.capacity;
+  jw.main_sweep = !in.count_only || in.projected_bits == 0;
+  jw.projected_bits = in.projected_bits;
+  r.tuning.variant = enqueue_join(jb, jw, tu, w.mid, st, &r.launches);
   check(cudaGetLastError(), "sweep launch");
   check(cudaEventRecord(w.stop, st), "event");
   unsigned long long hc[kCounters];
@@ -759,6 +794,7 @@ uint64_t tergpu_fnv1a(const void* bytes, uint64_t size, uint64_t state) {
 }
 
 void tergpu_release(void) {
+  tergpu::release_slots();
   std::lock_guard<std::mutex> lock(tergpu::g_mu);
   for (auto& w : tergpu::g_ws) {
     std::lock_guard<std::mutex> inner(w->mu);

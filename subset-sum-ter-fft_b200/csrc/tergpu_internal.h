@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include "count.cuh"
 #include "tergpu.h"
 
 #include <cstdint>
@@ -42,6 +43,9 @@ struct Workspace {
   // spinning: many slots share the host cores); the shared workspace spins
   cudaEvent_t sync_event = nullptr;
   std::map<int, Buffer> buf;
+  // captured attempt graphs by shape (n), with buffers of their own: kept across
+  // calls and across release_buffers, freed by destroy_workspace
+  std::map<uint32_t, std::shared_ptr<void>> plans;
   std::mutex mu;
 };
 
@@ -59,6 +63,12 @@ std::unique_ptr<Workspace> make_workspace(int device, bool blocking = false);
 void destroy_workspace(Workspace& w);
 // Returns a workspace's buffers to the device pool (stream-ordered, no wait).
 void release_buffers(Workspace& w);
+
+// The batch engine's slot workspaces: kept between calls with their graph
+// plans (a server's slots stay warm), freed by release_slots (tergpu_release).
+std::unique_ptr<Workspace> take_slot(int device);
+void give_slot(std::unique_ptr<Workspace> w);
+void release_slots();
 
 // Grow-only device buffer in slot `slot` of the workspace.
 void* ensure_bytes(Workspace& w, int slot, size_t bytes);
@@ -106,6 +116,44 @@ struct JoinResult {
 // count (count 0 means 1).  Throws Failure(InvalidInput) unless the count is a
 // power of two in [1, 64] and the index is below it.
 uint32_t checked_shards(uint32_t index, uint32_t count);
+
+// Family bits, filter bits, CTAs per family and variant of one join from its
+// list sizes (requested values win when not zero).
+Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
+                     uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards);
+
+// Device buffers of one join, sized by the caller for the lists' count bounds:
+// per list res / hi / id (bound + 2^fb + 16 entries), cnt / off / cur
+// (2^fb + 1 words), the counters (kCounters) and the triples (3 * cap words).
+struct JoinBuffers {
+  uint64_t* res[3];
+  uint8_t* hi[3];
+  uint32_t* id[3];
+  uint32_t *cnt[3], *off[3], *cur[3];
+  unsigned long long* counters;
+  uint32_t* triples;
+};
+
+// The inputs of one join: keys per list with host or device counts.
+struct JoinWork {
+  const uint64_t* key_lo[3];
+  const uint8_t* key_hi[3];
+  const uint32_t* id[3];
+  Count count[3];
+  uint32_t quotient_bits;
+  const uint8_t* cells;  // device or null
+  uint32_t shard, shards;
+  uint64_t cap;          // triples written (0: count only)
+  bool main_sweep;       // the full-width sweep (false: projected counts only)
+  uint32_t projected_bits;
+};
+
+// The join's device work on `st` -- partition, family layout, sweep(s) -- with
+// no host synchronization (a captured graph can hold it): the triples count
+// and the other counters stay in b.counters.  Records `mid` after the
+// partition when not null.  Returns the sweep variant that ran.
+uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu, cudaEvent_t mid,
+                      cudaStream_t st, uint32_t* launches);
 
 // Partition + sweep on keys already on the device (throws Failure).
 JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes);

@@ -61,6 +61,7 @@ class FullTerConfig:
     device: int = 0
     export_l1_capacity: int = 0   # > 0: return the last attempt's L1 lists as a Snapshot
     capture_only: bool = False    # stop after L1 (the device stream_full_ter_root_lists)
+    no_graph: bool = False        # n = 36 / 72: run stage by stage instead of one graph per attempt
 
 
 @dataclass
@@ -111,7 +112,7 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     target = np.ascontiguousarray(instance.target_le, dtype=np.uint64)
     ain = AttemptIn()
     ain.n = instance.n
-    ain.flags = 1 if config.capture_only else 0
+    ain.flags = (1 if config.capture_only else 0) | (4 if config.no_graph else 0)
     ain.values_le = values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.target_le = target.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.seed = config.seed & (2**64 - 1)

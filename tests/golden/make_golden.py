@@ -127,6 +127,27 @@ def whole_root_plants(tmp: Path):
     return out
 
 
+def seed_roots(tmp: Path):
+    """The six published n=108 roots (benchmark instance, attempt 0): the
+    reference's capture sizes and its frozen ARWLF over the declared 16-cell
+    sample with 32-bit projected counts (about 3 minutes per seed, in parallel)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(seed):
+        snap = tmp / f"s108_{seed:x}.snap"
+        cap = O.ref_run("capture", 108, seed, 0, "auth", snap, timeout=3600)[0]
+        row = O.ref_run("snaproot", snap, "arwlf", 16, 32, timeout=3600)[0]
+        snap.unlink()
+        keep = ("triples", "triple_sum", "triple_xor", "triple_sum2", "residue", "residue_sum",
+                "structural", "witnesses", "pairs", "projected_hits")
+        return {"seed": seed, "level1": cap["level1"], "level2": cap["level2"],
+                "arwlf16": {k: row[k] for k in keep}}
+
+    seeds = [0x1001, 0x2003, 0x3007, 0x4001, 0x5003, 0x6007]
+    with ThreadPoolExecutor(max_workers=6) as pool:
+        return list(pool.map(one, seeds))
+
+
 SECTIONS = {
     "n36_attempts": lambda tmp: n36_attempts(),
     "n36_snapshot": n36_snapshot,
@@ -134,6 +155,7 @@ SECTIONS = {
     "n72_roots": n72_roots,
     "root_reports": root_reports,
     "whole_root_plants": whole_root_plants,
+    "seed_roots": seed_roots,
 }
 
 

@@ -118,3 +118,16 @@ def test_attempt_statuses():
     bad = instance.benchmark_instance(48, 5)
     res = attempt.solve_full_ter(bad, attempt.FullTerConfig(seed=5))
     assert res.status == _abi.INVALID_CONFIGURATION
+
+
+@pytest.mark.parametrize("n,seed,first,count", [(36, ANCHOR_SEED, 0, 8), (36, 358, 0, 2),
+                                               (72, ANCHOR_SEED, 0, 3), (72, 0x7201, 19, 4)])
+def test_graph_attempts_equal_stage_by_stage(n, seed, first, count):
+    """n = 36 and 72 run each attempt as one captured CUDA graph; the same
+    attempts stage by stage give the same levels, counts, status and witness."""
+    from tergpu import batch
+
+    inst, graphed = _attempt(n, seed, first, count)
+    _, staged = _attempt(n, seed, first, count, no_graph=True)
+    assert batch.same_result(graphed, staged)
+    assert graphed.attempts and graphed.attempts[0]["level1"] == staged.attempts[0]["level1"]
