@@ -385,9 +385,11 @@ void size_plan(GraphPlan* g, uint32_t n, uint32_t r1, uint32_t r2, uint64_t l3) 
   const uint32_t qbits = b1 - r2;
   const uint32_t fb_l2 = std::max<uint32_t>(6, qbits > 17 ? qbits - 17 : 6);
   const uint32_t filt_l2 = std::clamp<uint32_t>(qbits - fb_l2, 10, 20);
-  g->tu_l2 = choose_tuning(g->cap_l2, g->cap_l2, qbits, 0, fb_l2, filt_l2, 0, 1);
+  const double l2 = (double)l3 * l3 / std::ldexp(1.0, r2);  // expected L2 list size
+  g->tu_l2 = choose_tuning(g->cap_l2, g->cap_l2, qbits, 0, fb_l2, filt_l2, 0, 1, (uint64_t)l2);
   const uint32_t qroot = n - r1;
-  g->tu_root = choose_tuning((uint64_t)l1, (uint64_t)l1, std::min<uint32_t>(qroot, 64), 0, 0, 0, 0, 1);
+  g->tu_root = choose_tuning((uint64_t)l1, (uint64_t)l1, std::min<uint32_t>(qroot, 64), 0, 0, 0, 0, 1,
+                             (uint64_t)l1);
   const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
   const uint32_t rb = 16 * w64 + 4 * w32;
   const uint32_t nbk = 1u << r2;

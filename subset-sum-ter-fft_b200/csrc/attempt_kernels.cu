@@ -264,37 +264,67 @@ __global__ void __launch_bounds__(1024) k_canon_small(ConstEntryArrays raw, Segm
 }
 
 // One CTA of 1024 threads: exclusive scan of n <= 65536 values; out[n] = total.
+// Tiles of 8192 values pass through shared memory, so global reads and writes
+// are coalesced; each thread scans 8 consecutive values of a tile (one pad
+// word per 32 keeps those reads free of bank conflicts).
 __global__ void __launch_bounds__(1024) k_scan_small(const uint32_t* __restrict__ in, uint32_t n,
                                                      uint32_t* __restrict__ out) {
+  constexpr uint32_t kPer = 8, kTileN = 1024 * kPer;
+  __shared__ uint32_t tile[kTileN + kTileN / 32];
   __shared__ uint32_t warp_tot[32];
-  const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
-  const uint32_t begin = threadIdx.x * per, end = min(n, begin + per);
-  uint32_t local = 0;
-  for (uint32_t i = begin; i < end; ++i) local += in[i];
-  uint32_t v = local;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint32_t o = __shfl_up_sync(kFull, v, d);
-    if (lane >= (uint32_t)d) v += o;
-  }
-  if (lane == 31) warp_tot[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < blockDim.x / 32 ? warp_tot[lane] : 0;
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t o = __shfl_up_sync(kFull, w, d);
-      if (lane >= (uint32_t)d) w += o;
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < n; base += kTileN) {
+    const uint32_t m = min(kTileN, n - base);
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      const uint32_t i = threadIdx.x + 1024u * k;
+      tile[i + (i >> 5)] = i < m ? in[base + i] : 0u;
     }
-    warp_tot[lane] = w;
+    __syncthreads();
+    uint32_t v[kPer];
+    uint32_t local = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      const uint32_t i = threadIdx.x * kPer + k;
+      v[k] = tile[i + (i >> 5)];
+      local += v[k];
+    }
+    uint32_t x = local;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(kFull, x, d);
+      if (lane >= (uint32_t)d) x += o;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = warp_tot[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(kFull, w, d);
+        if (lane >= (uint32_t)d) w += o;
+      }
+      warp_tot[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = carry + x - local + (warp > 0 ? warp_tot[warp - 1] : 0u);
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      const uint32_t i = threadIdx.x * kPer + k;
+      tile[i + (i >> 5)] = run;
+      run += v[k];
+    }
+    carry += warp_tot[31];
+    __syncthreads();
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+      const uint32_t i = threadIdx.x + 1024u * k;
+      if (i < m) out[base + i] = tile[i + (i >> 5)];
+    }
+    __syncthreads();  // the next tile reuses tile[] and warp_tot[]
   }
-  __syncthreads();
-  uint32_t run = v - local + (warp > 0 ? warp_tot[warp - 1] : 0);
-  for (uint32_t i = begin; i < end; ++i) {
-    const uint32_t c = in[i];
-    out[i] = run;
-    run += c;
-  }
-  if (threadIdx.x == blockDim.x - 1) out[n] = run;
+  if (threadIdx.x == 0) out[n] = carry;
 }
 
 // ---- generic exclusive scan of uint32 (three kernels) ----------------------

@@ -499,7 +499,7 @@ __device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff,
 }
 
 template <int R>
-__global__ void __launch_bounds__(kSweep3Threads, 2) k_sweep3(const SweepArgs a) {
+__global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a) {
   static_assert(R == 4 || R == 8, "32 tests per mask");
   constexpr int QPC = 32 / R;  // A entries per 32-test mask
   extern __shared__ __align__(16) uint32_t smem[];

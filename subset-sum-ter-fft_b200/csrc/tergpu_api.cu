@@ -134,8 +134,11 @@ uint32_t ceil_log2(uint64_t v) {
 // a B family has entries (measured best at n=108: 19 filter bits, false-pass
 // rate |D_u| / 2^(wb+5) ~ 0.3 %); narrower filters make the probes of 32
 // consecutive sorted B entries nearly conflict-free but pass too many pairs.
+// v3 (bank-free probes, one CTA per SM): 16x as many words (20 filter bits at
+// n=108, false-pass rate ~ 0.16 %).
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
-                     uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards) {
+                     uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards,
+                     uint64_t n_q) {
   Tuning t;
   t.variant = variant == 0 ? 3u : variant;
   const bool v2 = t.variant != 1;
@@ -154,6 +157,8 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   const uint64_t avg_x = std::max<uint64_t>(1, n_x >> t.fb);
   if (filter_req != 0) {
     t.wb = filter_req - 5;
+  } else if (t.variant == 3) {
+    t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 4, 6, 15);
   } else if (v2) {
     t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 3, 6, 14);
   } else {
@@ -162,8 +167,12 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   t.sort_bits = std::min<uint32_t>(t.wb, 12);
   const uint32_t nfam = 1u << t.fb;
   const uint32_t nloc = std::max<uint32_t>(1, nfam / shards);  // target families per shard
-  const uint32_t target_ctas = 148 * 2 * 8;
-  t.s_split = std::clamp<uint32_t>((target_ctas + nloc - 1) / nloc, 1, nfam);
+  uint64_t target_ctas = 148 * (t.variant == 3 ? 1 : 2) * 8;  // about 8 waves of resident CTAs
+  if (n_q != 0) {
+    const double pairs = static_cast<double>(n_q) * static_cast<double>(n_x) / shards;
+    target_ctas = std::min<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / (1u << 20)) + 1);
+  }
+  t.s_split = static_cast<uint32_t>(std::clamp<uint64_t>((target_ctas + nloc - 1) / nloc, 1, nfam));
   return t;
 }
 
@@ -294,7 +303,7 @@ uint32_t size_bucket(uint64_t n) {
 
 Tuned autotune(Workspace& w, const JoinInput& in, uint64_t input_bytes, float* spent_ms) {
   const uint32_t F = std::min<uint32_t>(in.quotient_bits, 64);
-  const Tuning base = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, 0, 0, 3, 1);
+  const Tuning base = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, 0, 0, 3, 1, in.count[0]);
   Tuned best;
   float best_ms = 0;
   *spent_ms = 0;
@@ -363,7 +372,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   const uint32_t Q = in.quotient_bits;
   const uint32_t F = std::min<uint32_t>(Q, 64);
   r.tuning = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, in.family_bits,
-                           in.filter_bits, in.sweep_variant, in.shards);
+                           in.filter_bits, in.sweep_variant, in.shards, in.count[0]);
   const Tuning& tu = r.tuning;
   checked_shards(in.shard, in.shards);
   if (tu.fb < 6 || tu.fb > 16 || tu.fb + 2 > F || tu.wb < 5 || tu.wb > 15 ||

@@ -118,9 +118,12 @@ struct JoinResult {
 uint32_t checked_shards(uint32_t index, uint32_t count);
 
 // Family bits, filter bits, CTAs per family and variant of one join from its
-// list sizes (requested values win when not zero).
+// list sizes (requested values win when not zero).  With the A list size n_q,
+// small joins get fewer CTAs (about 2^20 pairs each at least), so a join of a
+// few million pairs does not occupy every SM with CTAs that mostly build filters.
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
-                     uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards);
+                     uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards,
+                     uint64_t n_q = 0);
 
 // Device buffers of one join, sized by the caller for the lists' count bounds:
 // per list res / hi / id (bound + 2^fb + 16 entries), cnt / off / cur
