@@ -498,10 +498,15 @@ __device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff,
   __syncthreads();
 }
 
+// Compile-time row count of a sweep chunk (selects the unrolled probe loop).
+template <int V>
+struct RowsTag {
+  static constexpr int value = V;
+};
+
 template <int R>
 __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a) {
-  static_assert(R == 4 || R == 8, "32 tests per mask");
-  constexpr int QPC = 32 / R;  // A entries per 32-test mask
+  static_assert(R >= 1 && R <= 8, "at most 8 rows of B entries per chunk");
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint32_t item_counter;
   const uint32_t nfam = 1u << a.fb;
@@ -556,99 +561,120 @@ __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a)
     const uint32_t qoff = a.q.off[s];
     const uint32_t xoff = a.x.off[t];
 
-    uint32_t nx4[R];  // -4 * w_x
+    // Rows of 32 B entries this chunk holds: the last chunk of a family runs
+    // with only its occupied rows (RR of them, QP A entries per mask of
+    // QP * RR <= 32 tests; test k sits at bit kTests - 1 - k).  QP <= 16: the
+    // pair loads read at most 15 entries past a family, inside the 16 entries
+    // of slack every partitioned list carries past its last family.
+    const uint32_t rows = min(static_cast<uint32_t>(R), (nx - xbase + 31u) >> 5);
+    auto run_item = [&](auto rows_tag) {
+      constexpr int RR = decltype(rows_tag)::value;
+      constexpr int QP = ((32 / RR) & ~1) < 16 ? ((32 / RR) & ~1) : 16;
+      constexpr uint32_t kTests = QP * RR;
+      uint32_t nx4[RR];  // -4 * w_x
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const uint32_t xi = xbase + r * 32u + lane;
-      const uint32_t wx = xi < nx ? static_cast<uint32_t>(a.x.res[xoff + xi]) : 0u;
-      nx4[r] = 0u - (wx << 2);
-      xs[r * 32u + lane] = wx;
-    }
-    const uint32_t cadd = 0u - 4u * kap - 4u;  // 4 * ~(w + kap) = -4 w - 4 kap - 4
+      for (int r = 0; r < RR; ++r) {
+        const uint32_t xi = xbase + r * 32u + lane;
+        const uint32_t wx = xi < nx ? static_cast<uint32_t>(a.x.res[xoff + xi]) : 0u;
+        nx4[r] = 0u - (wx << 2);
+        xs[r * 32u + lane] = wx;
+      }
+      const uint32_t cadd = 0u - 4u * kap - 4u;  // 4 * ~(w + kap) = -4 w - 4 kap - 4
 
-    uint32_t qlen = 0;
-    auto drain = [&]() {
-      __syncwarp();
-      for (uint32_t e = lane; e < qlen; e += 32u) {
-        const uint2 rec = wq[e];
-        const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
-        uint32_t mm = rec.y;
-        while (mm != 0u) {
-          const uint32_t b = __ffs(mm) - 1u;
-          mm &= mm - 1u;
-          const uint32_t k = 31u - b;
-          const uint32_t qi = j + k / R;
-          const uint32_t xi = xbase + (k % R) * 32u + ln;
-          if (qi >= nq || xi >= nx) continue;
-          ++c_surv;
-          const uint64_t rq = a.q.res[qoff + qi];
-          const uint32_t w = static_cast<uint32_t>(rq) + kap + xs[(k % R) * 32u + ln];
-          auto check = [&](uint32_t idx) {
-            const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
-            const uint64_t ms = sum & mmask;
-            if ((a.y.res[yoff + idx] & mmask) != ms) return;
-            if (a.project) {
-              ++c_proj;
-              return;
+      uint32_t qlen = 0;
+      auto drain = [&]() {
+        __syncwarp();
+        for (uint32_t e = lane; e < qlen; e += 32u) {
+          const uint2 rec = wq[e];
+          const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
+          uint32_t mm = rec.y;
+          while (mm != 0u) {
+            const uint32_t b = __ffs(mm) - 1u;
+            mm &= mm - 1u;
+            const uint32_t k = (kTests - 1u) - b;
+            const uint32_t qi = j + k / RR;
+            const uint32_t xi = xbase + (k % RR) * 32u + ln;
+            if (qi >= nq || xi >= nx) continue;
+            ++c_surv;
+            const uint64_t rq = a.q.res[qoff + qi];
+            const uint32_t w = static_cast<uint32_t>(rq) + kap + xs[(k % RR) * 32u + ln];
+            auto check = [&](uint32_t idx) {
+              const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
+              const uint64_t ms = sum & mmask;
+              if ((a.y.res[yoff + idx] & mmask) != ms) return;
+              if (a.project) {
+                ++c_proj;
+                return;
+              }
+              ++c_fast;
+              if (a.hi_bits != 0u) {
+                const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                       static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+                if (high != a.y.hi[yoff + idx]) return;
+              }
+              const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+              if (slot < a.cap) {
+                a.triples[3 * slot] = a.q.id[qoff + qi];
+                a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+                a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+              }
+            };
+            if (yshared) {
+              uint32_t h = yhash_of<kY3HashBits>(w);
+              for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+                if (ywin[v - 1u] == w) check(v - 1u);
+                h = (h + 1u) & ((1u << kY3HashBits) - 1u);
+              }
+            } else {
+              ++c_fall;
+              for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
             }
-            ++c_fast;
-            if (a.hi_bits != 0u) {
-              const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
-                                     static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
-              if (high != a.y.hi[yoff + idx]) return;
-            }
-            const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
-            if (slot < a.cap) {
-              a.triples[3 * slot] = a.q.id[qoff + qi];
-              a.triples[3 * slot + 1] = a.x.id[xoff + xi];
-              a.triples[3 * slot + 2] = a.y.id[yoff + idx];
-            }
-          };
-          if (yshared) {
-            uint32_t h = yhash_of<kY3HashBits>(w);
-            for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
-              if (ywin[v - 1u] == w) check(v - 1u);
-              h = (h + 1u) & ((1u << kY3HashBits) - 1u);
-            }
-          } else {
-            ++c_fall;
-            for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
           }
         }
+        __syncwarp();
+        qlen = 0;
+      };
+
+      const uint64_t* qr = a.q.res + qoff;
+      for (uint32_t j = 0; j < nq; j += QP) {
+        uint32_t m = 0;
+#pragma unroll
+        for (int p = 0; p < QP / 2; ++p) {
+          const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qr + j + 2 * p);
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const uint32_t c4 = static_cast<uint32_t>(e ? qq.y : qq.x) * 0xFFFFFFFCu + cadd;
+#pragma unroll
+            for (int r = 0; r < RR; ++r) {
+              // t4 = c4 - 4 w_x as an IMAD (multiplier `one` is 1 but opaque to the
+              // compiler), so the add runs on the FMA pipe beside the integer ALU work
+              uint32_t t4;
+              asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(t4) : "r"(nx4[r]), "r"(a.one), "r"(c4));
+              const uint32_t w = *reinterpret_cast<const uint32_t*>(bmb + (t4 & amask));
+              m = __funnelshift_l(__funnelshift_l(w, w, __umulhi(t4, 32u)), m, 1);
+            }
+          }
+        }
+        if (__any_sync(kFull, m != 0u)) {
+          const bool has = m != 0u;
+          const uint32_t ball = __ballot_sync(kFull, has);
+          if (qlen + __popc(ball) > kQueueCap) drain();
+          if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
+          qlen += __popc(ball);
+        }
       }
-      __syncwarp();
-      qlen = 0;
+      drain();
     };
-
-    const uint64_t* qr = a.q.res + qoff;
-    for (uint32_t j = 0; j < nq; j += QPC) {
-      uint32_t m = 0;
-#pragma unroll
-      for (int p = 0; p < QPC / 2; ++p) {
-        const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qr + j + 2 * p);
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const uint32_t c4 = static_cast<uint32_t>(e ? qq.y : qq.x) * 0xFFFFFFFCu + cadd;
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            // t4 = c4 - 4 w_x as an IMAD (multiplier `one` is 1 but opaque to the
-            // compiler), so the add runs on the FMA pipe beside the integer ALU work
-            uint32_t t4;
-            asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(t4) : "r"(nx4[r]), "r"(a.one), "r"(c4));
-            const uint32_t w = *reinterpret_cast<const uint32_t*>(bmb + (t4 & amask));
-            m = __funnelshift_l(__funnelshift_l(w, w, __umulhi(t4, 32u)), m, 1);
-          }
-        }
-      }
-      if (__any_sync(kFull, m != 0u)) {
-        const bool has = m != 0u;
-        const uint32_t ball = __ballot_sync(kFull, has);
-        if (qlen + __popc(ball) > kQueueCap) drain();
-        if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
-        qlen += __popc(ball);
-      }
+    switch (rows) {
+      case 1: run_item(RowsTag<1>{}); break;
+      case 2: run_item(RowsTag<2>{}); break;
+      case 3: run_item(RowsTag<3>{}); break;
+      case 4: run_item(RowsTag<4>{}); break;
+      case 5: run_item(RowsTag<5 <= R ? 5 : R>{}); break;
+      case 6: run_item(RowsTag<6 <= R ? 6 : R>{}); break;
+      case 7: run_item(RowsTag<7 <= R ? 7 : R>{}); break;
+      default: run_item(RowsTag<R>{}); break;
     }
-    drain();
   }
 
   for (int d = 16; d > 0; d >>= 1) {
