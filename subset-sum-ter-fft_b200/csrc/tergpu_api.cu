@@ -150,6 +150,12 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
     const double per = v2 ? 2048.0 : 1024.0;
     const double ideal = std::log2(std::max<double>(1.0, static_cast<double>(n_d) / per));
     t.fb = static_cast<uint32_t>(std::max(6.0, std::floor(ideal + 0.5)));
+    if (t.variant == 3 && n_d >= (128u << 7)) {
+      // small roots (the n = 72 root, 3.6e4 targets): 128 families of ~280
+      // entries keep 24 warps per CTA busy (measured 0.33 ms against 0.44 ms
+      // with 64 families)
+      t.fb = std::max<uint32_t>(t.fb, 7);
+    }
     t.fb = std::min(t.fb, fb_max);
     t.fb = std::max<uint32_t>(t.fb, 6);
   }
@@ -158,7 +164,7 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   if (filter_req != 0) {
     t.wb = filter_req - 5;
   } else if (t.variant == 3) {
-    t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 4, 6, 15);
+    t.wb = 15;  // the widest filter the 24-warp CTA holds: best measured at n = 72 and 108
   } else if (v2) {
     t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 3, 6, 14);
   } else {

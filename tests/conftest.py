@@ -26,5 +26,12 @@ def oracle_mod():
     return oracle
 
 
+@pytest.fixture(scope="session")
+def n72_anchor_attempt(oracle_mod):
+    """The oracle's attempt 0 of the n=72 anchor instance with its L1 lists
+    (about 80 s on one core: computed once per session)."""
+    return oracle_mod.attempt(72, 19797034556212562, 0, export_l1=True)
+
+
 def hexint(v):
     return int(v, 16) if isinstance(v, str) else int(v)

@@ -4,8 +4,9 @@ Run on a machine where oracle/_ref/terref was built from the reference sources
 (python __graft_entry__.py, then python tests/golden/make_golden.py).  Every
 number written here is printed by the reference itself (solve_full_ter,
 capture_to_file, the frozen K2 / K2_WIDE / ARWLF backends, the synthetic-root
-brute-force oracle of ter2_root/tests/ter_synthetic_root.hpp); nothing is typed
-in by hand.
+brute-force oracle of ter2_root/tests/ter_synthetic_root.hpp) or read from the
+reference's own published run records (published_runs); nothing is typed in by
+hand.
 """
 from __future__ import annotations
 
@@ -148,6 +149,31 @@ def seed_roots(tmp: Path):
         return list(pool.map(one, seeds))
 
 
+REFERENCE = Path("/root/reference")
+
+
+def published_runs(tmp: Path):
+    """The reference's own published run records, read from its results tree:
+    the whole-root ARWLF row of the n=108 seed 0x1001 root with its planted
+    output (results/arwlf/whole-root-20261003/runs.jsonl) and the per-attempt
+    rows of the n=72 seed 0x7201 full solve
+    (results/arwlf/full-solve-n72-s0x7201-arwlf/attempts.jsonl)."""
+    keep_run = ("root", "n", "root_seed", "Q", "W", "anchor_cell", "plant_seed", "first_planted",
+                "planted", "cells", "logical_pairs", "residue_exact", "structural", "full_q",
+                "residue_sum", "witnesses", "planted_ok", "status")
+    runs = [json.loads(line) for line in
+            (REFERENCE / "results/arwlf/whole-root-20261003/runs.jsonl").read_text().splitlines() if line]
+    arwlf = [r for r in runs if r["backend"] == "arwlf"][0]
+    keep_att = ("status", "n", "seed", "attempt", "attempt_seed", "residue_exact", "structural_triples",
+                "unique_parents", "planted_found", "parents")
+    atts = [json.loads(line) for line in
+            (REFERENCE / "results/arwlf/full-solve-n72-s0x7201-arwlf/attempts.jsonl").read_text().splitlines()
+            if line]
+    return {"whole_root_n108": {k: arwlf[k] for k in keep_run},
+            "solve_n72_s0x7201": sorted(({k: a[k] for k in keep_att} for a in atts),
+                                        key=lambda a: a["attempt"])}
+
+
 SECTIONS = {
     "n36_attempts": lambda tmp: n36_attempts(),
     "n36_snapshot": n36_snapshot,
@@ -156,6 +182,7 @@ SECTIONS = {
     "root_reports": root_reports,
     "whole_root_plants": whole_root_plants,
     "seed_roots": seed_roots,
+    "published_runs": published_runs,
 }
 
 

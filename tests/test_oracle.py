@@ -61,9 +61,9 @@ def test_planted_synthetic_triples_satisfy_equation(oracle_mod):
         assert (va + vb - vd) % (1 << 69) == 0
 
 
-def test_n72_anchor_level_sizes(oracle_mod, golden):
+def test_n72_anchor_level_sizes(n72_anchor_attempt, golden):
     g = golden["n72_roots"][0]
-    got = oracle_mod.attempt(72, ANCHOR_SEED, 0)
+    got = n72_anchor_attempt
     assert got["level1"] == g["level1"] == [19109, 32496, 33505]
     assert got["level2"] == g["level2"]
 

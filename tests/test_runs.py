@@ -1,0 +1,79 @@
+"""Run records (tergpu.runs) on the CPU: the reference's anchor sample, its
+positive planting against the reference's own plant of the n=72 anchor root
+(golden whole_root_plants, printed by the reference harness), and the
+whole-root runner's resume / refuse rules, which act before any device work."""
+import json
+
+import numpy as np
+
+ANCHOR_SEED = 19797034556212562
+
+
+def _n72_anchor_snapshot(att):
+    from tergpu import snapshot
+
+    l1 = att["l1"]
+    recs = []
+    for g in range(3):
+        pos = np.stack([l1["pos0"][g], l1["pos1"][g]], axis=1)
+        neg = np.stack([l1["neg0"][g], l1["neg1"][g]], axis=1)
+        res = np.stack([l1["res_lo"][g] & np.uint64(0xFFFFFFFF), l1["res_lo"][g] >> np.uint64(32),
+                        l1["res_hi"][g] & np.uint64(0xFFFFFFFF)], axis=1).astype("<u4")
+        rec = np.concatenate([pos.astype("<u8").view(np.uint8), neg.astype("<u8").view(np.uint8),
+                              res.view(np.uint8)], axis=1)
+        recs.append(np.ascontiguousarray(rec).reshape(-1))
+
+    def words(v):
+        return np.array([(v >> (32 * k)) & 0xFFFFFFFF for k in range(3)], dtype=np.uint32)
+
+    return snapshot.Snapshot(n=72, r1=att["r1"], r2=att["r2"], attempt=0, seed=ANCHOR_SEED,
+                             attempt_seed=ANCHOR_SEED, records=recs,
+                             child_targets=[words(t) for t in att["t1"]],
+                             root_target=words(att["root_target"]), level2_sizes=att["level2"])
+
+
+def test_anchor_sample_and_hashes(oracle_mod, golden):
+    from tergpu import runs, workload
+
+    assert runs.anchor_cell() == golden["whole_root_plants"][0]["anchor_cell"] == 2730
+    assert (runs.select_cells(16) == oracle_mod.select_cells(16)).all()
+    vals = np.array([0, 1, 0x5EED5EED, 2**64 - 1], dtype=np.uint64)
+    assert [runs.mix64(int(v)) for v in vals] == [int(x) for x in workload.mix64(vals)]
+
+
+def test_plant_matches_reference_on_n72_anchor_root(n72_anchor_attempt, golden):
+    from tergpu import runs, snapshot
+
+    g = golden["whole_root_plants"][0]
+    assert g["n"] == 72 and g["seed"] == ANCHOR_SEED
+    snap = _n72_anchor_snapshot(n72_anchor_attempt)
+    assert snap.entries == [19109, 32496, 33505]
+    p = runs.plant_positive(snap, runs.anchor_cell())
+    assert p.first_planted == g["first_planted"]
+    assert p.expected == g["expected"]
+    assert p.d_lo == g["d_lo"] and p.d_hi == g["d_hi"]
+    # the planted record derives exactly the planted key and completes the pair
+    _, lo, hi, _ = snapshot.root_keys(p.snapshot)
+    assert int(lo[2][p.first_planted]) == g["d_lo"][0] and int(hi[2][p.first_planted]) == g["d_hi"][0]
+    a, b, c = p.expected[0]
+    nmask = (1 << 72) - 1
+    res = [snapshot._words_to_int(p.snapshot.residues(l)[e]) for l, e in enumerate((a, b, c))]
+    root = snapshot._words_to_int(snap.root_target) & nmask
+    assert (res[0] + res[1] + res[2]) & nmask == root
+    digits = sum(runs._digits(p.snapshot, l, e).astype(int) for l, e in enumerate((a, b, c)))
+    neg, zero, pos = runs.structural_parent_counts(72)
+    assert set(digits.tolist()) <= {-1, 0, 1}
+    assert ((digits == -1).sum(), (digits == 0).sum(), (digits == 1).sum()) == (neg, zero, pos)
+
+
+def test_whole_root_resume_and_refusal(tmp_path):
+    from tergpu import runs
+
+    rows = [{"run_id": "gpu-1", "chunk": "all", "backend": "gpu", "status": "COMPLETED", "root": "r1"},
+            {"run_id": "k2-1", "chunk": "all", "backend": "k2", "status": "COMPLETED", "root": "r1"}]
+    (tmp_path / "runs.jsonl").write_text("".join(json.dumps(r) + "\n" for r in rows))
+    # a finished run id is not rerun; one recorded with another backend or root is refused
+    assert runs.whole_root(None, "r1", "gpu-1", tmp_path) == (0, None)
+    assert runs.whole_root(None, "r1", "k2-1", tmp_path) == (2, None)
+    assert runs.whole_root(None, "r2", "gpu-1", tmp_path) == (2, None)
+    assert len((tmp_path / "runs.jsonl").read_text().splitlines()) == 2
