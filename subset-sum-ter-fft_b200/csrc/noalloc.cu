@@ -203,7 +203,6 @@ extern "C" int tergpu_root_run_noalloc(const tergpu_root_in* in, tergpu_root_out
   a.cells = in->cells;  // device pointer or null
   a.fb = fb;
   a.s_split = s_split;
-  a.one = 1;
   a.shard = 0;
   a.shards = 1;
   a.wb = wb;

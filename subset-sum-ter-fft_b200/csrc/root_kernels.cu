@@ -646,18 +646,15 @@ __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a)
             const uint32_t c4 = static_cast<uint32_t>(e ? qq.y : qq.x) * 0xFFFFFFFCu + cadd;
 #pragma unroll
             for (int r = 0; r < RR; ++r) {
-              // t4 = c4 - 4 w_x as an IMAD (multiplier `one` is 1 but opaque to the
-              // compiler), so the add runs on the FMA pipe beside the integer ALU work
-              uint32_t t4;
-              asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(t4) : "r"(nx4[r]), "r"(a.one), "r"(c4));
+              const uint32_t t4 = c4 + nx4[r];  // 4 T = 4 ~(w_q + kappa) - 4 w_x
               const uint32_t w = *reinterpret_cast<const uint32_t*>(bmb + (t4 & amask));
               m = __funnelshift_l(__funnelshift_l(w, w, __umulhi(t4, 32u)), m, 1);
             }
           }
         }
-        if (__any_sync(kFull, m != 0u)) {
-          const bool has = m != 0u;
-          const uint32_t ball = __ballot_sync(kFull, has);
+        const bool has = m != 0u;
+        const uint32_t ball = __ballot_sync(kFull, has);
+        if (ball != 0u) {
           if (qlen + __popc(ball) > kQueueCap) drain();
           if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
           qlen += __popc(ball);

@@ -49,7 +49,6 @@ struct SweepArgs {
   const uint8_t* cells;     // 4096 bytes over the low 6 key bits, or null
   uint32_t fb;              // family bits
   uint32_t s_split;         // CTAs per target family
-  uint32_t one;             // 1 (an IMAD multiplier the compiler cannot fold)
   uint32_t shard;           // this call joins the target families u == shard (mod shards)
   uint32_t shards;          // power of two, 1..64 (1: the whole root)
   uint32_t wb;              // log2 of filter words (filter bits = wb + 5)

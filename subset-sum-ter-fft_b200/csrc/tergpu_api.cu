@@ -261,7 +261,6 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
   a.cells = j.cells;
   a.fb = tu.fb;
   a.s_split = tu.s_split;
-  a.one = 1;
   a.shard = j.shard;
   a.shards = j.shards;
   a.wb = tu.wb;
