@@ -485,9 +485,13 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint64_t* __
                                                               uint32_t* __restrict__ counts) {
   __shared__ uint32_t hist[256];
   const uint64_t n = cnt.get();
+  const uint64_t base = (uint64_t)blockIdx.x * kTile;
+  if (base >= n) {  // a tile past the device count (grids are sized by capacity): zero counts
+    counts[(uint64_t)threadIdx.x * nb + blockIdx.x] = 0;
+    return;
+  }
   hist[threadIdx.x] = 0;
   __syncthreads();
-  const uint64_t base = (uint64_t)blockIdx.x * kTile;
   for (uint32_t i = threadIdx.x; i < kTile; i += kRadixThreads) {
     if (base + i < n) atomicAdd(&hist[digit_of(khi[base + i], klo[base + i], word, shift)], 1u);
   }
@@ -503,6 +507,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(
     Count cnt, uint32_t word, uint32_t shift, uint32_t nb, const uint32_t* __restrict__ offsets,
     uint64_t* __restrict__ ohi, uint64_t* __restrict__ olo, uint32_t* __restrict__ oidx) {
   const uint64_t n = cnt.get();
+  if ((uint64_t)blockIdx.x * kTile >= n) return;  // nothing to scatter (uniform per block)
   __shared__ uint32_t wcnt[kRadixThreads / 32][256];
   __shared__ uint32_t goff[256];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

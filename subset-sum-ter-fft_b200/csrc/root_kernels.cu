@@ -297,10 +297,15 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
 }
 
 
+// Compile-time row count of a sweep chunk (selects the unrolled probe loop).
+template <int V>
+struct RowsTag {
+  static constexpr int value = V;
+};
+
 template <bool ALIGNED, int R>
 __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) {
-  static_assert(R == 4 || R == 8, "32 tests per mask");
-  constexpr int QPC = 32 / R;  // A entries per 32-test mask
+  static_assert(R >= 1 && R <= 8, "at most 8 rows of B entries per chunk");
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint32_t item_counter;
   const uint32_t nfam = 1u << a.fb;
@@ -356,101 +361,118 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
     const uint32_t qoff = a.q.off[s];
     const uint32_t xoff = a.x.off[t];
 
-    uint32_t xw[R];
+    // The last chunk of a family runs with only its occupied rows (as in k_sweep3).
+    const uint32_t rows = min(static_cast<uint32_t>(R), (nx - xbase + 31u) >> 5);
+    auto run_item = [&](auto rows_tag) {
+      constexpr int RR = decltype(rows_tag)::value;
+      constexpr int QP = ((32 / RR) & ~1) < 16 ? ((32 / RR) & ~1) : 16;
+      constexpr uint32_t kTests = QP * RR;
+      uint32_t xw[RR];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const uint32_t xi = xbase + r * 32u + lane;
-      xw[r] = xi < nx ? window_of<ALIGNED>(a.x.res[xoff + xi] & mmask, a.mrb) : 0u;
-      xs[r * 32u + lane] = xw[r];
-    }
-    const uint32_t kapw = kap << kap_shift;
+      for (int r = 0; r < RR; ++r) {
+        const uint32_t xi = xbase + r * 32u + lane;
+        xw[r] = xi < nx ? window_of<ALIGNED>(a.x.res[xoff + xi] & mmask, a.mrb) : 0u;
+        xs[r * 32u + lane] = xw[r];
+      }
+      const uint32_t kapw = kap << kap_shift;
 
-    uint32_t qlen = 0;
-    auto drain = [&]() {
-      __syncwarp();
-      for (uint32_t e = lane; e < qlen; e += 32u) {
-        const uint2 rec = wq[e];
-        const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
-        uint32_t mm = rec.y;
-        while (mm != 0u) {
-          const uint32_t b = __ffs(mm) - 1u;
-          mm &= mm - 1u;
-          const uint32_t k = 31u - b;
-          const uint32_t qi = j + k / R;
-          const uint32_t xi = xbase + (k % R) * 32u + ln;
-          if (qi >= nq || xi >= nx) continue;
-          ++c_surv;
-          // the 32-bit window of the sum from the A residual (L1-resident: the
-          // warp just streamed it) and the staged B window; full residuals are
-          // read only when a D entry carries the same window
-          const uint64_t rq = a.q.res[qoff + qi];
-          const uint32_t w = window_of<ALIGNED>(rq & mmask, a.mrb) + kapw + xs[(k % R) * 32u + ln];
-          auto check = [&](uint32_t idx) {
-            const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
-            const uint64_t ms = sum & mmask;
-            if ((a.y.res[yoff + idx] & mmask) != ms) return;
-            if (a.project) {
-              ++c_proj;
-              return;
+      uint32_t qlen = 0;
+      auto drain = [&]() {
+        __syncwarp();
+        for (uint32_t e = lane; e < qlen; e += 32u) {
+          const uint2 rec = wq[e];
+          const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
+          uint32_t mm = rec.y;
+          while (mm != 0u) {
+            const uint32_t b = __ffs(mm) - 1u;
+            mm &= mm - 1u;
+            const uint32_t k = (kTests - 1u) - b;
+            const uint32_t qi = j + k / RR;
+            const uint32_t xi = xbase + (k % RR) * 32u + ln;
+            if (qi >= nq || xi >= nx) continue;
+            ++c_surv;
+            // the 32-bit window of the sum from the A residual (L1-resident: the
+            // warp just streamed it) and the staged B window; full residuals are
+            // read only when a D entry carries the same window
+            const uint64_t rq = a.q.res[qoff + qi];
+            const uint32_t w = window_of<ALIGNED>(rq & mmask, a.mrb) + kapw + xs[(k % RR) * 32u + ln];
+            auto check = [&](uint32_t idx) {
+              const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
+              const uint64_t ms = sum & mmask;
+              if ((a.y.res[yoff + idx] & mmask) != ms) return;
+              if (a.project) {
+                ++c_proj;
+                return;
+              }
+              ++c_fast;
+              if (a.hi_bits != 0u) {
+                const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                       static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+                if (high != a.y.hi[yoff + idx]) return;
+              }
+              const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+              if (slot < a.cap) {
+                a.triples[3 * slot] = a.q.id[qoff + qi];
+                a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+                a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+              }
+            };
+            if (yshared) {
+              uint32_t h = yhash_of(w);
+              for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+                if (ywin[v - 1u] == w) check(v - 1u);
+                h = (h + 1u) & ((1u << kYHashBits) - 1u);
+              }
+            } else {
+              ++c_fall;
+              for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
             }
-            ++c_fast;
-            if (a.hi_bits != 0u) {
-              const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
-                                     static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
-              if (high != a.y.hi[yoff + idx]) return;
-            }
-            const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
-            if (slot < a.cap) {
-              a.triples[3 * slot] = a.q.id[qoff + qi];
-              a.triples[3 * slot + 1] = a.x.id[xoff + xi];
-              a.triples[3 * slot + 2] = a.y.id[yoff + idx];
-            }
-          };
-          if (yshared) {
-            uint32_t h = yhash_of(w);
-            for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
-              if (ywin[v - 1u] == w) check(v - 1u);
-              h = (h + 1u) & ((1u << kYHashBits) - 1u);
-            }
-          } else {
-            ++c_fall;
-            for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
           }
         }
-      }
-      __syncwarp();
-      qlen = 0;
-    };
+        __syncwarp();
+        qlen = 0;
+      };
 
-    const uint64_t* qr = a.q.res + qoff;
-    for (uint32_t j = 0; j < nq; j += QPC) {
-      uint32_t m = 0;
+      const uint64_t* qr = a.q.res + qoff;
+      for (uint32_t j = 0; j < nq; j += QP) {
+        uint32_t m = 0;
 #pragma unroll
-      for (int p = 0; p < QPC / 2; ++p) {
-        // uniform address: one broadcast load of two A residuals (families start
-        // on even entries; the array carries slack past its end)
-        const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qr + j + 2 * p);
+        for (int p = 0; p < QP / 2; ++p) {
+          // uniform address: one broadcast load of two A residuals (families start
+          // on even entries; the array carries slack past its end)
+          const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qr + j + 2 * p);
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const uint32_t nqw = ~(window_of<ALIGNED>((e ? qq.y : qq.x) & mmask, a.mrb) + kapw);
+          for (int e = 0; e < 2; ++e) {
+            const uint32_t nqw = ~(window_of<ALIGNED>((e ? qq.y : qq.x) & mmask, a.mrb) + kapw);
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const uint32_t tt = nqw - xw[r];
-            const uint32_t w = bm[__umulhi(tt, word_mul)];
-            m = __funnelshift_l(__funnelshift_l(w, w, tt >> rot_shift), m, 1);
+            for (int r = 0; r < RR; ++r) {
+              const uint32_t tt = nqw - xw[r];
+              const uint32_t w = bm[__umulhi(tt, word_mul)];
+              m = __funnelshift_l(__funnelshift_l(w, w, tt >> rot_shift), m, 1);
+            }
           }
         }
-      }
-      if (__any_sync(kFull, m != 0u)) {
-        // one record per lane: test k = (2p + e) * R + r sits at bit 31 - k
+        // one record per lane: test k = (2p + e) * RR + r sits at bit kTests - 1 - k
         const bool has = m != 0u;
         const uint32_t ball = __ballot_sync(kFull, has);
-        if (qlen + __popc(ball) > kQueueCap) drain();
-        if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
-        qlen += __popc(ball);
+        if (ball != 0u) {
+          if (qlen + __popc(ball) > kQueueCap) drain();
+          if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
+          qlen += __popc(ball);
+        }
       }
+      drain();
+    };
+    switch (rows) {
+      case 1: run_item(RowsTag<1>{}); break;
+      case 2: run_item(RowsTag<2>{}); break;
+      case 3: run_item(RowsTag<3>{}); break;
+      case 4: run_item(RowsTag<4>{}); break;
+      case 5: run_item(RowsTag<5 <= R ? 5 : R>{}); break;
+      case 6: run_item(RowsTag<6 <= R ? 6 : R>{}); break;
+      case 7: run_item(RowsTag<7 <= R ? 7 : R>{}); break;
+      default: run_item(RowsTag<R>{}); break;
     }
-    drain();
   }
 
   for (int d = 16; d > 0; d >>= 1) {
@@ -497,12 +519,6 @@ __device__ __forceinline__ void build_target3(const SweepArgs& a, uint32_t yoff,
   }
   __syncthreads();
 }
-
-// Compile-time row count of a sweep chunk (selects the unrolled probe loop).
-template <int V>
-struct RowsTag {
-  static constexpr int value = V;
-};
 
 template <int R>
 __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a) {
