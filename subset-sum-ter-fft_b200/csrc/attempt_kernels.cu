@@ -39,6 +39,13 @@ int blocks_for(uint64_t n, int threads, int cap = 148 * 16) {
   return b == 0 ? 1 : (int)b;
 }
 
+// Blocks for a grid-stride kernel over `c`.  A device count (a captured graph's
+// launch, sized by a capacity the real count mostly stays far below) gets about
+// two CTAs per SM, so the launch does not spend SM time on empty CTAs.
+int blocks_for_count(const Count& c, int threads) {
+  return blocks_for(c.cap, threads, c.dev != nullptr ? 148 * 2 : 148 * 16);
+}
+
 __device__ __forceinline__ ConstEntryArrays offset_view(ConstEntryArrays e, uint64_t off) {
   return ConstEntryArrays{e.pos0 + off, e.pos1 + off, e.res_lo + off, e.res_hi + off};
 }
@@ -710,7 +717,7 @@ void launch_l2_quotients(ConstEntryArrays l, Count count, uint32_t b1, uint32_t 
                          uint64_t t_hi, int negate, uint64_t tau, uint64_t* key, cudaStream_t st,
                          const uint32_t* doff, const uint64_t* dvals) {
   if (count.cap == 0) return;
-  k_l2_quotients<<<blocks_for(count.cap, 256), 256, 0, st>>>(l, count, doff, b1, r2, t_lo, t_hi, negate,
+  k_l2_quotients<<<blocks_for_count(count, 256), 256, 0, st>>>(l, count, doff, b1, r2, t_lo, t_hi, negate,
                                                              tau, dvals, key);
 }
 
@@ -719,7 +726,7 @@ void launch_l1_parents(const uint32_t* triples, Count ntriples, ConstEntryArrays
                        unsigned long long* count, cudaStream_t st, const uint32_t* doff) {
   cudaMemsetAsync(count, 0, 8, st);
   if (ntriples.cap == 0) return;
-  k_l1_parents<<<blocks_for(ntriples.cap, 256), 256, 0, st>>>(triples, ntriples, x, y, z, doff, n,
+  k_l1_parents<<<blocks_for_count(ntriples, 256), 256, 0, st>>>(triples, ntriples, x, y, z, doff, n,
                                                               expected_ones, out, count);
 }
 
@@ -751,7 +758,7 @@ void radix_sort_entries(ConstEntryArrays in, Count cnt, uint64_t vary_pos0, uint
   uint32_t* counts = w32 + 2 * count;
   uint32_t* offsets = counts + cells + 1;
   uint32_t* scan_scratch = offsets + cells + 1;
-  k_radix_init<<<blocks_for(count, 256), 256, 0, st>>>(in, cnt, khi[0], klo[0], idx[0]);
+  k_radix_init<<<blocks_for_count(cnt, 256), 256, 0, st>>>(in, cnt, khi[0], klo[0], idx[0]);
   int cur = 0;
   for (uint32_t word = 0; word < 2; ++word) {  // word 0: pos1 (less significant), word 1: pos0
     const uint64_t vary = word == 0 ? vary_pos1 : vary_pos0;
@@ -775,9 +782,9 @@ void launch_gather_unique(ConstEntryArrays in, const uint32_t* perm, Count cnt, 
     cudaMemsetAsync(kept, 0, 8, st);
     return;
   }
-  k_unique_flags<<<blocks_for(count, 256), 256, 0, st>>>(in, perm, cnt, flags);
+  k_unique_flags<<<blocks_for_count(cnt, 256), 256, 0, st>>>(in, perm, cnt, flags);
   launch_scan_u32(flags, count, starts, scratch, st);
-  k_gather_kept<<<blocks_for(count, 256), 256, 0, st>>>(in, perm, cnt, flags, starts, out, kept);
+  k_gather_kept<<<blocks_for_count(cnt, 256), 256, 0, st>>>(in, perm, cnt, flags, starts, out, kept);
 }
 
 void launch_or_reduce(ConstEntryArrays in, uint64_t count, unsigned long long* acc, cudaStream_t st) {
@@ -792,7 +799,7 @@ void launch_copy_count(const unsigned long long* src, unsigned long long* dst, c
 
 void launch_pack_records(ConstEntryArrays in, Count count, uint32_t n, uint8_t* records, cudaStream_t st) {
   if (count.cap == 0) return;
-  k_pack_records<<<blocks_for(count.cap, 256), 256, 0, st>>>(in, count, n, records);
+  k_pack_records<<<blocks_for_count(count, 256), 256, 0, st>>>(in, count, n, records);
 }
 
 }  // namespace tergpu

@@ -956,6 +956,13 @@ int grid_for(uint64_t n, int threads) {
   return blocks == 0 ? 1 : static_cast<int>(blocks);
 }
 
+// grid_for of a grid-stride kernel over `c`: about two CTAs per SM for a device
+// count (a captured graph's capacity-sized launch).
+int grid_for_count(const Count& c, int threads) {
+  const int g = grid_for(c.cap, threads);
+  return c.dev != nullptr && g > 148 * 2 ? 148 * 2 : g;
+}
+
 }  // namespace
 
 // Allows a kernel the device's whole opt-in shared memory, once per device and
@@ -991,7 +998,7 @@ void prepare_root_kernels() {
 
 void launch_hist(const uint64_t* key, Count n, uint32_t fmask, uint32_t* cnt, cudaStream_t st) {
   if (n.cap == 0) return;
-  k_hist<<<grid_for(n.cap, 256), 256, 0, st>>>(key, n, fmask, cnt);
+  k_hist<<<grid_for_count(n, 256), 256, 0, st>>>(key, n, fmask, cnt);
 }
 
 void launch_scan(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor,
@@ -1003,7 +1010,7 @@ void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_
                     uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
                     uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st) {
   if (n.cap == 0) return;
-  k_scatter<<<grid_for(n.cap, 256), 256, 0, st>>>(key_lo, key_hi, id, n, fb, fast_mask, hi_mask, cursor,
+  k_scatter<<<grid_for_count(n, 256), 256, 0, st>>>(key_lo, key_hi, id, n, fb, fast_mask, hi_mask, cursor,
                                              res, hi, out_id);
 }
 
@@ -1073,12 +1080,12 @@ void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t
 
 void launch_record_keys(const RecordKeyArgs& a, cudaStream_t st) {
   if (a.count.cap == 0) return;
-  k_record_keys<<<grid_for(a.count.cap, 256), 256, 0, st>>>(a);
+  k_record_keys<<<grid_for_count(a.count, 256), 256, 0, st>>>(a);
 }
 
 void launch_authority(const AuthorityArgs& a, cudaStream_t st) {
   if (a.count.cap == 0) return;
-  k_authority<<<grid_for(a.count.cap, 128), 128, 0, st>>>(a);
+  k_authority<<<grid_for_count(a.count, 128), 128, 0, st>>>(a);
 }
 
 }  // namespace tergpu
