@@ -178,7 +178,7 @@ def plant_positive(snap, cell: int, count: int = 1, seed: int = PLANT_SEED) -> P
     lo_mask = (1 << lo_bits) - 1
     hi_mask = (1 << (Q - 64)) - 1 if Q > 64 else 0
     nmask = (1 << n) - 1
-    root = snapmod._words_to_int(snap.root_target) & nmask
+    root = snapmod.words_to_int(snap.root_target) & nmask
     res = [snap.residues(l) for l in range(2)]
     want = structural_parent_counts(n)
     key_size = snap.entries[2]
@@ -200,8 +200,8 @@ def plant_positive(snap, cell: int, count: int = 1, seed: int = PLANT_SEED) -> P
         c_digits = _complete_digits(_digits(snap, 0, a), _digits(snap, 1, b), want)
         if c_digits is None:
             continue
-        ra = snapmod._words_to_int(res[0][a]) & nmask
-        rb = snapmod._words_to_int(res[1][b]) & nmask
+        ra = snapmod.words_to_int(res[0][a]) & nmask
+        rb = snapmod.words_to_int(res[1][b]) & nmask
         rc = (root - ra - rb) & nmask
         used.add((qi, xi))
         if (dl & (FAMILIES - 1)) != u:

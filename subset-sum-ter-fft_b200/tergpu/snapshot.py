@@ -199,7 +199,8 @@ def save(snap: Snapshot, path: os.PathLike | str, git_commit: str = "tergpu") ->
     return offset
 
 
-def _words_to_int(words) -> int:
+def words_to_int(words) -> int:
+    """Little-endian 32-bit words (a residue or a target) as one integer."""
     v = 0
     for k, w in enumerate(words):
         v |= int(w) << (32 * k)
@@ -216,8 +217,8 @@ def root_keys(snap: Snapshot):
     Q = n - r1
     nmask = (1 << n) - 1
     qmask = (1 << Q) - 1
-    T = _words_to_int(snap.root_target) & nmask
-    c = [_words_to_int(t) & nmask for t in snap.child_targets]
+    T = words_to_int(snap.root_target) & nmask
+    c = [words_to_int(t) & nmask for t in snap.child_targets]
     tau = (((T - c[0] - c[1] - c[2]) & nmask) >> r1) & qmask
     lo_out, hi_out = [], []
     for l in range(3):

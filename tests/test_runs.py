@@ -57,8 +57,8 @@ def test_plant_matches_reference_on_n72_anchor_root(n72_anchor_attempt, golden):
     assert int(lo[2][p.first_planted]) == g["d_lo"][0] and int(hi[2][p.first_planted]) == g["d_hi"][0]
     a, b, c = p.expected[0]
     nmask = (1 << 72) - 1
-    res = [snapshot._words_to_int(p.snapshot.residues(l)[e]) for l, e in enumerate((a, b, c))]
-    root = snapshot._words_to_int(snap.root_target) & nmask
+    res = [snapshot.words_to_int(p.snapshot.residues(l)[e]) for l, e in enumerate((a, b, c))]
+    root = snapshot.words_to_int(snap.root_target) & nmask
     assert (res[0] + res[1] + res[2]) & nmask == root
     digits = sum(runs._digits(p.snapshot, l, e).astype(int) for l, e in enumerate((a, b, c)))
     neg, zero, pos = runs.structural_parent_counts(72)
