@@ -54,6 +54,10 @@ OPS_PER_PAIR = 5
 # launch on the default workload (the whole authentic n=108 root of seed 0x1001), from one
 # ncu capture of that launch; other workloads and variants report null
 SWEEP_DRAM_BYTES = {"k_sweep3": 2.571e9 + 355.7e6}
+# The reference's published whole-root ARWLF run of this root (seed 0x1001, attempt 0,
+# all 4096 cells, 25,189,929,333,072 logical pairs) took 3,575,458 ms on one core
+# (results/arwlf/whole-root-20261003/summary.md:10 in the reference): its pairs/s.
+PUBLISHED_ARWLF_PAIRS_PER_S = 25_189_929_333_072 / 3575.458
 
 
 def parse():
@@ -358,7 +362,9 @@ def run_tergpu(args):
             "metric": METRIC, "value": pairs / (ms / 1000.0), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "scaling": "strong" if sharded else "weak",
+            "vs_baseline": (pairs / (ms / 1000.0) / PUBLISHED_ARWLF_PAIRS_PER_S
+                            if not args.synthetic and args.seed == 0x1001 else None),
             "dtype": "u64",
             "data": ("synthetic" if args.synthetic else
                      "authentic: L1 lists generated on the device by this library's attempt "
