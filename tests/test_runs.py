@@ -77,3 +77,22 @@ def test_whole_root_resume_and_refusal(tmp_path):
     assert runs.whole_root(None, "r1", "k2-1", tmp_path) == (2, None)
     assert runs.whole_root(None, "r2", "gpu-1", tmp_path) == (2, None)
     assert len((tmp_path / "runs.jsonl").read_text().splitlines()) == 2
+
+
+def test_cli_usage_errors(tmp_path):
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    pkg = Path(__file__).resolve().parent.parent / "subset-sum-ter-fft_b200"
+    env = dict(os.environ, PYTHONPATH=str(pkg))
+    # neither a snapshot nor an instance to capture: usage, exit 2, nothing written
+    r = subprocess.run([sys.executable, "-m", "tergpu.runs", "whole-root", f"--out-dir={tmp_path}",
+                        "--run=x"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2 and not (tmp_path / "runs.jsonl").exists()
+    # an unreadable snapshot: load failure, exit 3
+    r = subprocess.run([sys.executable, "-m", "tergpu.runs", "solve-attempt",
+                        f"--snapshot={tmp_path / 'missing.snap'}", f"--out={tmp_path / 'a.jsonl'}"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 3 and not (tmp_path / "a.jsonl").exists()
