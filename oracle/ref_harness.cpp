@@ -12,8 +12,8 @@
 //   terref capture N SEED ATTEMPT KIND OUT
 //       root_snapshot::capture_to_file (ter2_root/frozen/ter_root_snapshot.cpp:124).
 //   terref snaproot SNAP BACKEND CELLS PROJ
-//       load_snapshot_workload + build_family_keys + build_root_index, optional
-//       select_microproblems(CELLS), then one backend into an authority sink.
+//       load_snapshot_workload + build_family_keys + build_root_index, the cell
+//       selection CELLS (apply_cells), then one backend into an authority sink.
 //   terref synth BITS SEED SIZE POOL OUT
 //       ter2_root/tests/ter_synthetic_root.hpp make_root; writes the three key
 //       lists to OUT and prints the brute-force oracle digest.
@@ -132,7 +132,26 @@ int cmd_solve(int argc, char** argv) {
               << ",\"valid_roots\":" << a.level1_to_level0.valid_root_count
               << ",\"prefilter_bits\":" << a.level1_to_level0.prefilter_bits
               << ",\"root_ns\":" << a.level1_to_level0.elapsed_ns
-              << ",\"total_ns\":" << a.total_ns << "}\n";
+              << ",\"total_ns\":" << a.total_ns;
+    const auto stage = [](const char* name, const ter::FullTerStageTelemetry& s) {
+      std::ostringstream o;
+      o << ",\"" << name << "\":{\"pairs\":" << s.pair_candidates
+        << ",\"modular\":" << s.modular_candidates << ",\"structural\":" << s.structural_rejects
+        << ",\"distribution\":" << s.distribution_rejects
+        << ",\"survivors\":" << s.survivors_before_dedup
+        << ",\"deduplicated\":" << s.survivors_after_dedup
+        << ",\"pair_records\":" << s.pair_records << ",\"quotient_bits\":" << s.quotient_bits
+        << ",\"prefilter_bits\":" << s.prefilter_bits
+        << ",\"low_prefilter\":" << s.low_prefilter_candidates
+        << ",\"full_quotient_rejects\":" << s.full_quotient_rejects
+        << ",\"valid_roots\":" << s.valid_root_count
+        << ",\"policy\":" << static_cast<unsigned>(s.effective_root_output_policy)
+        << ",\"early_stopped\":" << (s.early_stopped ? 1 : 0)
+        << ",\"fingerprint\":" << hex64(s.output_fingerprint) << "}";
+      return o.str();
+    };
+    std::cout << stage("binary", a.level3_to_level2) << stage("middle", a.level2_to_level1)
+              << stage("root", a.level1_to_level0) << "}\n";
   }
   std::cout << "{\"status\":" << static_cast<int>(result.status) << ",\"r1\":" << t.parameters.r1
             << ",\"r2\":" << t.parameters.r2 << ",\"l3\":[" << t.physical_level3_sizes[0] << ","
@@ -216,11 +235,49 @@ std::string run_backend(const std::string& backend, const mr8::Dataset& data, rg
   return o.str();
 }
 
+// CELLS selects the microproblems (index s * 64 + t) a backend runs:
+//   a count N       the reference's declared subsample, select_microproblems(N)
+//                   (ter_root_queue_kernels.cpp:111-132); N >= 4096 keeps all;
+//   mod:P:I:M       the first M cells c with c % P == I (disjoint slices);
+//   perm:S:C        positions [S, S + C) of the reference's own shuffled order,
+//                   i.e. select_microproblems(S + C) minus select_microproblems(S):
+//                   successive windows are disjoint and spread over all families.
+void apply_cells(rg::RootIndex& index, const std::string& spec) {
+  if (spec.rfind("mod:", 0) == 0) {
+    unsigned p = 1, i = 0, m = 4096;
+    std::sscanf(spec.c_str(), "mod:%u:%u:%u", &p, &i, &m);
+    index.selected.fill(0U);
+    index.selected_count = 0U;
+    for (std::uint32_t c = 0; c < 4096U && index.selected_count < m; ++c) {
+      if (p != 0U && c % p == i) {
+        index.selected[c] = 1U;
+        ++index.selected_count;
+      }
+    }
+  } else if (spec.rfind("perm:", 0) == 0) {
+    unsigned s = 0, c = 0;
+    std::sscanf(spec.c_str(), "perm:%u:%u", &s, &c);
+    s = std::min(s, 4096U);
+    c = std::min(c, 4096U - s);
+    rg::select_microproblems(index, s);
+    const auto before = index.selected;
+    rg::select_microproblems(index, s + c);
+    index.selected_count = 0U;
+    for (std::uint32_t cell = 0; cell < 4096U; ++cell) {
+      index.selected[cell] = (index.selected[cell] != 0U && before[cell] == 0U) ? 1U : 0U;
+      index.selected_count += index.selected[cell];
+    }
+  } else {
+    const auto cells = static_cast<std::uint32_t>(std::strtoul(spec.c_str(), nullptr, 0));
+    if (cells < 4096U) { rg::select_microproblems(index, cells); }
+  }
+}
+
 int cmd_snaproot(int argc, char** argv) {
   if (argc < 6) { return 2; }
   const std::string path = argv[2];
   const std::string backend = argv[3];
-  const auto cells = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
+  const std::string cells_arg = argv[4];
   const auto proj = static_cast<std::uint32_t>(std::strtoul(argv[5], nullptr, 0));
   const auto workload = rg::load_snapshot_workload(path, true);
   if (workload->status != rg::WorkloadStatus::Completed) {
@@ -232,7 +289,7 @@ int cmd_snaproot(int argc, char** argv) {
   const mr8::Dataset& data = *workload->data;
   rg::RootIndex index;
   rg::build_root_index(data, index);
-  if (cells < 4096U) { rg::select_microproblems(index, cells); }
+  apply_cells(index, cells_arg);
   std::vector<std::array<ter::EntryId, 3>> witnesses;
   rg::RootSink sink;
   sink.data = &data;
@@ -322,29 +379,13 @@ int cmd_keysroot(int argc, char** argv) {
     return 1;
   }
   const std::string backend = argv[3];
-  // CELLS: a count (the reference's declared subsample) or "mod:P:I:M" -- the
-  // first M cells c (index s * 64 + t) with c % P == I, for disjoint slices.
   const std::string cells_arg = argv[4];
-  const auto cells = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
   const int reps = std::max(1, std::atoi(argv[5]));
   const auto proj = static_cast<std::uint32_t>(std::strtoul(argv[6], nullptr, 0));
   const auto build_start = Clock::now();
   sr::finish(root);
   const double build_ms = std::chrono::duration<double, std::milli>(Clock::now() - build_start).count();
-  if (cells_arg.rfind("mod:", 0) == 0) {
-    unsigned p = 1, i = 0, m = 4096;
-    std::sscanf(cells_arg.c_str(), "mod:%u:%u:%u", &p, &i, &m);
-    root.index.selected.fill(0U);
-    root.index.selected_count = 0U;
-    for (std::uint32_t c = 0; c < 4096U && root.index.selected_count < m; ++c) {
-      if (p != 0U && c % p == i) {
-        root.index.selected[c] = 1U;
-        ++root.index.selected_count;
-      }
-    }
-  } else if (cells < 4096U) {
-    rg::select_microproblems(root.index, cells);
-  }
+  apply_cells(root.index, cells_arg);
   std::uint64_t pairs = 0U;
   for (std::uint32_t s = 0; s < 64U; ++s)
     for (std::uint32_t t = 0; t < 64U; ++t)

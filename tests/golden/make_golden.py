@@ -11,6 +11,7 @@ hand.
 from __future__ import annotations
 
 import json
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -128,28 +129,140 @@ def whole_root_plants(tmp: Path):
     return out
 
 
+# Config-3 seeds at n=108: the six published roots (results/arwlf/holdout-snapshots)
+# and 26 fresh ones, 0x108001 .. 0x10801a.
+PUBLISHED_SEEDS_108 = [0x1001, 0x2003, 0x3007, 0x4001, 0x5003, 0x6007]
+FRESH_SEEDS_108 = [0x108000 + k for k in range(1, 27)]
+# Unplanted roots the reference's frozen ARWLF runs over all 4096 cells.
+WHOLE_ROOT_SEEDS_108 = [0x2003, 0x3007]
+WHOLE_ROOT_SLICES = 8
+JOBS = int(os.environ.get("TERGPU_GOLDEN_JOBS", max(1, min(7, (os.cpu_count() or 2) - 1))))
+
+_DIGEST_KEEP = ("triples", "triple_sum", "triple_xor", "triple_sum2", "full_q", "residue",
+                "residue_sum", "structural", "witnesses", "pairs", "projected_hits")
+
+
+def _snap_checksums(path: Path) -> list:
+    """The three per-list FNV-1a-64 checksums the reference wrote into its
+    .snap header (ter2_root/frozen/ter_root_snapshot.cpp:94-101)."""
+    sys.path.insert(0, str(HERE.parent.parent / "subset-sum-ter-fft_b200"))
+    import numpy as np
+
+    from tergpu import snapshot
+
+    head = np.fromfile(path, dtype=snapshot.HEADER_DTYPE, count=1)[0]
+    return [f"0x{int(c):016x}" for c in head["checksum"]]
+
+
+def _capture_108(tmp: Path, seed: int) -> tuple[Path, dict]:
+    snap = tmp / f"s108_{seed:x}.snap"
+    cap = O.ref_run("capture", 108, seed, 0, "auth", snap, timeout=3600)[0]
+    return snap, cap
+
+
 def seed_roots(tmp: Path):
-    """The six published n=108 roots (benchmark instance, attempt 0): the
-    reference's capture sizes and its frozen ARWLF over the declared 16-cell
-    sample with 32-bit projected counts (about 3 minutes per seed, in parallel)."""
+    """Config 3's 32 n=108 roots (benchmark instance, attempt 0): per seed the
+    reference's capture sizes, the three L1 list checksums of its .snap header
+    and its frozen ARWLF over the declared 16-cell sample with 32-bit projected
+    counts (about 3.5 minutes of one core per seed; seeds run in parallel)."""
     from concurrent.futures import ThreadPoolExecutor
 
     def one(seed):
-        snap = tmp / f"s108_{seed:x}.snap"
-        cap = O.ref_run("capture", 108, seed, 0, "auth", snap, timeout=3600)[0]
+        snap, cap = _capture_108(tmp, seed)
         row = O.ref_run("snaproot", snap, "arwlf", 16, 32, timeout=3600)[0]
+        sums = _snap_checksums(snap)
         snap.unlink()
-        keep = ("triples", "triple_sum", "triple_xor", "triple_sum2", "residue", "residue_sum",
-                "structural", "witnesses", "pairs", "projected_hits")
-        return {"seed": seed, "level1": cap["level1"], "level2": cap["level2"],
-                "arwlf16": {k: row[k] for k in keep}}
+        return {"seed": seed, "published": seed in PUBLISHED_SEEDS_108, "level1": cap["level1"],
+                "level2": cap["level2"], "file_bytes": cap["file_bytes"], "checksums": sums,
+                "arwlf16": {k: row[k] for k in _DIGEST_KEEP}}
 
-    seeds = [0x1001, 0x2003, 0x3007, 0x4001, 0x5003, 0x6007]
-    with ThreadPoolExecutor(max_workers=6) as pool:
-        return list(pool.map(one, seeds))
+    with ThreadPoolExecutor(max_workers=JOBS) as pool:
+        return list(pool.map(one, PUBLISHED_SEEDS_108 + FRESH_SEEDS_108))
 
 
-REFERENCE = Path("/root/reference")
+def merge_digests(rows: list) -> dict:
+    """Sink digests of disjoint cell slices combine field by field: counts and
+    multiset sums add (mod 2^64), the xor hash xors, witnesses concatenate
+    (RootSink::emit_triple, ter2_root/frozen/ter_root_queue_kernels.cpp:165-195)."""
+    out = {"triples": 0, "full_q": 0, "residue": 0, "structural": 0, "pairs": 0,
+           "projected_hits": 0, "cells": 0, "witnesses": []}
+    sums = {"triple_sum": 0, "triple_sum2": 0, "residue_sum": 0}
+    xor = 0
+    for r in rows:
+        for k in ("triples", "full_q", "residue", "structural", "pairs", "projected_hits", "cells"):
+            out[k] += int(r[k])
+        for k in sums:
+            sums[k] = (sums[k] + int(r[k], 16)) % (1 << 64)
+        xor ^= int(r["triple_xor"], 16)
+        out["witnesses"] += r["witnesses"]
+    out["witnesses"].sort()
+    for k, v in sums.items():
+        out[k] = f"0x{v:016x}"
+    out["triple_xor"] = f"0x{xor:016x}"
+    return out
+
+
+def whole_roots(tmp: Path):
+    """The reference's frozen ARWLF over every cell of unplanted n=108 roots
+    (seeds WHOLE_ROOT_SEEDS_108, attempt 0) with 32-bit projected counts: each
+    root runs as WHOLE_ROOT_SLICES disjoint cell slices in parallel processes
+    (about 3 hours of one core per root), merged with merge_digests."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=JOBS) as pool:
+        captures = list(pool.map(lambda seed: _capture_108(tmp, seed), WHOLE_ROOT_SEEDS_108))
+        specs = [f"mod:{WHOLE_ROOT_SLICES}:{i}:4096" for i in range(WHOLE_ROOT_SLICES)]
+        jobs = [(snap, spec) for snap, _ in captures for spec in specs]
+        rows = list(pool.map(
+            lambda job: O.ref_run("snaproot", job[0], "arwlf", job[1], 32, timeout=8 * 3600)[0],
+            jobs))
+    out = []
+    for k, (seed, (snap, cap)) in enumerate(zip(WHOLE_ROOT_SEEDS_108, captures)):
+        part = rows[k * WHOLE_ROOT_SLICES:(k + 1) * WHOLE_ROOT_SLICES]
+        out.append({"seed": seed, "attempt": 0, "level1": cap["level1"],
+                    "checksums": _snap_checksums(snap), "slices": WHOLE_ROOT_SLICES,
+                    "slice_ms": [r["ms"] for r in part], "arwlf": merge_digests(part)})
+        snap.unlink()
+    return out
+
+
+def attempt_telemetry(tmp: Path):
+    """solve_full_ter's per-attempt telemetry (every stage counter and output
+    fingerprint) and the run fingerprint, under FirstWitness (the reference's
+    default) and FullCanonicalOutput, for the n=36 cases of both generators and
+    the n=72 authentic roots: the anchor's attempt 0 and the 0x7201 solve that is
+    Found at attempt 21 (its root counters stop at the first witness)."""
+    out = []
+    cases = [(36, kind, seed, 8) for kind in ("auth", "build") for seed in (ANCHOR_SEED, 0x1001, 0x2A)]
+    cases += [(72, "auth", ANCHOR_SEED, 1), (72, "auth", 0x7201, 22)]
+    for n, kind, seed, attempts in cases:
+        for policy in ("first", "canon"):
+            rows = O.ref_run("solve", n, seed, attempts, kind, policy, 0, timeout=1800)
+            out.append({"n": n, "kind": kind, "seed": seed, "attempts": attempts, "policy": policy,
+                        "rows": rows[:-1], "final": rows[-1]})
+    return out
+
+
+def full_bench_rows(tmp: Path):
+    """The reference's own ter_full_bench (bench/ter_full_bench.cpp, built from its
+    sources into oracle/_ref/ter_full_bench): its CSV header and row for the
+    device command line to reproduce."""
+    import subprocess
+
+    binary = HERE.parent.parent / "oracle" / "_ref" / "ter_full_bench"
+    out = []
+    for n, seed, limit in ((36, ANCHOR_SEED, 8), (36, 0x1001, 8), (36, 0x2A, 8), (72, ANCHOR_SEED, 1),
+                           (72, 0x7201, 22)):
+        args = [f"--n={n}", f"--seed={seed}", f"--attempt-limit={limit}", "--warmup=0", "--repeat=1"]
+        proc = subprocess.run([str(binary), *args], capture_output=True, text=True, timeout=1800)
+        if proc.returncode != 0:
+            raise RuntimeError(f"ter_full_bench {args} failed: {proc.stderr}")
+        lines = [l for l in proc.stdout.splitlines() if l and not l.startswith("#")]
+        out.append({"args": args, "header": lines[0], "row": lines[1]})
+    return out
+
+
+REFERENCE = Path(os.environ.get("TER_REFERENCE_DIR", "/root/reference"))
 
 
 def published_runs(tmp: Path):
@@ -182,6 +295,9 @@ SECTIONS = {
     "root_reports": root_reports,
     "whole_root_plants": whole_root_plants,
     "seed_roots": seed_roots,
+    "whole_roots": whole_roots,
+    "attempt_telemetry": attempt_telemetry,
+    "full_bench_rows": full_bench_rows,
     "published_runs": published_runs,
 }
 
@@ -193,12 +309,15 @@ def main():
         raise SystemExit("oracle/_ref/terref missing: build it where the reference sources exist")
     wanted = sys.argv[1:] or list(SECTIONS)
     target = HERE / "reference_golden.json"
-    golden = json.loads(target.read_text()) if target.exists() else {}
-    with tempfile.TemporaryDirectory() as d:
+    # TERGPU_GOLDEN_TMP: where captures (0.84 GB each at n=108) are written
+    with tempfile.TemporaryDirectory(dir=os.environ.get("TERGPU_GOLDEN_TMP")) as d:
         for name in wanted:
-            golden[name] = SECTIONS[name](Path(d))
-    target.write_text(json.dumps(golden, indent=1, sort_keys=True) + "\n")
-    print("wrote", target, "sections", wanted)
+            section = SECTIONS[name](Path(d))
+            # re-read right before writing: another run may have written other sections
+            golden = json.loads(target.read_text()) if target.exists() else {}
+            golden[name] = section
+            target.write_text(json.dumps(golden, indent=1, sort_keys=True) + "\n")
+            print("wrote", target, "section", name, flush=True)
 
 
 if __name__ == "__main__":
