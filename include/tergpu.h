@@ -21,9 +21,12 @@
 extern "C" {
 #endif
 
-/* 2: tergpu_root_in / tergpu_root_records_in gained shard_index and shard_count;
- * callers compiled against another version must not call in (the adapter checks). */
-#define TERGPU_ABI_VERSION 2
+/* 2: tergpu_root_in / tergpu_root_records_in gained shard_index and shard_count.
+ * 3: tergpu_attempt_in gained root_policy, tergpu_attempt_stats the reference's
+ *    per-stage counters and output fingerprints, tergpu_attempt_out the run
+ *    fingerprint and the level-3 time.
+ * Callers compiled against another version must not call in (the adapter checks). */
+#define TERGPU_ABI_VERSION 3
 
 enum tergpu_status {
   TERGPU_COMPLETED = 0,
@@ -213,13 +216,32 @@ typedef struct {
   int32_t status;              /* TERGPU_FOUND or TERGPU_NO_WITNESS_THIS_ATTEMPT */
   uint64_t level2_sizes[9];
   uint64_t level1_sizes[3];
-  uint64_t level0_size;        /* distinct valid parents */
+  uint64_t level0_size;        /* parents the root policy retains (FirstWitness: 0 or 1) */
   uint64_t l3_modular;         /* L3 -> L2 pairs meeting the congruence */
   uint64_t l2_modular;         /* L2 -> L1 triples meeting the quotient congruence */
-  uint64_t root_modular;       /* full-Q root triples (residue-exact) */
-  uint64_t valid_roots;        /* ... with a binary weight-n/2 parent (pre-dedup) */
+  uint64_t root_modular;       /* root triples passing the full quotient (and, for Q > 64,
+                                  the residue words): FirstWitness counts up to the stop */
+  uint64_t valid_roots;        /* ... with a binary weight-n/2 parent, pre-dedup (the
+                                  reference's valid_root_count for the policy) */
   uint64_t root_pairs;         /* |L1_0| * |L1_1| */
   double l2_ms, l1_ms, root_ms, total_ms;
+  /* The reference's FullTerStageTelemetry counters (include/ter/full_ter.hpp:111-146)
+   * for level3_to_level2 (l3_*), level2_to_level1 (l2_*) and level1_to_level0 (root_*).
+   * Filled on every attempt; the root's low-prefilter count and the output
+   * fingerprints need TERGPU_ATTEMPT_TELEMETRY (0 without it). */
+  uint64_t attempt_seed;       /* seed + attempt */
+  uint64_t l3_pairs, l3_structural_rejects, l3_distribution_rejects, l3_survivors;
+  uint64_t l2_pairs, l2_structural_rejects, l2_distribution_rejects, l2_survivors;
+  uint64_t root_structural_rejects, root_distribution_rejects;
+  uint64_t root_low_prefilter;         /* triples equal on the low root_prefilter_bits */
+  uint64_t root_full_quotient_rejects; /* ... failing the full quotient / residue words */
+  uint32_t root_quotient_bits, root_prefilter_bits;
+  uint32_t root_policy;        /* the policy the root ran with (TERGPU_ROOT_POLICY_*) */
+  uint32_t root_early_stopped; /* FirstWitness stopped at a valid root */
+  uint64_t l2_fingerprint;     /* stage_fingerprint of the nine L2 lists */
+  uint64_t l1_fingerprint;     /* ... of the three L1 lists */
+  uint64_t l0_fingerprint;     /* ... of the retained L0 parents */
+  double verification_ms;      /* host verification of the witness */
 } tergpu_attempt_stats;
 
 /* tergpu_attempt_in.flags */
@@ -229,6 +251,11 @@ typedef struct {
                                           graph (fixed capacities, counts kept on the device);
                                           this flag runs the stage-by-stage path instead.
                                           Same results */
+#define TERGPU_ATTEMPT_TELEMETRY 8u    /* the reference's full attempt telemetry: the root's
+                                          low-prefilter count (one more count-only root
+                                          join), every stage's output_fingerprint (the
+                                          canonical lists are downloaded and hashed on the
+                                          host) and out->fingerprint.  Runs stage by stage */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return
@@ -246,7 +273,21 @@ typedef struct {
   uint64_t memory_limit_bytes; /* 0: no ceiling */
   const volatile int32_t *cancel; /* host flag, polled between stages; may be NULL */
   int32_t device;
+  uint32_t root_policy;        /* TERGPU_ROOT_POLICY_* (the numerics of ter::RootOutputPolicy,
+                                  include/ter/full_ter.hpp:79-83) */
 } tergpu_attempt_in;
+
+/* tergpu_attempt_in.root_policy.  FirstWitness (the reference's default): the
+ * root stops at the first valid triple in the order the reference's tiled
+ * reporter visits triples (src/tiled_q3report.cpp:365-410: window m = i + j of
+ * the prefilter buckets, bucket i of A, then A's and B's EntryIds, then C's
+ * EntryId descending); that triple's parent is the witness and the root's
+ * counters stop there.  FullCanonicalOutput: every valid parent, sorted and
+ * deduplicated; the witness is the first of them.  CountOnly: valid roots are
+ * counted, none is retained (no witness). */
+#define TERGPU_ROOT_POLICY_FIRST_WITNESS 0u
+#define TERGPU_ROOT_POLICY_COUNT_ONLY 1u
+#define TERGPU_ROOT_POLICY_FULL_CANONICAL 2u
 
 typedef struct {
   int32_t status;
@@ -266,6 +307,10 @@ typedef struct {
   uint64_t device_bytes_held;   /* device bytes the call's workspace held at its end (its peak:
                                    buffers only grow within a call; the shared workspace keeps
                                    buffers of earlier calls, a batch request starts empty) */
+  uint64_t fingerprint;         /* TERGPU_ATTEMPT_TELEMETRY: FullTerTelemetry::fingerprint
+                                   (src/full_ter.cpp:2532-2577) over the attempts this call ran
+                                   and the witness; the reference's value when attempt_first = 0 */
+  double level3_ms;             /* wall time of the level-3 enumeration */
 } tergpu_attempt_out;
 
 /* Replaces: solve_full_ter's attempt loop (src/full_ter.cpp:3125-3515) and

@@ -333,7 +333,8 @@ struct Solve {
   std::string message;
 };
 
-Solve solve(const Options& o, const Instance& inst, uint64_t seed, uint64_t time_limit_ms) {
+Solve solve(const Options& o, const Instance& inst, uint64_t seed, uint64_t time_limit_ms,
+            bool telemetry) {
   Solve s;
   s.stats.assign(o.attempt_limit, tergpu_attempt_stats{});
   volatile int32_t cancel = 0;
@@ -347,6 +348,9 @@ Solve solve(const Options& o, const Instance& inst, uint64_t seed, uint64_t time
   in.memory_limit_bytes = o.memory_limit_bytes;
   in.cancel = &cancel;
   in.device = o.device;
+  in.flags = telemetry ? TERGPU_ATTEMPT_TELEMETRY : 0u;
+  // the reference's bench keeps FirstWitness (include/ter/full_ter.hpp:105)
+  in.root_policy = TERGPU_ROOT_POLICY_FIRST_WITNESS;
   s.out.stats = s.stats.data();
   {
     const TimeGuard guard(time_limit_ms, &cancel);
@@ -438,7 +442,7 @@ int run_success_curve(const Options& o) {
       std::cerr << "failed to build benchmark instance for seed " << seed << '\n';
       return EXIT_FAILURE;
     }
-    const Solve s = solve(o, inst, seed, o.time_limit_ms);
+    const Solve s = solve(o, inst, seed, o.time_limit_ms, false);
     if (s.status == TERGPU_FOUND) {
       ++found;
       attempts_to_found.push_back(static_cast<uint64_t>(s.out.found_attempt) + 1);
@@ -494,7 +498,7 @@ int run_timed(const Options& o, const std::string& command) {
     return EXIT_FAILURE;
   }
   for (uint32_t i = 0; i < o.warmup; ++i) {
-    const Solve s = solve(o, inst, o.seed, o.time_limit_ms);
+    const Solve s = solve(o, inst, o.seed, o.time_limit_ms, true);
     if (!comparable(s.status)) {
       std::cerr << "full TER warmup did not reach a comparable terminal status: "
                 << status_name(s.status) << ": " << s.message << '\n';
@@ -502,9 +506,9 @@ int run_timed(const Options& o, const std::string& command) {
     }
   }
   Solve first;
-  std::vector<uint64_t> totals, binary, middle, root;
+  std::vector<uint64_t> totals, l3, binary, middle, root, verification;
   for (uint32_t rep = 0; rep < o.repeat; ++rep) {
-    Solve s = solve(o, inst, o.seed, o.time_limit_ms);
+    Solve s = solve(o, inst, o.seed, o.time_limit_ms, true);
     if (!comparable(s.status)) {
       std::cerr << "full TER run did not reach a comparable terminal status: "
                 << status_name(s.status) << ": " << s.message << '\n';
@@ -517,21 +521,20 @@ int run_timed(const Options& o, const std::string& command) {
     }
     const tergpu_attempt_stats& t = s.stats.back();
     totals.push_back(ns(s.out.total_ms));
+    l3.push_back(ns(s.out.level3_ms));
     binary.push_back(ns(t.l2_ms));
     middle.push_back(ns(t.l1_ms));
     root.push_back(ns(t.root_ms));
+    verification.push_back(ns(t.verification_ms));
     if (rep == 0) {
       first = std::move(s);
-    } else {
-      const tergpu_attempt_stats& f = first.stats.back();
-      if (s.status != first.status || s.stats.size() != first.stats.size() ||
-          std::memcmp(s.out.witness, first.out.witness, sizeof s.out.witness) != 0 ||
-          std::memcmp(t.level2_sizes, f.level2_sizes, sizeof f.level2_sizes) != 0 ||
-          std::memcmp(t.level1_sizes, f.level1_sizes, sizeof f.level1_sizes) != 0 ||
-          t.level0_size != f.level0_size || t.root_modular != f.root_modular) {
-        std::cerr << "full TER benchmark changed its exact result\n";
-        return EXIT_FAILURE;
-      }
+    } else if (s.status != first.status ||
+               std::memcmp(s.out.witness, first.out.witness, sizeof s.out.witness) != 0 ||
+               s.out.fingerprint != first.out.fingerprint) {
+      // the reference's repeat check: status, witness and telemetry fingerprint
+      // (bench/ter_full_bench.cpp:833-839)
+      std::cerr << "full TER benchmark changed its exact result\n";
+      return EXIT_FAILURE;
     }
   }
   const size_t executed = first.stats.size();
@@ -546,6 +549,10 @@ int run_timed(const Options& o, const std::string& command) {
     return EXIT_FAILURE;
   }
   const tergpu_attempt_stats& t = first.stats.back();
+  if (first.status == TERGPU_FOUND && t.status != TERGPU_FOUND) {
+    std::cerr << "Found result did not select a Found attempt\n";
+    return EXIT_FAILURE;
+  }
   std::vector<uint64_t> per_attempt;
   uint64_t sum_ns = 0, root_pairs = 0;
   for (const auto& a : first.stats) {
@@ -553,25 +560,75 @@ int run_timed(const Options& o, const std::string& command) {
     sum_ns += ns(a.total_ms);
     root_pairs += a.root_pairs;
   }
+  uint64_t l2_total = 0, l1_total = 0;
+  for (int i = 0; i < 9; ++i) l2_total += t.level2_sizes[i];
+  for (int i = 0; i < 3; ++i) l1_total += t.level1_sizes[i];
   print_metadata(o, command, executed);
+  // The reference's column set (bench/ter_full_bench.cpp:874-895).  Columns the
+  // device path has no counterpart for are printed empty: the CPU memory model
+  // (l3_list_bytes .. packed_vector_bytes except peak_working_bytes, which holds
+  // the device workspace's peak), the tiled reporter's internals (tile bits,
+  // probes, windows, auxiliary bytes, setup and scan times) and the root's
+  // output-byte accounting.  The device runs no tiled reporter (tiled_used 0)
+  // and materializes no pair records.
   std::cout << "status,n,r1,r2,L3_left,L3_right,L2_sizes,L1_sizes,L0,"
-               "l3_to_l2_ns,l2_to_l1_ns,l1_to_l0_ns,total_solver_ns,"
-               "binary_modular,middle_modular,root_pairs,root_modular,l1_to_l0_valid_roots,"
-               "peak_working_bytes,attempts_used,terminal_attempt_index,terminal_attempt_seed,"
-               "terminal_attempt_status,sum_attempt_ns,mean_attempt_ns,median_attempt_ns,"
-               "total_root_pair_candidates\n";
+               "l3_generation_ns,l3_to_l2_ns,l2_to_l1_ns,l1_to_l0_ns,"
+               "verification_ns,total_solver_ns,"
+               "binary_pairs,binary_modular,binary_structural_rejects,"
+               "binary_distribution_rejects,binary_survivors,binary_deduplicated,"
+               "middle_pairs,middle_modular,middle_structural_rejects,"
+               "middle_distribution_rejects,middle_survivors,middle_deduplicated,"
+               "root_pairs,root_modular,root_structural_rejects,"
+               "root_distribution_rejects,root_survivors,root_deduplicated,"
+               "l3_list_bytes,arithmetic_bytes,l2_list_bytes,l1_list_bytes,l0_list_bytes,"
+               "l2_active_bytes,l1_active_bytes,root_active_bytes,"
+               "peak_working_bytes,hot_entry_bytes,packed_vector_bytes,fingerprint,"
+               "l2_to_l1_tiled_used,l2_to_l1_pair_records,l2_to_l1_tile_bits,"
+               "l2_to_l1_tiled_pair_probes,l2_to_l1_tiled_nonempty_windows,"
+               "l2_to_l1_tiled_auxiliary_bytes,l2_to_l1_tiled_setup_ns,"
+               "l2_to_l1_tiled_scan_ns,"
+               "l1_to_l0_tiled_used,l1_to_l0_pair_records,l1_to_l0_quotient_bits,"
+               "l1_to_l0_prefilter_bits,l1_to_l0_low_prefilter_candidates,"
+               "l1_to_l0_full_quotient_rejects,l1_to_l0_tile_bits,"
+               "l1_to_l0_tiled_pair_probes,l1_to_l0_tiled_nonempty_windows,"
+               "l1_to_l0_tiled_auxiliary_bytes,l1_to_l0_tiled_setup_ns,"
+               "l1_to_l0_tiled_scan_ns,"
+               "l1_to_l0_root_policy,l1_to_l0_valid_roots,"
+               "l1_to_l0_early_stopped,l1_to_l0_output_peak_bytes,"
+               "l1_to_l0_output_live_bytes,l1_to_l0_working_peak_bytes,"
+               "l1_to_l0_first_witness_ceiling_bytes,"
+               "attempts_used,terminal_attempt_index,terminal_attempt_seed,"
+               "terminal_attempt_status,sum_attempt_ns,mean_attempt_ns,"
+               "median_attempt_ns,total_root_pair_candidates\n";
+  const char* empty = "";
   std::cout << status_name(first.status) << ',' << o.n << ',' << first.out.r1 << ','
             << first.out.r2 << ',' << first.out.level3_size << ',' << first.out.level3_size
             << ",\"" << join_sizes(t.level2_sizes, 9) << "\",\"" << join_sizes(t.level1_sizes, 3)
-            << "\"," << t.level0_size << ',' << median(binary) << ',' << median(middle) << ','
-            << median(root) << ',' << median(totals) << ',' << t.l3_modular << ','
-            << t.l2_modular << ',' << t.root_pairs << ',' << t.root_modular << ','
-            << t.valid_roots << ',' << first.out.device_bytes << ',' << executed << ','
-            << t.attempt << ',' << (o.seed + t.attempt) << ',' << status_name(t.status) << ','
-            << sum_ns << ',' << sum_ns / executed << ',' << median(per_attempt) << ','
+            << "\"," << t.level0_size << ',' << median(l3) << ',' << median(binary) << ','
+            << median(middle) << ',' << median(root) << ',' << median(verification) << ','
+            << median(totals) << ','
+            << t.l3_pairs << ',' << t.l3_modular << ',' << t.l3_structural_rejects << ','
+            << t.l3_distribution_rejects << ',' << t.l3_survivors << ',' << l2_total << ','
+            << t.l2_pairs << ',' << t.l2_modular << ',' << t.l2_structural_rejects << ','
+            << t.l2_distribution_rejects << ',' << t.l2_survivors << ',' << l1_total << ','
+            << t.root_pairs << ',' << t.root_modular << ',' << t.root_structural_rejects << ','
+            << t.root_distribution_rejects << ',' << t.valid_roots << ',' << t.level0_size << ',';
+  for (int i = 0; i < 8; ++i) std::cout << empty << ',';       // l3_list_bytes .. root_active_bytes
+  std::cout << first.out.device_bytes_held << ',' << empty << ',' << empty << ','
+            << first.out.fingerprint << ','
+            << 0 << ',' << 0 << ',';                               // tiled_used, pair_records
+  for (int i = 0; i < 6; ++i) std::cout << empty << ',';       // l2_to_l1 tiled internals
+  std::cout << 0 << ',' << 0 << ',' << t.root_quotient_bits << ',' << t.root_prefilter_bits << ','
+            << t.root_low_prefilter << ',' << t.root_full_quotient_rejects << ',';
+  for (int i = 0; i < 6; ++i) std::cout << empty << ',';       // l1_to_l0 tiled internals
+  std::cout << t.root_policy << ',' << t.valid_roots << ',' << t.root_early_stopped << ',';
+  for (int i = 0; i < 4; ++i) std::cout << empty << ',';       // root output bytes
+  std::cout << executed << ',' << t.attempt << ',' << t.attempt_seed << ',' << status_name(t.status)
+            << ',' << sum_ns << ',' << sum_ns / executed << ',' << median(per_attempt) << ','
             << root_pairs << '\n';
   if (o.require_found && first.status != TERGPU_FOUND) {
-    std::cerr << "status is " << status_name(first.status) << " and --require-found was requested\n";
+    std::cerr << "--require-found: terminal status was " << status_name(first.status)
+              << ", not Found\n";
     return EXIT_FAILURE;
   }
   return EXIT_SUCCESS;

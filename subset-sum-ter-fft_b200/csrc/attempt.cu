@@ -200,6 +200,7 @@ struct GraphCounts {      // device counts the host reads after an attempt
   unsigned long long l1[3];
   unsigned long long root_counters[kCounters];
   unsigned long long auth[3];
+  unsigned long long l1rej[3][2];  // per group: structural, distribution rejects
   unsigned int overflow;  // a segment above the canonical-sort capacity
 };
 
@@ -254,6 +255,159 @@ struct GraphPlan {
   }
 };
 
+// ---- the reference's telemetry hashes (src/full_ter.cpp:2431-2577): a chain
+// hash ^= value, hash *= 1099511628211 from 1469598103934665603 over 64-bit values.
+struct Fnv64 {
+  uint64_t h = 1469598103934665603ULL;
+  void mix(uint64_t v) {
+    h ^= v;
+    h *= 1099511628211ULL;
+  }
+};
+
+// One BigEntry of stage_fingerprint: digits.n, the packed digit words (W64
+// positive then W64 negative, all zero at FiniteSanity), then the residue's
+// 32-bit words without the zero words above the top one (BigInt keeps none).
+void mix_entry(Fnv64& f, uint32_t n, uint64_t pos0, uint64_t pos1, u128 res) {
+  const uint32_t w64 = (n + 63) / 64;
+  f.mix(n);
+  f.mix(pos0);
+  if (w64 > 1) f.mix(pos1);
+  for (uint32_t k = 0; k < w64; ++k) f.mix(0);
+  uint32_t words = 4;
+  while (words > 0 && (uint32_t)(res >> (32 * (words - 1))) == 0) --words;
+  for (uint32_t k = 0; k < words; ++k) f.mix((uint32_t)(res >> (32 * k)));
+}
+
+// stage_fingerprint of `count` device lists in canonical order: each list's
+// size, then its entries (downloaded to the host; the chain is sequential).
+uint64_t lists_fingerprint(Workspace& w, uint32_t n, const EntryArrays* lists, const uint64_t* sizes,
+                           int count, cudaStream_t st) {
+  Fnv64 f;
+  std::vector<uint64_t> p0, p1, rl, rh;
+  for (int l = 0; l < count; ++l) {
+    const uint64_t m = sizes[l];
+    f.mix(m);
+    if (m == 0) continue;
+    p0.resize(m);
+    p1.resize(m);
+    rl.resize(m);
+    rh.resize(m);
+    check(cudaMemcpyAsync(p0.data(), lists[l].pos0, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(p1.data(), lists[l].pos1, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(rl.data(), lists[l].res_lo, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(rh.data(), lists[l].res_hi, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    sync_stream(w, st, "fingerprint");
+    for (uint64_t i = 0; i < m; ++i) mix_entry(f, n, p0[i], p1[i], ((u128)rh[i] << 64) | rl[i]);
+  }
+  return f.h;
+}
+
+// The root's prefilter width and tile bits: min(24, Q, 32) and min(15, p)
+// (src/full_ter.cpp:1681-1686, include/ter/limitations.hpp:563-570).
+uint32_t root_prefilter_bits(uint32_t Q) { return std::min<uint32_t>(std::min<uint32_t>(24, Q), 32); }
+uint32_t root_tile_bits(uint32_t p) { return std::min<uint32_t>(15, p); }
+
+// Position of a root triple in the reference's tiled visit order (see
+// VisitBound): window m, bucket i of A, A's and B's EntryIds, then C's EntryId
+// descending.
+struct VisitKey {
+  uint32_t m, i, a, b, c;
+  bool before(const VisitKey& o) const {
+    if (m != o.m) return m < o.m;
+    if (i != o.i) return i < o.i;
+    if (a != o.a) return a < o.a;
+    if (b != o.b) return b < o.b;
+    return c > o.c;
+  }
+};
+
+// The root's outcome under the attempt's policy, from its full-Q triples and
+// their authority flags (k_authority): the retained parents (canonical order)
+// and the reference's root counters (the visitor's, src/full_ter.cpp:1537-1622).
+struct RootOutcome {
+  uint64_t modular = 0, structural = 0, distribution = 0, valid = 0;
+  bool stopped = false;  // FirstWitness stopped at `stop`
+  VisitKey stop{};
+  std::vector<std::array<uint64_t, 2>> parents;
+};
+
+RootOutcome pick_root(uint32_t n, uint32_t Q, uint32_t policy, const uint32_t* trip, const uint8_t* flags,
+                      uint64_t count, const uint64_t* d_key_a, const uint64_t* d_key_b,
+                      uint8_t* const recs[3], uint32_t rb) {
+  const uint32_t w64 = (n + 63) / 64;
+  RootOutcome o;
+  std::vector<uint64_t> mod;  // the visitor's modular candidates
+  for (uint64_t i = 0; i < count; ++i) {
+    if ((flags[i] & 1) != 0) {
+      mod.push_back(i);
+    } else if (Q <= 64) {
+      // a decisive quotient match always has the exact residue
+      t_error = "root triple with a full quotient match but another residue";
+      throw Failure{TERGPU_INVARIANT_VIOLATION};
+    }
+  }
+  auto parent_of = [&](uint64_t i) {
+    std::array<uint64_t, 2> p{0, 0};
+    for (int l = 0; l < 3; ++l) {
+      uint32_t wds[4] = {0, 0, 0, 0};  // the record's pos words (w64 <= 2)
+      check(cudaMemcpy(wds, recs[l] + (uint64_t)trip[3 * i + l] * rb, w64 * 8, cudaMemcpyDeviceToHost),
+            "record download");
+      p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
+      if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
+    }
+    return p;
+  };
+  bool any_valid = false;
+  for (uint64_t i : mod) any_valid = any_valid || (flags[i] & 4) != 0;
+  std::vector<uint64_t> counted = mod;
+  if (policy == TERGPU_ROOT_POLICY_FIRST_WITNESS && any_valid) {
+    const uint32_t p = root_prefilter_bits(Q), tb = root_tile_bits(p);
+    const uint64_t pm = (1ull << p) - 1ull;
+    std::vector<VisitKey> keys(mod.size());
+    int64_t first = -1;
+    for (size_t k = 0; k < mod.size(); ++k) {
+      const uint64_t i = mod[k];
+      uint64_t ka = 0, kb = 0;
+      check(cudaMemcpy(&ka, d_key_a + trip[3 * i], 8, cudaMemcpyDeviceToHost), "key download");
+      check(cudaMemcpy(&kb, d_key_b + trip[3 * i + 1], 8, cudaMemcpyDeviceToHost), "key download");
+      const uint32_t bi = (uint32_t)((ka & pm) >> tb);
+      keys[k] = VisitKey{bi + (uint32_t)((kb & pm) >> tb), bi, trip[3 * i], trip[3 * i + 1], trip[3 * i + 2]};
+      if ((flags[i] & 4) != 0 && (first < 0 || keys[k].before(keys[first]))) first = (int64_t)k;
+    }
+    o.stopped = true;
+    o.stop = keys[first];
+    counted.clear();
+    for (size_t k = 0; k < mod.size(); ++k)
+      if (!o.stop.before(keys[k])) counted.push_back(mod[k]);  // visited up to the stop
+    o.parents.push_back(parent_of(mod[first]));
+  }
+  o.modular = counted.size();
+  for (uint64_t i : counted) {
+    o.structural += (flags[i] >> 3) & 1;
+    o.distribution += (flags[i] >> 4) & 1;
+    o.valid += (flags[i] >> 2) & 1;
+  }
+  if (o.stopped) {
+    o.valid = 1;
+  } else if (policy == TERGPU_ROOT_POLICY_FULL_CANONICAL) {
+    for (uint64_t i : counted)
+      if ((flags[i] & 4) != 0) o.parents.push_back(parent_of(i));
+    std::sort(o.parents.begin(), o.parents.end());
+    o.parents.erase(std::unique(o.parents.begin(), o.parents.end()), o.parents.end());
+  }
+  return o;
+}
+
+// stage_fingerprint of the retained L0 parents: each parent's digits and the
+// root target as its residue (every retained parent is residue-exact).
+uint64_t l0_fingerprint(uint32_t n, const std::vector<std::array<uint64_t, 2>>& parents, u128 T) {
+  Fnv64 f;
+  f.mix(parents.size());
+  for (const auto& p : parents) mix_entry(f, n, p[0], p[1], T);
+  return f.h;
+}
+
 // Expected level sizes of the FiniteSanity shape (the preflight's means).
 double expected_l1(uint64_t l3, uint32_t r1, uint32_t r2) {
   const double l2 = (double)l3 * l3 / std::ldexp(1.0, r2);
@@ -307,7 +461,7 @@ void capture_attempt(GraphPlan& g, cudaStream_t st) {
     launch_copy_count(&g.jb.counters[kTriples], &dc->l2_triples[grp], st);
     launch_l1_parents(g.jb.triples, Count(g.cap_t, &g.jb.counters[kTriples]), as_const(g.l2all),
                       as_const(g.l2all), as_const(g.l2all), n, n / 6, g.cand, &dc->ncand[grp], st,
-                      &dc->bounds[3 * grp]);
+                      &dc->bounds[3 * grp], dc->l1rej[grp]);
     radix_sort_entries(as_const(g.cand), Count(g.cap_t, &dc->ncand[grp]), vary0, vary1, g.perm,
                        g.sort_scratch, st);
     launch_gather_unique(as_const(g.cand), g.perm, Count(g.cap_t, &dc->ncand[grp]), g.l1[grp], g.flags,
@@ -486,8 +640,8 @@ void graph_level3(GraphPlan& g, const std::vector<uint64_t>& weights, cudaStream
 
 // One attempt through the graph.  False when a capacity overflowed (the
 // attempt then runs stage by stage); else stats and the valid parents.
-bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, tergpu_attempt_stats* stat,
-                   std::vector<std::array<uint64_t, 2>>* parents, cudaStream_t st) {
+bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, uint32_t policy,
+                   tergpu_attempt_stats* stat, RootOutcome* root, cudaStream_t st) {
   const uint32_t n = g.n, r1 = g.r1, r2 = g.r2;
   const uint32_t b1 = std::min(r1, r2 + 32);
   const u128 m1 = mask128(b1), m2 = mask128(r2), nmask = mask128(n);
@@ -530,25 +684,20 @@ bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, tergpu
   if (overflow) return false;
   for (int i = 0; i < 9; ++i) stat->level2_sizes[i] = c.kept9[i];
   stat->l3_modular = c.bounds[9];
+  stat->l3_survivors = c.bounds[9];
   stat->l2_modular = c.l2_triples[0] + c.l2_triples[1] + c.l2_triples[2];
+  for (int grp = 0; grp < 3; ++grp) {
+    stat->l2_pairs += c.kept9[3 * grp] * c.kept9[3 * grp + 1];
+    stat->l2_structural_rejects += c.l1rej[grp][0];
+    stat->l2_distribution_rejects += c.l1rej[grp][1];
+    stat->l2_survivors += c.ncand[grp];
+  }
   for (int l = 0; l < 3; ++l) stat->level1_sizes[l] = c.l1[l];
   stat->root_pairs = c.l1[0] * c.l1[1];
-  stat->root_modular = c.root_counters[kTriples];
   const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
   const uint32_t rb = 16 * w64 + 4 * w32;
-  for (uint64_t i = 0; i < c.root_counters[kTriples]; ++i) {
-    if ((g.h_aflags[i] & 4) == 0) continue;
-    ++stat->valid_roots;
-    std::array<uint64_t, 2> p{0, 0};
-    for (int l = 0; l < 3; ++l) {
-      uint32_t wds[4] = {0, 0, 0, 0};  // the record's pos words (w64 <= 2)
-      check(cudaMemcpy(wds, g.recs[l] + (uint64_t)g.h_triples[3 * i + l] * rb, w64 * 8,
-                       cudaMemcpyDeviceToHost), "record download");
-      p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
-      if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
-    }
-    parents->push_back(p);
-  }
+  *root = pick_root(n, n - r1, policy, g.h_triples, g.h_aflags, c.root_counters[kTriples], g.rk_lo[0],
+                    g.rk_lo[1], g.recs, rb);
   return true;
 }
 
@@ -628,8 +777,15 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   // n = 36 and 72: each attempt as one captured graph (not for L1 exports)
   const bool exporting = (in->flags & TERGPU_ATTEMPT_CAPTURE_ONLY) != 0 || out->l1_records[0] != nullptr ||
                          out->l1_records[1] != nullptr || out->l1_records[2] != nullptr;
+  const bool telemetry = (in->flags & TERGPU_ATTEMPT_TELEMETRY) != 0;
+  const uint32_t policy = in->root_policy;
+  if (policy > TERGPU_ROOT_POLICY_FULL_CANONICAL) {
+    t_error = "root_policy must be FirstWitness (0), CountOnly (1) or FullCanonicalOutput (2)";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
+  const auto t_l3 = std::chrono::steady_clock::now();
   GraphPlan* plan = nullptr;
-  if (!exporting && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
+  if (!exporting && !telemetry && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
     plan = graph_plan(w, n, r1, r2, l3, st);
     held.plan = plan;
     if (plan != nullptr) graph_level3(*plan, weights, st);
@@ -656,6 +812,9 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     check(cudaGetLastError(), "level 3");
   };
   if (plan == nullptr) dynamic_level3();
+  sync_stream(w, st, "level 3");
+  out->level3_ms = ms_since(t_l3);
+  std::vector<tergpu_attempt_stats> run;  // every attempt's stats (the run fingerprint)
 
   int status = TERGPU_ATTEMPT_LIMIT_REACHED;
   out->attempts_run = 0;
@@ -667,12 +826,12 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     std::memset(&stat, 0, sizeof stat);
     stat.attempt = attempt;
     const Targets tg = random_targets(in->seed + attempt, r1, r2, T);
-    std::vector<std::array<uint64_t, 2>> parents;
+    RootOutcome root;
     bool graphed = false;
     if (plan != nullptr) {
-      graphed = graph_attempt(*plan, w, tg, T, &stat, &parents, st);
+      graphed = graph_attempt(*plan, w, tg, T, policy, &stat, &root, st);
       if (!graphed) {  // a capacity overflowed: this attempt runs stage by stage
-        parents.clear();
+        root = RootOutcome{};
         std::memset(&stat, 0, sizeof stat);
         stat.attempt = attempt;
         dynamic_level3();
@@ -718,7 +877,9 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       for (int i = 0; i < 9; ++i) l2n[i] = canonicalize(w, view(raw, hb[i]), sg.cnt[i], l2[i], st);
     }
     for (int i = 0; i < 9; ++i) stat.level2_sizes[i] = l2n[i];
+    stat.l3_survivors = stat.l3_modular;
     check(cudaGetLastError(), "L3 -> L2");
+    if (telemetry) stat.l2_fingerprint = lists_fingerprint(w, n, l2.data(), l2n.data(), 9, st);
     stat.l2_ms = ms_since(t_att);
     cancelled_check(in);
 
@@ -768,14 +929,20 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       EntryArrays cand = entry_slot(w, S_CAND, jr.triples);
       unsigned long long* acc = ensure<unsigned long long>(w, S_ACC, 64);
       launch_l1_parents(jr.d_triples, jr.triples, as_const(l2[3 * g]), as_const(l2[3 * g + 1]),
-                        as_const(l2[3 * g + 2]), n, n / 6, cand, acc + 4, st);
-      unsigned long long ncand = 0;
-      download(w, &ncand, acc + 4, 1, st);
+                        as_const(l2[3 * g + 2]), n, n / 6, cand, acc + 4, st, nullptr, acc + 6);
+      unsigned long long lc[4] = {0, 0, 0, 0};  // kept, (unused), structural, distribution rejects
+      download(w, lc, acc + 4, 4, st);
+      const unsigned long long ncand = lc[0];
+      stat.l2_pairs += l2n[3 * g] * l2n[3 * g + 1];
+      stat.l2_structural_rejects += lc[2];
+      stat.l2_distribution_rejects += lc[3];
+      stat.l2_survivors += ncand;
       l1[g] = entry_slot(w, S_L1 + 4 * g, ncand);
       l1n[g] = canonicalize(w, cand, ncand, l1[g], st);
       stat.level1_sizes[g] = l1n[g];
     }
     check(cudaGetLastError(), "L2 -> L1");
+    if (telemetry) stat.l1_fingerprint = lists_fingerprint(w, n, l1.data(), l1n.data(), 3, st);
     stat.l1_ms = ms_since(t_l1);
     cancelled_check(in);
 
@@ -845,7 +1012,6 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       jr = run_join(w, j, 0);
     }
     stat.root_pairs = jr.pairs;
-    stat.root_modular = jr.triples;
     std::vector<uint32_t> htrip;
     std::vector<uint8_t> hflags;
     if (jr.triples != 0) {
@@ -873,35 +1039,55 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       check(cudaMemcpyAsync(hflags.data(), dflags, jr.triples, cudaMemcpyDeviceToHost, st), "d2h");
       sync_stream(w, st, "sync");
     }
-    // valid roots: parents of the flagged triples
-    for (uint64_t i = 0; i < jr.triples; ++i) {
-      if ((hflags[i] & 4) == 0) continue;
-      ++stat.valid_roots;
-      std::array<uint64_t, 2> p{0, 0};
-      for (int l = 0; l < 3; ++l) {
-        uint32_t wds[4] = {0, 0, 0, 0};  // the record's pos words (w64 <= 2)
-        check(cudaMemcpy(wds, recs[l] + (uint64_t)htrip[3 * i + l] * rb, w64 * 8, cudaMemcpyDeviceToHost),
-              "record download");
-        p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
-        if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
+    root = pick_root(n, Q, policy, htrip.data(), hflags.data(), jr.triples, j.key_lo[0], j.key_lo[1], recs, rb);
+    if (telemetry) {
+      // the reporter's low-prefilter candidates: triples equal on the low p
+      // bits, counted up to the FirstWitness stop when there is one
+      const uint32_t pbits = root_prefilter_bits(Q);
+      JoinInput jp = j;
+      jp.projected_bits = pbits;
+      jp.count_only = true;
+      jp.capacity = 0;
+      if (root.stopped) {
+        jp.visit = VisitBound{1u, pbits, root_tile_bits(pbits), root.stop.m, root.stop.i, root.stop.a,
+                              root.stop.b, root.stop.c};
       }
-      parents.push_back(p);
+      const JoinResult pr = run_join(w, jp, 0);
+      stat.root_low_prefilter = pr.projected + (root.stopped ? 1 : 0);
     }
     stat.root_ms = ms_since(t_root);
     // L1 export of the attempt (records + targets), when the caller asked for it
     export_l1();
     }  // stage by stage
-    // the valid roots' distinct parents in canonical order (sorted, unique)
-    std::sort(parents.begin(), parents.end());
-    parents.erase(std::unique(parents.begin(), parents.end()), parents.end());
+    // the root's counters under the policy and the retained parents (level 0)
+    const uint32_t Qr = n - r1;
+    const auto& parents = root.parents;
+    stat.attempt_seed = in->seed + attempt;
+    stat.l3_pairs = 9ull * l3 * l3;  // every L3 -> L2 merge pairs the two halves
+    // the halves cover disjoint coordinates and hold n/36 ones each, so every
+    // L3 -> L2 parent is binary with n/18 ones: add_three rejects none
+    stat.l3_structural_rejects = 0;
+    stat.l3_distribution_rejects = 0;
+    stat.root_modular = root.modular;
+    stat.root_structural_rejects = root.structural;
+    stat.root_distribution_rejects = root.distribution;
+    stat.valid_roots = root.valid;
+    stat.root_quotient_bits = Qr;
+    stat.root_prefilter_bits = root_prefilter_bits(Qr);
+    stat.root_policy = policy;
+    stat.root_early_stopped = root.stopped ? 1u : 0u;
+    if (telemetry) {
+      stat.root_full_quotient_rejects = stat.root_low_prefilter - stat.root_modular;
+      stat.l0_fingerprint = l0_fingerprint(n, parents, T);
+    }
     stat.level0_size = parents.size();
-    stat.total_ms = ms_since(t_att);
     stat.status = parents.empty() ? TERGPU_NO_WITNESS_THIS_ATTEMPT : TERGPU_FOUND;
-    if (out->stats != nullptr) out->stats[k] = stat;
     out->attempts_run = k + 1;
 
     if (!parents.empty()) {
-      // verify the lowest parent: binary digits, weight n/2, weights sum to the target
+      // verify the retained parent (the policy's witness): binary digits,
+      // weight n/2, weights sum to the target (src/full_ter.cpp:2879-2908)
+      const auto t_ver = std::chrono::steady_clock::now();
       const auto& p = parents.front();
       u128 acc = 0;
       uint32_t weight = 0;
@@ -913,14 +1099,54 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
         ++weight;
         acc = (acc + ((u128)weights[2 * i + 1] << 64 | weights[2 * i])) & nmask;
       }
+      stat.verification_ms = ms_since(t_ver);
       if (weight != n / 2 || acc != T) {
         t_error = "root witness fails verification";
         return TERGPU_INVARIANT_VIOLATION;
       }
       out->found_attempt = attempt;
       status = TERGPU_FOUND;
-      break;
     }
+    stat.total_ms = ms_since(t_att);
+    if (out->stats != nullptr) out->stats[k] = stat;
+    run.push_back(stat);
+    if (status == TERGPU_FOUND) break;
+  }
+  if (telemetry) {
+    // FullTerTelemetry::fingerprint (src/full_ter.cpp:2532-2577)
+    Fnv64 f;
+    if (status == TERGPU_FOUND)
+      for (uint32_t i = 0; i < n; ++i) f.mix((uint64_t)out->witness[i] + 1u);
+    f.mix(in->seed);
+    f.mix(n);
+    f.mix(n);  // modulus bits: the full TER modulus is 2^n
+    f.mix(0);  // TerExecutionMode::FullTer
+    f.mix(0);  // ShapeFamily::FiniteSanity
+    f.mix(r1);
+    f.mix(r2);
+    f.mix(l3);
+    f.mix(l3);
+    f.mix(run.size());
+    for (const auto& a : run) {
+      f.mix(a.attempt_seed);
+      f.mix(a.attempt);
+      f.mix((uint64_t)a.status);
+      for (int i = 0; i < 9; ++i) f.mix(a.level2_sizes[i]);
+      for (int i = 0; i < 3; ++i) f.mix(a.level1_sizes[i]);
+      f.mix(a.level0_size);
+      f.mix(a.l3_modular);
+      f.mix(a.l2_modular);
+      f.mix(a.root_modular);
+      f.mix(a.root_quotient_bits);
+      f.mix(a.root_prefilter_bits);
+      f.mix(a.root_low_prefilter);
+      f.mix(a.root_full_quotient_rejects);
+      f.mix(0);  // pair_records: the root materializes no pair records
+      f.mix(a.l2_fingerprint);
+      f.mix(a.l1_fingerprint);
+      f.mix(a.l0_fingerprint);
+    }
+    out->fingerprint = f.h;
   }
   out->status = status;
   out->total_ms = ms_since(t_call);

@@ -442,7 +442,8 @@ __global__ void k_l2_quotients(ConstEntryArrays l, Count cnt, const uint32_t* __
 __global__ void k_l1_parents(const uint32_t* __restrict__ triples, Count ntc, ConstEntryArrays x,
                              ConstEntryArrays y, ConstEntryArrays z, const uint32_t* __restrict__ doff,
                              uint32_t n, uint32_t ones, EntryArrays out,
-                             unsigned long long* __restrict__ count) {
+                             unsigned long long* __restrict__ count,
+                             unsigned long long* __restrict__ rejects) {
   if (doff != nullptr) {
     x = offset_view(x, doff[0]);
     y = offset_view(y, doff[1]);
@@ -450,16 +451,25 @@ __global__ void k_l1_parents(const uint32_t* __restrict__ triples, Count ntc, Co
   }
   const u128 nm = nmask128(n);
   const uint64_t nt = ntc.get();
+  unsigned long long c_struct = 0, c_dist = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nt;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t a = triples[3 * i], b = triples[3 * i + 1], c = triples[3 * i + 2];
     const uint64_t a0 = x.pos0[a], a1 = x.pos1[a], b0 = y.pos0[b], b1 = y.pos1[b];
     const uint64_t c0 = z.pos0[c], c1 = z.pos1[c];
     // binary digits: a coordinate set in two children leaves {-1, 0, 1}
+    // (add_three's structural reject); then the digit counts (its distribution reject)
     const uint64_t two0 = (a0 & b0) | (a0 & c0) | (b0 & c0);
     const uint64_t two1 = (a1 & b1) | (a1 & c1) | (b1 & c1);
     const uint64_t p0 = a0 | b0 | c0, p1 = a1 | b1 | c1;
-    if ((two0 | two1) != 0 || (uint32_t)(__popcll(p0) + __popcll(p1)) != ones) continue;
+    if ((two0 | two1) != 0) {
+      ++c_struct;
+      continue;
+    }
+    if ((uint32_t)(__popcll(p0) + __popcll(p1)) != ones) {
+      ++c_dist;
+      continue;
+    }
     const u128 s = ((((u128)x.res_hi[a] << 64) | x.res_lo[a]) + (((u128)y.res_hi[b] << 64) | y.res_lo[b]) +
                     (((u128)z.res_hi[c] << 64) | z.res_lo[c])) & nm;
     const unsigned long long at = atomicAdd(count, 1ull);
@@ -467,6 +477,16 @@ __global__ void k_l1_parents(const uint32_t* __restrict__ triples, Count ntc, Co
     out.pos1[at] = p1;
     out.res_lo[at] = (uint64_t)s;
     out.res_hi[at] = (uint64_t)(s >> 64);
+  }
+  if (rejects != nullptr) {
+    for (int d = 16; d > 0; d >>= 1) {
+      c_struct += __shfl_down_sync(0xFFFFFFFFu, c_struct, d);
+      c_dist += __shfl_down_sync(0xFFFFFFFFu, c_dist, d);
+    }
+    if ((threadIdx.x & 31u) == 0u) {
+      if (c_struct != 0) atomicAdd(&rejects[0], c_struct);
+      if (c_dist != 0) atomicAdd(&rejects[1], c_dist);
+    }
   }
 }
 
@@ -723,11 +743,13 @@ void launch_l2_quotients(ConstEntryArrays l, Count count, uint32_t b1, uint32_t 
 
 void launch_l1_parents(const uint32_t* triples, Count ntriples, ConstEntryArrays x, ConstEntryArrays y,
                        ConstEntryArrays z, uint32_t n, uint32_t expected_ones, EntryArrays out,
-                       unsigned long long* count, cudaStream_t st, const uint32_t* doff) {
+                       unsigned long long* count, cudaStream_t st, const uint32_t* doff,
+                       unsigned long long* rejects) {
   cudaMemsetAsync(count, 0, 8, st);
+  if (rejects != nullptr) cudaMemsetAsync(rejects, 0, 16, st);
   if (ntriples.cap == 0) return;
   k_l1_parents<<<blocks_for_count(ntriples, 256), 256, 0, st>>>(triples, ntriples, x, y, z, doff, n,
-                                                              expected_ones, out, count);
+                                                              expected_ones, out, count, rejects);
 }
 
 uint64_t radix_scratch_words(uint64_t count) {

@@ -104,10 +104,13 @@ void launch_l2_quotients(ConstEntryArrays l, Count count, uint32_t b1, uint32_t 
 // exactly n/6 ones; valid parents are written compacted (order irrelevant: the
 // canonical sort follows).  *count receives the number written.
 // doff (device, may be null): x, y, z start doff[0], doff[1], doff[2] entries in.
+// rejects (device, may be null): [0] += triples whose children overlap (add_three's
+// structural rejects), [1] += disjoint triples with the wrong digit count (its
+// distribution rejects); cleared first.
 void launch_l1_parents(const uint32_t* triples, Count ntriples, ConstEntryArrays x,
                        ConstEntryArrays y, ConstEntryArrays z, uint32_t n, uint32_t expected_ones,
                        EntryArrays out, unsigned long long* count, cudaStream_t st,
-                       const uint32_t* doff = nullptr);
+                       const uint32_t* doff = nullptr, unsigned long long* rejects = nullptr);
 
 // Stable LSD radix sort of `count` entries by (pos0, pos1) as one 128-bit key
 // with pos0 most significant (the reference's packed_less on the word vector),

@@ -28,6 +28,25 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 template <uint32_t BITS = kYHashBits>
 __device__ __forceinline__ uint32_t yhash_of(uint32_t w) { return (w * 0x9E3779B1u) >> (32 - BITS); }
 
+// Whether a projected hit (A entry at qat, B entry at xat of families s and t,
+// D entry at yat) counts under the visit bound (VisitBound, root_kernels.cuh).
+__device__ __forceinline__ bool visit_counts(const SweepArgs& a, uint32_t s, uint32_t t, uint64_t qat,
+                                             uint64_t xat, uint64_t yat) {
+  const VisitBound& v = a.visit;
+  if (v.on == 0u) return true;
+  const uint64_t pm = (1ull << v.pbits) - 1ull;
+  const uint64_t ka = ((a.q.res[qat] << a.fb) | s) & pm;
+  const uint64_t kb = ((a.x.res[xat] << a.fb) | t) & pm;
+  const uint32_t i = static_cast<uint32_t>(ka >> v.tb);
+  const uint32_t m = i + static_cast<uint32_t>(kb >> v.tb);
+  if (m != v.m) return m < v.m;
+  if (i != v.i) return i < v.i;
+  const uint32_t ia = a.q.id[qat], ib = a.x.id[xat], ic = a.y.id[yat];
+  if (ia != v.a) return ia < v.a;
+  if (ib != v.b) return ib < v.b;
+  return ic > v.c;
+}
+
 template <bool ALIGNED>
 __device__ __forceinline__ uint32_t window_of(uint64_t r, uint32_t mrb) {
   // ALIGNED (fewer than 32 residual bits compared): left-align so the 32-bit
@@ -270,7 +289,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
         auto check = [&](uint32_t idx) {
           if ((a.y.res[yoff + idx] & mmask) != ms) return;
           if (a.project) {
-            ++c_proj;
+            if (visit_counts(a, s, t, qoff + qi, xoff + xi, yoff + idx)) ++c_proj;
             return;
           }
           ++c_fast;
@@ -466,7 +485,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
               const uint64_t ms = sum & mmask;
               if ((a.y.res[yoff + idx] & mmask) != ms) return;
               if (a.project) {
-                ++c_proj;
+                if (visit_counts(a, s, t, qoff + qi, xoff + xi, yoff + idx)) ++c_proj;
                 return;
               }
               ++c_fast;
@@ -684,7 +703,7 @@ __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a)
               const uint64_t ms = sum & mmask;
               if ((a.y.res[yoff + idx] & mmask) != ms) return;
               if (a.project) {
-                ++c_proj;
+                if (visit_counts(a, s, t, qoff + qi, xoff + xi, yoff + idx)) ++c_proj;
                 return;
               }
               ++c_fast;
@@ -1004,6 +1023,10 @@ __global__ void k_authority(const AuthorityArgs a) {
       }
       if (ok && nneg == 2u && npos == 2u + a.n / 6u) flags |= 2;
       if (ok && nneg == 0u && npos == a.n / 2u) flags |= 4;
+      // add_three's verdict against the root counts {n/2 zero, n/2 positive}
+      // (src/full_ter.cpp:732-790): invalid digits, else wrong digit counts
+      if (!ok) flags |= 8;
+      else if (!(nneg == 0u && npos == a.n / 2u)) flags |= 16;
     }
     if (a.flags != nullptr) a.flags[i] = flags;
     c_res += flags & 1;

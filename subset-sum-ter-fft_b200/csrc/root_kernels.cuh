@@ -44,6 +44,20 @@ struct ListView {
   const uint32_t* cnt;
 };
 
+// Counting bound in the order the reference's tiled reporter visits the
+// prefilter candidates of a root (src/tiled_q3report.cpp:365-410, with lists
+// fed in EntryId order, src/full_ter.cpp:1785-1810): a triple (a, b, c) whose
+// low-p-bit keys are k_a, k_b is visited at (m, i, id_a, id_b, -id_c) with
+// i = k_a >> tb, m = i + (k_b >> tb); the C entries of one window slot are
+// visited by descending EntryId.  With `on` set, a projected sweep counts only
+// the triples visited before (m, i, a, b, c).
+struct VisitBound {
+  uint32_t on;
+  uint32_t pbits;   // p, the prefilter width (<= 32)
+  uint32_t tb;      // tile bits
+  uint32_t m, i, a, b, c;
+};
+
 struct SweepArgs {
   ListView q, x, y;
   const uint8_t* cells;     // 4096 bytes over the low 6 key bits, or null
@@ -56,6 +70,7 @@ struct SweepArgs {
   uint32_t rb;              // full residual width (carry into the high byte)
   uint32_t hi_bits;         // key bits above 64 (0 when Q <= 64)
   uint32_t project;         // 1: count triples on mrb residual bits only
+  VisitBound visit;         // projected counts: only triples visited before this bound
   uint32_t* triples;        // 3 * cap
   unsigned long long cap;
   unsigned long long* counters;  // [0] triples [1] survivors [2] fast [3] projected [4] fallback
@@ -125,7 +140,10 @@ struct RecordKeyArgs {
 void launch_record_keys(const RecordKeyArgs& a, cudaStream_t st);
 
 // Authority chain for the emitted triples: residue sum == T, FiniteSanity
-// structural count, root rule (binary parent of weight n/2).
+// structural count, root rule (binary parent of weight n/2).  Flags per triple:
+// bit0 residue-exact; of those, bit1 FiniteSanity structural (the RootSink count),
+// bit2 valid root, bit3 add_three structural reject (invalid digits), bit4
+// add_three distribution reject (digit counts other than the root's).
 struct AuthorityArgs {
   const uint8_t* records[3];
   uint32_t record_bytes, res_offset, words32, words64, n;

@@ -285,6 +285,7 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
   }
   if (j.projected_bits != 0) {
     a.project = 1;
+    a.visit = j.visit;
     a.mrb = j.projected_bits - tu.fb;
     sweep(a);
     *launches += 1;
@@ -450,6 +451,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   jw.cap = in.count_only ? 0 : in.capacity;
   jw.main_sweep = !in.count_only || in.projected_bits == 0;
   jw.projected_bits = in.projected_bits;
+  jw.visit = in.visit;
   r.tuning.variant = enqueue_join(jb, jw, tu, w.mid, st, &r.launches);
   check(cudaGetLastError(), "sweep launch");
   check(cudaEventRecord(w.stop, st), "event");

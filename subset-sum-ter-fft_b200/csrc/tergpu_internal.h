@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "count.cuh"
+#include "root_kernels.cuh"
 #include "tergpu.h"
 
 #include <cstdint>
@@ -100,6 +101,7 @@ struct JoinInput {
   bool autotune = false;   // pick fb / filter bits / variant by timing a sample first
   uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
   cudaStream_t stream;
+  VisitBound visit{};      // projected counts only before this bound (root_kernels.cuh)
 };
 
 struct JoinResult {
@@ -149,6 +151,7 @@ struct JoinWork {
   uint64_t cap;          // triples written (0: count only)
   bool main_sweep;       // the full-width sweep (false: projected counts only)
   uint32_t projected_bits;
+  VisitBound visit{};
 };
 
 // The join's device work on `st` -- partition, family layout, sweep(s) -- with

@@ -37,11 +37,19 @@ STATUS_NAMES = {
 
 ROOT_COUNT_ONLY = 1
 ROOT_DEVICE_INPUTS = 2
-ABI_VERSION = 2  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
+ABI_VERSION = 3  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
 ROOT_SWEEP_V1 = 4
 ROOT_SWEEP_V2 = 8
 ROOT_AUTOTUNE = 16
 MAX_QUOTIENT_BITS = 72
+# tergpu_attempt_in.root_policy: the numerics of ter::RootOutputPolicy
+ROOT_POLICY_FIRST_WITNESS = 0
+ROOT_POLICY_COUNT_ONLY = 1
+ROOT_POLICY_FULL_CANONICAL = 2
+ATTEMPT_CAPTURE_ONLY = 1
+ATTEMPT_PREFLIGHT = 2
+ATTEMPT_NO_GRAPH = 4
+ATTEMPT_TELEMETRY = 8
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _u32p = ctypes.POINTER(ctypes.c_uint32)

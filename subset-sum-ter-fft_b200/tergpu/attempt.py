@@ -26,6 +26,17 @@ class AttemptStats(ctypes.Structure):
         ("valid_roots", ctypes.c_uint64), ("root_pairs", ctypes.c_uint64),
         ("l2_ms", ctypes.c_double), ("l1_ms", ctypes.c_double), ("root_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("attempt_seed", ctypes.c_uint64),
+        ("l3_pairs", ctypes.c_uint64), ("l3_structural_rejects", ctypes.c_uint64),
+        ("l3_distribution_rejects", ctypes.c_uint64), ("l3_survivors", ctypes.c_uint64),
+        ("l2_pairs", ctypes.c_uint64), ("l2_structural_rejects", ctypes.c_uint64),
+        ("l2_distribution_rejects", ctypes.c_uint64), ("l2_survivors", ctypes.c_uint64),
+        ("root_structural_rejects", ctypes.c_uint64), ("root_distribution_rejects", ctypes.c_uint64),
+        ("root_low_prefilter", ctypes.c_uint64), ("root_full_quotient_rejects", ctypes.c_uint64),
+        ("root_quotient_bits", ctypes.c_uint32), ("root_prefilter_bits", ctypes.c_uint32),
+        ("root_policy", ctypes.c_uint32), ("root_early_stopped", ctypes.c_uint32),
+        ("l2_fingerprint", ctypes.c_uint64), ("l1_fingerprint", ctypes.c_uint64),
+        ("l0_fingerprint", ctypes.c_uint64), ("verification_ms", ctypes.c_double),
     ]
 
 
@@ -36,6 +47,7 @@ class AttemptIn(ctypes.Structure):
         ("seed", ctypes.c_uint64), ("attempt_first", ctypes.c_uint32),
         ("attempt_count", ctypes.c_uint32), ("memory_limit_bytes", ctypes.c_uint64),
         ("cancel", ctypes.POINTER(ctypes.c_int32)), ("device", ctypes.c_int32),
+        ("root_policy", ctypes.c_uint32),
     ]
 
 
@@ -48,6 +60,7 @@ class AttemptOut(ctypes.Structure):
         ("l1_capacity", ctypes.c_uint64 * 3), ("child_targets", (ctypes.c_uint32 * 4) * 3),
         ("root_target", ctypes.c_uint32 * 4), ("device_bytes", ctypes.c_uint64),
         ("total_ms", ctypes.c_double), ("device_bytes_held", ctypes.c_uint64),
+        ("fingerprint", ctypes.c_uint64), ("level3_ms", ctypes.c_double),
     ]
 
 
@@ -62,6 +75,9 @@ class FullTerConfig:
     export_l1_capacity: int = 0   # > 0: return the last attempt's L1 lists as a Snapshot
     capture_only: bool = False    # stop after L1 (the device stream_full_ter_root_lists)
     no_graph: bool = False        # n = 36 / 72: run stage by stage instead of one graph per attempt
+    # RootOutputPolicy (include/ter/full_ter.hpp:79-83); FirstWitness is the reference's default
+    root_policy: int = _abi.ROOT_POLICY_FIRST_WITNESS
+    telemetry: bool = False       # the reference's full telemetry: prefilter counts, fingerprints
 
 
 @dataclass
@@ -77,28 +93,42 @@ class FullTerResult:
     total_ms: float = 0.0
     device_bytes: int = 0        # the preflight's predicted bytes
     device_bytes_held: int = 0   # bytes the workspace held at the end of the call
+    fingerprint: int = 0         # FullTerTelemetry::fingerprint (telemetry runs)
+    level3_ms: float = 0.0
 
     @property
     def status_name(self) -> str:
         return _abi.STATUS_NAMES.get(self.status, str(self.status))
 
 
+_STAT_INTS = ("attempt_seed", "l3_pairs", "l3_structural_rejects", "l3_distribution_rejects",
+              "l3_survivors", "l2_pairs", "l2_structural_rejects", "l2_distribution_rejects",
+              "l2_survivors", "root_structural_rejects", "root_distribution_rejects",
+              "root_low_prefilter", "root_full_quotient_rejects", "root_quotient_bits",
+              "root_prefilter_bits", "root_policy", "root_early_stopped", "l2_fingerprint",
+              "l1_fingerprint", "l0_fingerprint")
+
+
 def _stats_dict(s: AttemptStats) -> dict:
-    return {
+    d = {
         "attempt": int(s.attempt), "status": int(s.status),
         "level2": [int(v) for v in s.level2_sizes], "level1": [int(v) for v in s.level1_sizes],
         "level0": int(s.level0_size), "l3_modular": int(s.l3_modular),
         "l2_modular": int(s.l2_modular), "root_modular": int(s.root_modular),
         "valid_roots": int(s.valid_roots), "root_pairs": int(s.root_pairs),
         "l2_ms": float(s.l2_ms), "l1_ms": float(s.l1_ms), "root_ms": float(s.root_ms),
-        "total_ms": float(s.total_ms),
+        "total_ms": float(s.total_ms), "verification_ms": float(s.verification_ms),
     }
+    for name in _STAT_INTS:
+        d[name] = int(getattr(s, name))
+    return d
 
 
 def _result(st: int, out: AttemptOut, stats, n: int) -> FullTerResult:
     res = FullTerResult(status=st, r1=int(out.r1), r2=int(out.r2), level3_size=int(out.level3_size),
                         total_ms=float(out.total_ms), device_bytes=int(out.device_bytes),
                         device_bytes_held=int(out.device_bytes_held),
+                        fingerprint=int(out.fingerprint), level3_ms=float(out.level3_ms),
                         attempts=[_stats_dict(stats[i]) for i in range(int(out.attempts_run))])
     if st == _abi.FOUND:
         res.witness = np.array(out.witness[:n], dtype=np.uint8)
@@ -112,7 +142,9 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     target = np.ascontiguousarray(instance.target_le, dtype=np.uint64)
     ain = AttemptIn()
     ain.n = instance.n
-    ain.flags = (1 if config.capture_only else 0) | (4 if config.no_graph else 0)
+    ain.flags = ((_abi.ATTEMPT_CAPTURE_ONLY if config.capture_only else 0)
+                 | (_abi.ATTEMPT_NO_GRAPH if config.no_graph else 0)
+                 | (_abi.ATTEMPT_TELEMETRY if config.telemetry else 0))
     ain.values_le = values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.target_le = target.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.seed = config.seed & (2**64 - 1)
@@ -121,6 +153,7 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     ain.memory_limit_bytes = config.memory_limit_bytes
     ain.cancel = ctypes.pointer(cancel) if cancel is not None else None
     ain.device = config.device
+    ain.root_policy = config.root_policy
     stats = (AttemptStats * max(1, config.attempt_limit))()
     out = AttemptOut()
     out.stats = ctypes.cast(stats, ctypes.POINTER(AttemptStats))

@@ -23,6 +23,37 @@ def test_library_exports_every_declared_symbol():
     assert lib.tergpu_abi_version() == int(version)
 
 
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """Every ctypes mirror has the C struct's size and field offsets (a C probe
+    compiled against include/tergpu.h prints them)."""
+    import subprocess
+
+    from tergpu import _abi, attempt, batch
+
+    mirrors = {"tergpu_root_in": _abi.RootIn, "tergpu_root_out": _abi.RootOut,
+               "tergpu_root_records_in": _abi.RootRecordsIn,
+               "tergpu_root_records_out": _abi.RootRecordsOut,
+               "tergpu_attempt_stats": attempt.AttemptStats, "tergpu_attempt_in": attempt.AttemptIn,
+               "tergpu_attempt_out": attempt.AttemptOut, "tergpu_batch_in": batch.BatchIn,
+               "tergpu_batch_out": batch.BatchOut}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "tergpu.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    for line in out.splitlines():
+        cname, field, value = line.split()
+        py = mirrors[cname]
+        got = ctypes.sizeof(py) if field == "size" else getattr(py, field).offset
+        assert got == int(value), (cname, field, got, value)
+
+
 def test_fnv1a_known_answers():
     from tergpu import snapshot
 

@@ -59,6 +59,7 @@ def test_preflight_refusals():
     (["--mode=success-curve", "--repeat=3"], 1, "--repeat does not apply"),
     (["--attempt-limit=0"], 1, "invalid --attempt-limit value"),
     (["--fixture"], 2, "does not implement"),
+    (["--guided"], 2, "does not implement"),
     (["--family=paper-rounded"], 2, "does not implement"),
     (["--nonsense"], 1, "usage"),
 ])
@@ -81,6 +82,45 @@ def test_attempt_cost_row_matches_reference(golden):
     assert row["L1_sizes"] == ":".join(map(str, last["level1"]))
     assert row["attempts_used"] == "3" and row["terminal_attempt_index"] == "2"
     assert int(row["root_modular"]) == last["root_modular"]
+
+
+# ter_full_bench columns whose values the device row must reproduce exactly; the
+# others are timings, the CPU memory model and the tiled reporter's internals.
+SHARED_COLUMNS = (
+    "status", "n", "r1", "r2", "L3_left", "L3_right", "L2_sizes", "L1_sizes", "L0",
+    "binary_pairs", "binary_modular", "binary_structural_rejects", "binary_distribution_rejects",
+    "binary_survivors", "binary_deduplicated", "middle_pairs", "middle_modular",
+    "middle_structural_rejects", "middle_distribution_rejects", "middle_survivors",
+    "middle_deduplicated", "root_pairs", "root_modular", "root_structural_rejects",
+    "root_distribution_rejects", "root_survivors", "root_deduplicated", "fingerprint",
+    "l2_to_l1_pair_records", "l1_to_l0_pair_records", "l1_to_l0_quotient_bits",
+    "l1_to_l0_prefilter_bits", "l1_to_l0_low_prefilter_candidates",
+    "l1_to_l0_full_quotient_rejects", "l1_to_l0_root_policy", "l1_to_l0_valid_roots",
+    "l1_to_l0_early_stopped", "attempts_used", "terminal_attempt_index", "terminal_attempt_seed",
+    "terminal_attempt_status", "total_root_pair_candidates",
+)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(5))
+def test_row_matches_reference_ter_full_bench(golden, case):
+    """The device row against the reference's own ter_full_bench row (built from
+    bench/ter_full_bench.cpp): the same header, and every count column plus the
+    telemetry fingerprint equal.  The n=72 0x7201 run is Found at attempt 21
+    under FirstWitness, so its root counters stop at the reference's first
+    witness in its tiled visit order."""
+    g = golden["full_bench_rows"][case]
+    ref = csv_rows(g["header"] + "\n" + g["row"])[0]
+    p = run(*g["args"], "--memory-limit-mib=65536", timeout=1200)
+    assert p.returncode == 0, p.stderr
+    lines = [l for l in p.stdout.splitlines() if l and not l.startswith("#")]
+    assert lines[0] == g["header"]
+    row = csv_rows(p.stdout)[0]
+    for col in SHARED_COLUMNS:
+        assert row[col] == ref[col], (g["args"], col, row[col], ref[col])
+    for col, v in row.items():
+        assert v == "" or v.lstrip("-").replace(".", "").isdigit() or col.endswith("status") \
+            or col.endswith("_sizes"), (col, v)
 
 
 @pytest.mark.gpu

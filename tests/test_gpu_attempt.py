@@ -24,9 +24,10 @@ def _attempt(n, seed, first, count, kind="auth", **kw):
 def test_n36_attempts_match_reference(golden, case):
     from tergpu import _abi, instance
 
-    g = golden["n36_attempts"][case]
+    g = golden["n36_attempts"][case]  # solve_full_ter with FullCanonicalOutput
     for row in g["attempts"]:
-        inst, res = _attempt(36, g["seed"], row["attempt"], 1, kind=g["kind"])
+        inst, res = _attempt(36, g["seed"], row["attempt"], 1, kind=g["kind"],
+                             root_policy=_abi.ROOT_POLICY_FULL_CANONICAL)
         assert (res.r1, res.r2) == (g["final"]["r1"], g["final"]["r2"])
         a = res.attempts[0]
         for key in ("level2", "level1", "level0", "l3_modular", "l2_modular"):
@@ -37,6 +38,58 @@ def test_n36_attempts_match_reference(golden, case):
             assert res.status == _abi.FOUND and instance.verify_witness(inst, res.witness)
         else:
             assert res.status == _abi.ATTEMPT_LIMIT_REACHED
+
+
+STAGES = {
+    # reference FullTerStageTelemetry field -> device stats field, per stage
+    "binary": {"pairs": "l3_pairs", "modular": "l3_modular", "structural": "l3_structural_rejects",
+               "distribution": "l3_distribution_rejects", "survivors": "l3_survivors",
+               "fingerprint": "l2_fingerprint"},
+    "middle": {"pairs": "l2_pairs", "modular": "l2_modular", "structural": "l2_structural_rejects",
+               "distribution": "l2_distribution_rejects", "survivors": "l2_survivors",
+               "fingerprint": "l1_fingerprint"},
+    "root": {"pairs": "root_pairs", "modular": "root_modular",
+             "structural": "root_structural_rejects", "distribution": "root_distribution_rejects",
+             "survivors": "valid_roots", "deduplicated": "level0", "quotient_bits": "root_quotient_bits",
+             "prefilter_bits": "root_prefilter_bits", "low_prefilter": "root_low_prefilter",
+             "full_quotient_rejects": "root_full_quotient_rejects", "valid_roots": "valid_roots",
+             "policy": "root_policy", "early_stopped": "root_early_stopped",
+             "fingerprint": "l0_fingerprint"},
+}
+
+
+@pytest.mark.parametrize("case", range(16))
+def test_attempt_telemetry_matches_reference(golden, case):
+    """Every stage counter, every stage output fingerprint and the run fingerprint
+    of solve_full_ter, under FirstWitness and FullCanonicalOutput, on both
+    instance generators at n=36 and on the n=72 authentic roots (0x7201 is Found
+    at attempt 21: FirstWitness stops its root counters at the reference's first
+    witness in the tiled visit order)."""
+    from tergpu import _abi
+
+    g = golden["attempt_telemetry"][case]
+    policy = (_abi.ROOT_POLICY_FIRST_WITNESS if g["policy"] == "first"
+              else _abi.ROOT_POLICY_FULL_CANONICAL)
+    _, res = _attempt(g["n"], g["seed"], 0, g["attempts"], kind=g["kind"], root_policy=policy,
+                      telemetry=True, memory_limit_bytes=64 << 30)
+    final = g["final"]
+    assert res.status == final["status"]
+    assert res.fingerprint == hexint(final["fingerprint"]), (g["n"], g["kind"], g["seed"], g["policy"])
+    assert len(res.attempts) == len(g["rows"])
+    if res.status == _abi.FOUND:
+        assert "".join(str(int(d)) for d in res.witness) == final["witness"]
+    for a, row in zip(res.attempts, g["rows"]):
+        assert a["attempt_seed"] == row["seed"] and a["status"] == row["status"]
+        assert a["level2"] == row["level2"] and a["level1"] == row["level1"]
+        assert a["level0"] == row["level0"]
+        for stage, fields in STAGES.items():
+            for ref_key, dev_key in fields.items():
+                want = row[stage][ref_key]
+                want = hexint(want) if ref_key == "fingerprint" else want
+                assert a[dev_key] == want, (g["kind"], g["seed"], g["policy"], row["attempt"], stage,
+                                            ref_key, a[dev_key], want)
+        assert sum(a["level2"]) == row["binary"]["deduplicated"]
+        assert sum(a["level1"]) == row["middle"]["deduplicated"]
 
 
 def test_n36_attempt_loop_stops_like_the_reference(golden):
