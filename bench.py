@@ -14,9 +14,10 @@ resolution).  Inputs (226 MB) exceed L2 (126 MB), so no flush is needed.
            launching stream, max over ranks).
   e2e    : the same pairs/s through the public C ABI with pinned HOST key
            buffers: upload, partition, sweep, result download per step.
-  --impl reference : the reference's frozen ARWLF (built from its sources into
-           oracle/_ref) on the box's host cores, one process per core over
-           disjoint cells of the same root.
+  --impl reference : the reference's own CPU path on the box's host cores: its
+           capture of the same root (stream_full_ter_root_lists, untimed), then
+           its frozen ARWLF over successive windows of its shuffled cell order,
+           one pinned process per host core (no part of this library runs).
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own independent
 root (seed + rank) -- weak scaling, no data-path collective.  --shard-root
@@ -48,8 +49,12 @@ UNIT = "pairs/s"
 SIZES = (3_650_689, 6_900_048, 6_896_564)
 QBITS = 69
 PLANTED = 8
-# per logical pair the sweep issues at least: IADD, LOP (word offset), LDS, 2x SHF.funnel
-OPS_PER_PAIR = 5
+# The sweep's roofline: 2 INT32 ops per logical pair (one add forming the sum, one
+# test), the algorithmic minimum, against 148 SMs x 128 INT32 lanes x the SM clock.
+OPS_PER_PAIR = 2
+INT32_LANES = 148 * 128
+# secondary view: the instructions per pair of the kernel's probe design
+DESIGN_OPS_PER_PAIR = 5
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one default-variant sweep
 # launch on the default workload (the whole authentic n=108 root of seed 0x1001), from one
 # ncu capture of that launch; other workloads and variants report null
@@ -72,8 +77,8 @@ def parse():
     p.add_argument("--filter-bits", type=int, default=0)
     p.add_argument("--sweep-v1", action="store_true", help="sweep variant 1 (A/B runs)")
     p.add_argument("--sweep-v2", action="store_true", help="sweep variant 2 (A/B runs)")
-    p.add_argument("--cpu-cells", type=int, default=6,
-                   help="cells of the reference's declared subsample timed on one core")
+    p.add_argument("--cpu-cells", type=int, default=1,
+                   help="cells per timed pass of the reference's CPU legs (per process)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--batch", action="store_true",
@@ -124,7 +129,8 @@ def authentic_root(seed: int):
     q, lo, hi, _ = snapshot.root_keys(res.snapshot)
     keys = tergpu.RootKeys(quotient_bits=q, lo=lo, hi=hi)
     return keys, {"capture_ms": capture_ms, "level2": res.attempts[0]["level2"],
-                  "level1": res.attempts[0]["level1"], "setup_s": time.perf_counter() - t0}
+                  "level1": res.attempts[0]["level1"], "setup_s": time.perf_counter() - t0}, \
+        res.snapshot
 
 
 class ClockSampler:
@@ -201,14 +207,14 @@ def run_tergpu(args):
     my_shards = shards_of_rank(rank, world) if sharded else [0]
     shard_count = shard_count_for(world) if sharded else 1
     root_seed = args.seed if sharded else args.seed + rank
-    capture = None
+    capture = snap_obj = None
     if args.synthetic:
         sizes = sizes_for(args)
         keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=root_seed,
                                        planted=PLANTED)
         planted = {(sizes[0] - 1 - i, sizes[1] - 1 - i, sizes[2] - 1 - i) for i in range(PLANTED)}
     else:
-        keys, capture = authentic_root(root_seed)
+        keys, capture, snap_obj = authentic_root(root_seed)
         sizes = tuple(len(a) for a in keys.lo)
         planted = set()
     lib = _abi.load()
@@ -357,7 +363,9 @@ def run_tergpu(args):
         sweep_bytes = sum(sizes) * 8
         sweep_kernel = "k_sweep" if args.sweep_v1 else ("k_sweep2" if args.sweep_v2 else "k_sweep3")
         part_bytes = sum(sizes) * (2 * 9 + 8 + 13 + 4)  # hist read, scatter read + write
-        issue_peak = 148 * 4 * 32 * sm_mhz * 1e6 / OPS_PER_PAIR
+        int32_peak = INT32_LANES * sm_mhz * 1e6  # INT32 ops/s
+        sweep_pairs_s = local_pairs / (sweep_ms / 1000.0)
+        design_peak = INT32_LANES * sm_mhz * 1e6 / DESIGN_OPS_PER_PAIR
         result = {
             "metric": METRIC, "value": pairs / (ms / 1000.0), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
@@ -378,18 +386,26 @@ def run_tergpu(args):
                        "filter_survivors": survivors, "full_q_triples": triples,
                        "parallelism": (f"shards{shard_count}-over-{world}" if sharded
                                        else f"replicas{world}")},
-            "roofline": {"bound": "hbm", "kernel": sweep_kernel,
-                         "achieved": sweep_bytes / (sweep_ms / 1000.0) / 1e9, "peak": hbm,
-                         "unit": "GB/s", "frac": sweep_bytes / (sweep_ms / 1000.0) / 1e9 / hbm,
-                         "peak_source": peak_src,
+            # the sweep is neither HBM- nor tensor-bound: its roofline is INT32 issue
+            # at the algorithmic 2 ops per logical pair
+            "roofline": {"bound": "int32", "kernel": sweep_kernel,
+                         "achieved": sweep_pairs_s * OPS_PER_PAIR / 1e9, "peak": int32_peak / 1e9,
+                         "unit": "Gop/s", "frac": sweep_pairs_s * OPS_PER_PAIR / int32_peak,
+                         "ops_per_pair": OPS_PER_PAIR,
+                         "peak_source": f"148 SMs x 128 INT32 lanes x {sm_mhz:.0f} MHz (the SM clock "
+                                        "sampled during the timed region)",
                          "traffic": (SWEEP_DRAM_BYTES.get(sweep_kernel)
                                      if not args.synthetic and args.seed == 0x1001 else None),
-                         "note": "the sweep is bound on chip (issue, shared-memory probes), not by "
-                                 "HBM: see issue_roofline"},
+                         "algorithmic_bytes": sweep_bytes},
+            "hbm_roofline": {"bound": "hbm", "kernel": sweep_kernel,
+                             "achieved": sweep_bytes / (sweep_ms / 1000.0) / 1e9, "peak": hbm,
+                             "unit": "GB/s", "frac": sweep_bytes / (sweep_ms / 1000.0) / 1e9 / hbm,
+                             "peak_source": peak_src},
             "issue_roofline": {"bound": "int32-issue", "kernel": sweep_kernel, "unit": "pairs/s",
-                               "achieved": local_pairs / (sweep_ms / 1000.0), "peak": issue_peak,
-                               "frac": local_pairs / (sweep_ms / 1000.0) / issue_peak,
-                               "ops_per_pair": OPS_PER_PAIR, "sm_mhz": sm_mhz},
+                               "achieved": sweep_pairs_s, "peak": design_peak,
+                               "frac": sweep_pairs_s / design_peak,
+                               "ops_per_pair": DESIGN_OPS_PER_PAIR, "sm_mhz": sm_mhz,
+                               "note": "secondary: the probe design's instructions per pair"},
             "partition_roofline": {"bound": "hbm", "unit": "GB/s",
                                    "achieved": part_bytes / (part_ms / 1000.0) / 1e9, "peak": hbm,
                                    "frac": part_bytes / (part_ms / 1000.0) / 1e9 / hbm,
@@ -401,7 +417,12 @@ def run_tergpu(args):
             result["e2e"] = e2e
     # the reference's CPU path on this host, rank 0 at N=1 only
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(keys, args)
+        if snap_obj is None:
+            result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                                      "sample": "the reference's root path runs on captured "
+                                                "authentic roots only (not --synthetic)"}
+        else:
+            result["cpu_baseline"] = cpu_baseline(snap_obj, args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -409,54 +430,99 @@ def run_tergpu(args):
         print(json.dumps(result), flush=True)
 
 
-def write_keys(keys, path: Path):
-    with open(path, "wb") as f:
-        f.write(b"TERKEYS1")
-        f.write(np.array([keys.quotient_bits, 0], dtype=np.uint32).tobytes())
-        f.write(np.array([len(a) for a in keys.lo], dtype=np.uint64).tobytes())
-        for l in range(3):
-            f.write(np.ascontiguousarray(keys.lo[l], dtype=np.uint64).tobytes())
-            f.write(np.ascontiguousarray(keys.hi[l], dtype=np.uint8).tobytes())
-            f.write(b"\0" * ((8 - len(keys.lo[l]) % 8) % 8))
-
-
 def ref_binary():
-    return ROOT / "oracle" / "_ref" / "terref"
+    """The reference harness for timing: the -march=native build when this host's
+    CPU has every flag of the CPU that built it, else the portable build."""
+    plain = ROOT / "oracle" / "_ref" / "terref"
+    native = ROOT / "oracle" / "_ref" / "terref_native"
+    flags = ROOT / "oracle" / "_ref" / "native_flags.txt"
+    if native.exists() and flags.exists():
+        need = set(flags.read_text().split())
+        have = set()
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                have = set(line.split(":", 1)[1].split())
+                break
+        if need <= have:
+            return native, "g++ -O2 -march=native"
+    return plain, "g++ -O2 -march=x86-64-v3 (this host lacks a flag of the native build's CPU)"
 
 
-def cpu_baseline(keys, args):
-    """The reference's frozen ARWLF on one host core over its declared cell subsample."""
-    binary = ref_binary()
+def cpu_model() -> str:
+    for line in Path("/proc/cpuinfo").read_text().splitlines():
+        if line.startswith("model name"):
+            return line.split(":", 1)[1].strip()
+    return "unknown"
+
+
+def snaptime(binary, snap, backend, cells, reps, first, stride, core=None, timeout=3600):
+    """The reference's own root path on one core: load_snapshot_workload of SNAP
+    (untimed), then `reps` timed passes of `backend` over successive windows of
+    its shuffled cell order (oracle/ref_harness.cpp, snaptime)."""
+    cmd = [str(binary), "snaptime", str(snap), backend, "0", str(cells), str(reps), str(first),
+           str(stride)]
+    if core is not None:
+        cmd = ["taskset", "-c", str(core)] + cmd
+    return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+
+
+def rows_of(proc, timeout=3600):
+    out, err = proc.communicate(timeout=timeout)
+    rows = [json.loads(x) for x in out.splitlines() if x.startswith("{")]
+    if proc.returncode != 0 or not rows or "error" in rows[0]:
+        raise RuntimeError(f"reference harness failed: {err[-300:]} {out[-300:]}")
+    return rows
+
+
+def target_families(cells) -> int:
+    """Distinct target families u = (s + t) mod 64 of cells s * 64 + t."""
+    return len({((c >> 6) + (c & 63)) & 63 for c in cells})
+
+
+def cpu_baseline(snapshot_obj, args):
+    """The reference's frozen ARWLF on one pinned host core over the same root,
+    read through the reference's own load_snapshot_workload: 3 warm-up and 7 timed
+    passes over successive cells of its shuffled cell order, the median (the
+    protocol of TER_L1_to_L0_ARWLF_Architecture_v1.0.md:138-142), and K2_WIDE
+    timed beside it on one cell."""
+    from tergpu import snapshot
+
+    binary, build = ref_binary()
     if not binary.exists():
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/terref was not built"}
+    cells = max(1, args.cpu_cells)
     with tempfile.TemporaryDirectory() as d:
-        path = Path(d) / "root.keys"
-        write_keys(keys, path)
-        proc = subprocess.run(["taskset", "-c", "0", str(binary), "keysroot", str(path), "arwlf",
-                               str(args.cpu_cells), "2", "0"], capture_output=True, text=True,
-                              timeout=900)
-    rows = [json.loads(x) for x in proc.stdout.splitlines() if x.startswith("{")]
-    if proc.returncode != 0 or not rows:
-        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"failed: {proc.stderr[-200:]}"}
-    row = min(rows, key=lambda r: r["ms"])
-    return {"value": row["pairs"] / (row["ms"] / 1000.0), "unit": UNIT, "cores": 1,
-            "kind": "reference", "host_cores": os.cpu_count(),
-            "sample": (f"frozen ARWLF (reference sources, g++ -O2 -march=x86-64-v3) on the "
-                       f"reference's declared subsample of {args.cpu_cells} of 4096 cells of the "
-                       f"same root ({row['pairs']} logical pairs), best of 2, 1 pinned core"),
-            "ms": row["ms"], "pairs": row["pairs"],
-            "digest_triples": row["triples"]}
+        path = Path(d) / "root.snap"
+        snapshot.save(snapshot_obj, path, git_commit="reference")
+        arwlf = rows_of(snaptime(binary, path, "arwlf", cells, 10, 0, cells, core=0))
+        wide = rows_of(snaptime(binary, path, "k2wide", cells, 1, 10 * cells, cells, core=0))
+    timed = arwlf[3:]
+    rates = [r["pairs"] / (r["ms"] / 1000.0) for r in timed]
+    v = statistics.median(rates)
+    k2w = wide[0]
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "host_cores": os.cpu_count(),
+            "cpu": cpu_model(), "build": build,
+            "sample": (f"frozen ARWLF (reference sources, {build}) on 1 pinned core over the same "
+                       f"root loaded by the reference's load_snapshot_workload: 3 warm-up + 7 timed "
+                       f"passes of {cells} cell(s) each, successive windows of its shuffled cell "
+                       f"order ({sum(r['pairs'] for r in timed)} timed pairs), median"),
+            "pass_ms": [r["ms"] for r in timed], "pass_pairs": [r["pairs"] for r in timed],
+            "k2_wide": {"value": k2w["pairs"] / (k2w["ms"] / 1000.0), "unit": UNIT, "cores": 1,
+                        "pairs": k2w["pairs"], "ms": k2w["ms"],
+                        "sample": f"frozen K2_WIDE, one pass over {cells} cell(s)"}}
 
 
 def run_reference(args):
+    """The reference's own CPU path only: its capture of the root, its workload
+    loader and its frozen ARWLF (oracle/_ref/terref, compiled from its sources);
+    nothing of this library is imported or run here."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     sizes = sizes_for(args)
-    binary = ref_binary()
+    binary, build = ref_binary()
     base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "config": {"workload": workload_name(sizes, args.synthetic, args.seed), "seed": args.seed,
@@ -465,43 +531,50 @@ def run_reference(args):
         base["unavailable"] = "reference harness oracle/_ref/terref was not built on this host"
         print(json.dumps(base), flush=True)
         return
-    from tergpu import workload
-
     if args.synthetic:
-        keys = workload.synthetic_root(sizes=sizes, quotient_bits=QBITS, seed=args.seed,
-                                       planted=PLANTED)
-    else:
-        # the authentic root's L1 lists come from the device attempt pipeline
-        # (bit-identical to the reference's capture); only ARWLF is timed
-        keys, _ = authentic_root(args.seed)
-        sizes = tuple(len(a) for a in keys.lo)
-        base["config"]["workload"] = workload_name(sizes, False, args.seed)
+        base["unavailable"] = "the reference's root path runs on captured authentic roots only"
+        print(json.dumps(base), flush=True)
+        return
     procs_n = max(1, min(os.cpu_count() or 1, 64))
-    cells_per = max(1, args.cpu_cells)
+    cells = max(1, args.cpu_cells)
     reps = max(1, args.steps + args.warmup)
     with tempfile.TemporaryDirectory() as d:
-        path = Path(d) / "root.keys"
-        write_keys(keys, path)
-        procs = []
-        for i in range(procs_n):
-            procs.append(subprocess.Popen(
-                ["taskset", "-c", str(i % (os.cpu_count() or 1)), str(binary), "keysroot", str(path),
-                 "arwlf", f"mod:{procs_n}:{i}:{cells_per}", str(reps), "0"],
-                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
-        outs = [p.communicate(timeout=3600) for p in procs]
-    per_rep = [[json.loads(x) for x in o.splitlines() if x.startswith("{")] for o, _ in outs]
-    values = []
+        snap = Path(d) / "root.snap"
+        t0 = time.perf_counter()
+        cap = subprocess.run([str(binary), "capture", "108", str(args.seed), "0", "auth", str(snap)],
+                             capture_output=True, text=True, timeout=3600)
+        capture_s = time.perf_counter() - t0
+        caps = [json.loads(x) for x in cap.stdout.splitlines() if x.startswith("{")]
+        if cap.returncode != 0 or not caps:
+            base["unavailable"] = f"the reference's capture failed: {cap.stderr[-200:]}"
+            print(json.dumps(base), flush=True)
+            return
+        sizes = tuple(caps[0]["level1"])
+        base["config"]["workload"] = workload_name(sizes, False, args.seed)
+        # process i, pass r: cells [(r * P + i) * C, +C) of the shuffled order
+        procs = [snaptime(binary, snap, "arwlf", cells, reps, i * cells, procs_n * cells, core=i)
+                 for i in range(procs_n)]
+        per_proc = [rows_of(p) for p in procs]
+    values, timed_cells = [], []
     for rep in range(args.warmup, reps):
-        pairs = sum(rows[rep]["pairs"] for rows in per_rep)
-        ms = max(rows[rep]["ms"] for rows in per_rep)
+        pairs = sum(rows[rep]["pairs"] for rows in per_proc)
+        ms = max(rows[rep]["ms"] for rows in per_proc)
         values.append(pairs / (ms / 1000.0))
+        for rows in per_proc:
+            timed_cells += rows[rep]["cell_ids"]
     v = statistics.median(values)
-    pairs_step = sum(rows[-1]["pairs"] for rows in per_rep)
+    pairs_step = statistics.median(sum(rows[rep]["pairs"] for rows in per_proc)
+                                   for rep in range(args.warmup, reps))
+    sample = (f"the reference's capture of the root ({capture_s:.0f} s, untimed), then its frozen "
+              f"ARWLF ({build}) in {procs_n} pinned processes, each pass {cells} cell(s) per "
+              f"process from successive windows of its shuffled cell order; {len(set(timed_cells))} "
+              f"distinct timed cells over {target_families(timed_cells)} of 64 target families; "
+              f"per step: pairs of all processes / the slowest process; median over the timed steps")
+    base["config"]["sample"] = sample
     base.update({
         "value": v, "ms_per_step": pairs_step / v * 1000.0,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs_n, "kind": "reference",
-                         "sample": (f"frozen ARWLF, {procs_n} processes x {cells_per} disjoint "
-                                    f"cells of the same root per step ({pairs_step} pairs)")},
+                         "cpu": cpu_model(), "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(base), flush=True)

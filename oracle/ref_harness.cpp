@@ -14,6 +14,11 @@
 //   terref snaproot SNAP BACKEND CELLS PROJ
 //       load_snapshot_workload + build_family_keys + build_root_index, the cell
 //       selection CELLS (apply_cells), then one backend into an authority sink.
+//   terref snaptime SNAP BACKEND PROJ CELLS REPS FIRST STRIDE
+//       load_snapshot_workload once (untimed), then REPS timed passes of one
+//       backend; pass r runs the cells perm:((FIRST + r * STRIDE) mod 4096):CELLS
+//       (successive windows of the reference's shuffled cell order) into a fresh
+//       authority sink; one JSON row per pass.
 //   terref synth BITS SEED SIZE POOL OUT
 //       ter2_root/tests/ter_synthetic_root.hpp make_root; writes the three key
 //       lists to OUT and prints the brute-force oracle digest.
@@ -311,6 +316,59 @@ int cmd_snaproot(int argc, char** argv) {
   return 0;
 }
 
+int cmd_snaptime(int argc, char** argv) {
+  if (argc < 9) { return 2; }
+  const std::string path = argv[2];
+  const std::string backend = argv[3];
+  const auto proj = static_cast<std::uint32_t>(std::strtoul(argv[4], nullptr, 0));
+  const auto cells = static_cast<std::uint32_t>(std::strtoul(argv[5], nullptr, 0));
+  const int reps = std::max(1, std::atoi(argv[6]));
+  const auto first = static_cast<std::uint32_t>(std::strtoul(argv[7], nullptr, 0));
+  const auto stride = static_cast<std::uint32_t>(std::strtoul(argv[8], nullptr, 0));
+  const auto load_start = Clock::now();
+  const auto workload = rg::load_snapshot_workload(path, true);
+  if (workload->status != rg::WorkloadStatus::Completed) {
+    std::cout << "{\"error\":\"" << rg::status_label(workload->status) << ": "
+              << workload->status_detail << "\"}\n";
+    return 1;
+  }
+  const a64::FamilyKeys keys = a64::build_family_keys(*workload);
+  const mr8::Dataset& data = *workload->data;
+  rg::RootIndex index;
+  rg::build_root_index(data, index);
+  const double load_ms = std::chrono::duration<double, std::milli>(Clock::now() - load_start).count();
+  for (int rep = 0; rep < reps; ++rep) {
+    const std::uint32_t at = (first + static_cast<std::uint32_t>(rep) * stride) % 4096U;
+    const std::uint32_t take = std::min(cells, 4096U - at);
+    apply_cells(index, "perm:" + std::to_string(at) + ":" + std::to_string(take));
+    std::vector<std::array<ter::EntryId, 3>> witnesses;
+    rg::RootSink sink;
+    sink.data = &data;
+    sink.index = &index;
+    sink.authority = &workload->authority;
+    sink.witnesses = &witnesses;
+    sink.reset();
+    double ms = 0.0;
+    const std::string extra = run_backend(backend, data, index, keys, sink, proj, &ms);
+    std::uint64_t pairs = 0U;
+    for (std::uint32_t s = 0; s < 64U; ++s)
+      for (std::uint32_t t = 0; t < 64U; ++t)
+        if (index.active(s, t)) pairs += data.q_family[s].size() * data.x_family[t].size();
+    std::cout << "{\"backend\":\"" << backend << "\",\"rep\":" << rep << ",\"first_cell\":" << at
+              << ",\"cell_ids\":[";
+    bool any = false;
+    for (std::uint32_t c = 0; c < 4096U; ++c) {
+      if (index.selected[c] == 0U) continue;
+      std::cout << (any ? "," : "") << c;
+      any = true;
+    }
+    std::cout << "],\"cells\":" << index.selected_count << ",\"pairs\":" << pairs
+              << ",\"load_ms\":" << load_ms << ",\"ms\":" << ms << "," << digest_json(sink.digest)
+              << "," << extra << "}\n" << std::flush;
+  }
+  return 0;
+}
+
 bool write_keys(const std::string& path, const sr::Synthetic& root) {
   std::ofstream f(path, std::ios::binary);
   const char magic[8] = {'T', 'E', 'R', 'K', 'E', 'Y', 'S', '1'};
@@ -509,7 +567,7 @@ int cmd_report(int argc, char** argv) {
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::cerr << "usage: terref solve|capture|snaproot|synth|keysroot ...\n";
+    std::cerr << "usage: terref solve|capture|snaproot|snaptime|synth|keysroot|plant|report ...\n";
     return 2;
   }
   const std::string cmd = argv[1];
@@ -517,6 +575,7 @@ int main(int argc, char** argv) {
   if (cmd == "solve") { rc = cmd_solve(argc, argv); }
   else if (cmd == "capture") { rc = cmd_capture(argc, argv); }
   else if (cmd == "snaproot") { rc = cmd_snaproot(argc, argv); }
+  else if (cmd == "snaptime") { rc = cmd_snaptime(argc, argv); }
   else if (cmd == "synth") { rc = cmd_synth(argc, argv); }
   else if (cmd == "keysroot") { rc = cmd_keysroot(argc, argv); }
   else if (cmd == "report") { rc = cmd_report(argc, argv); }
