@@ -378,10 +378,12 @@ int tergpu_attempt_batch(const tergpu_batch_in *in, tergpu_batch_out *out);
  * offered here; family bits are limited to 6..10.
  *
  * The first call on a device looks up the array's device address (a lookup,
- * not an allocation); make that first call before any stream capture.  Every
- * call reuses the same array, so calls whose work overlaps on the GPU race:
- * issue them one after another.  join_ms / partition_ms / sweep_ms are not
- * measured (no events are created) and read 0.
+ * not an allocation).  Every call waits for its stream to finish (it reads the
+ * counters back), so a call on a stream under capture is refused with
+ * TERGPU_INVALID_INPUT.  The call leaves the caller's current device as it
+ * found it.  Every call reuses the same array, so calls whose work overlaps on
+ * the GPU race: issue them one after another.  join_ms / partition_ms /
+ * sweep_ms are not measured (no events are created) and read 0.
  */
 int tergpu_root_run_noalloc(const tergpu_root_in *in, tergpu_root_out *out);
 

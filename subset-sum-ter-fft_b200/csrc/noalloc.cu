@@ -16,7 +16,11 @@
 //
 // Set-up: the first call on a device looks up the device address of the array
 // (cudaGetSymbolAddress, with that device current) and remembers it; it is a
-// lookup, not an allocation.  Make that first call before any stream capture.
+// lookup, not an allocation.  Every call also waits for its stream to finish
+// the join (it reads the counters back), so a call on a stream that is being
+// captured is refused with TERGPU_INVALID_INPUT and the capture is left intact.
+// The call makes `device` current for its work and restores the caller's
+// current device before it returns.
 //
 // Every call uses the same array and leaves the last call's contents in it; the
 // call clears what must start at zero.  Two calls whose work overlaps on the
@@ -83,9 +87,25 @@ uint32_t ceil_log2_u64(uint64_t v) {
 
 extern "C" const char* tergpu_noalloc_last_error(void) { return tergpu::t_noalloc_error; }
 
+namespace tergpu {
+namespace {
+// Restores the calling thread's current device on every return path.
+struct DeviceGuard {
+  int saved = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+  }
+  ~DeviceGuard() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
+}  // namespace
+}  // namespace tergpu
+
 extern "C" int tergpu_root_run_noalloc(const tergpu_root_in* in, tergpu_root_out* out) {
   using namespace tergpu;
   t_noalloc_error[0] = '\0';
+  const DeviceGuard restore;
   const auto t0 = std::chrono::steady_clock::now();
   if (in == nullptr || out == nullptr) return fail(TERGPU_INVALID_INPUT, "null argument");
   if ((in->flags & TERGPU_ROOT_DEVICE_INPUTS) == 0) {
@@ -154,6 +174,13 @@ extern "C" int tergpu_root_run_noalloc(const tergpu_root_in* in, tergpu_root_out
 
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(in->stream);
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing(st, &capturing)) != cudaSuccess) return fail_cuda(e, "cudaStreamIsCapturing");
+  if (capturing != cudaStreamCaptureStatusNone) {
+    return fail(TERGPU_INVALID_INPUT,
+                "the no-allocation entry waits for its stream and cannot run on a capturing stream");
+  }
   {
     std::lock_guard<std::mutex> lock(g_scratch_mu);
     if (g_scratch_ptr[device] == nullptr) {
@@ -163,7 +190,6 @@ extern "C" int tergpu_root_run_noalloc(const tergpu_root_in* in, tergpu_root_out
       g_scratch_ptr[device] = p;
     }
   }
-  cudaStream_t st = static_cast<cudaStream_t>(in->stream);
   Carver carve{static_cast<unsigned char*>(g_scratch_ptr[device]), 0};
   ListView views[3];
   uint64_t* res[3];
@@ -245,7 +271,9 @@ extern "C" int tergpu_root_run_noalloc(const tergpu_root_in* in, tergpu_root_out
   out->sweep_ms = 0;
   out->family_bits = fb;
   out->filter_bits = wb + 5;
-  out->kernel_launches = 3 * 3 + 2 + (in->count[1] != 0 ? 1 : 0) + 1;
+  uint32_t launches = 2 + (in->count[1] != 0 ? 1 : 0) + 1;  // max-family x2, family sort, sweep
+  for (int l = 0; l < 3; ++l) launches += (in->count[l] != 0 ? 2 : 0) + 1;  // hist + scatter, scan
+  out->kernel_launches = launches;
   out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (!count_only && hc[kTriples] > out->capacity) return TERGPU_OUTPUT_OVERFLOW;
   return TERGPU_COMPLETED;

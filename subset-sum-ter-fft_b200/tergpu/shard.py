@@ -8,8 +8,10 @@ two <= 64) is the set of pairs with key_a + key_b == g (mod G), i.e. the D
 entries with key_d == g (mod G); the G shards are disjoint and their union is
 the whole root.
 
-Rank r of a world of W ranks takes the shards r, r + W, r + 2W, ... of
-G = the smallest power of two >= W, runs them through the backend (each rank
+Rank r of a world of W > 1 ranks takes the shards r, r + W, r + 2W, ... of
+G = 64 (the finest split the cell grid allows: a rank's share is at most
+ceil(64 / W) / (64 / W) of the mean, 1.10 for W <= 8, whatever W is), runs them
+through the backend (each rank
 reads all of A and B and the D families of its shards; there is no exchange
 inside the join), and the only collective is one gather of the triples (a count
 plus a few 12-byte records) and of the telemetry sums, so every rank ends with
@@ -27,13 +29,12 @@ MAX_SHARDS = 64
 
 
 def shard_count_for(world: int) -> int:
-    """Shards a world of `world` ranks splits one root into (a power of two)."""
+    """Shards a world of `world` ranks splits one root into: 1 for a single
+    rank, else all 64 (dealt round-robin, so non-power-of-two worlds stay
+    balanced)."""
     if world < 1 or world > MAX_SHARDS:
         raise ValueError(f"world size {world} outside [1, {MAX_SHARDS}]")
-    g = 1
-    while g < world:
-        g <<= 1
-    return g
+    return 1 if world == 1 else MAX_SHARDS
 
 
 def shards_of_rank(rank: int, world: int) -> list[int]:

@@ -57,6 +57,10 @@ def test_shard_assignment_covers_each_shard_once():
         assert g >= world and g & (g - 1) == 0
         got = sorted(i for r in range(world) for i in shards_of_rank(r, world))
         assert got == list(range(g))
+        # balance: no rank holds more than ceil(64 / W) shards of 64
+        if world > 1:
+            most = max(len(shards_of_rank(r, world)) for r in range(world))
+            assert g == 64 and most == -(-64 // world)
     with pytest.raises(ValueError):
         shard_count_for(65)
     with pytest.raises(ValueError):
