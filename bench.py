@@ -77,6 +77,7 @@ def parse():
     p.add_argument("--filter-bits", type=int, default=0)
     p.add_argument("--sweep-v1", action="store_true", help="sweep variant 1 (A/B runs)")
     p.add_argument("--sweep-v2", action="store_true", help="sweep variant 2 (A/B runs)")
+    p.add_argument("--sweep-v3", action="store_true", help="sweep variant 3 (A/B runs)")
     p.add_argument("--cpu-cells", type=int, default=1,
                    help="cells per timed pass of the reference's CPU legs (per process)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -232,7 +233,8 @@ def run_tergpu(args):
         rin.quotient_bits = QBITS
         rin.flags = (_abi.ROOT_DEVICE_INPUTS if resident else 0) | \
             (_abi.ROOT_SWEEP_V1 if args.sweep_v1 else 0) | \
-            (_abi.ROOT_SWEEP_V2 if args.sweep_v2 else 0)
+            (_abi.ROOT_SWEEP_V2 if args.sweep_v2 else 0) | \
+            (_abi.ROOT_SWEEP_V3 if args.sweep_v3 else 0)
         for l in range(3):
             rin.count[l] = sizes[l]
             if resident:
@@ -361,7 +363,8 @@ def run_tergpu(args):
         sm_mhz = clk.get("sm_mhz") or 1965.0
         # algorithmic HBM bytes of one sweep launch: each partitioned list read once (8 B keys)
         sweep_bytes = sum(sizes) * 8
-        sweep_kernel = "k_sweep" if args.sweep_v1 else ("k_sweep2" if args.sweep_v2 else "k_sweep3")
+        sweep_kernel = {1: "k_sweep", 2: "k_sweep2", 3: "k_sweep3", 4: "k_sweep4"}.get(
+            int(outs[-1].sweep_variant), "k_sweep3")
         part_bytes = sum(sizes) * (2 * 9 + 8 + 13 + 4)  # hist read, scatter read + write
         int32_peak = INT32_LANES * sm_mhz * 1e6  # INT32 ops/s
         sweep_pairs_s = local_pairs / (sweep_ms / 1000.0)
@@ -445,7 +448,10 @@ def ref_binary():
                 break
         if need <= have:
             return native, "g++ -O2 -march=native"
-    return plain, "g++ -O2 -march=x86-64-v3 (this host lacks a flag of the native build's CPU)"
+        missing = " ".join(sorted(need - have)[:12])
+        return plain, (f"g++ -O2 -march=x86-64-v3 (this host lacks CPU flags of the native build: "
+                       f"{missing})")
+    return plain, "g++ -O2 -march=x86-64-v3"
 
 
 def cpu_model() -> str:

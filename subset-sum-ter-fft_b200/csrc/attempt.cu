@@ -574,6 +574,19 @@ void size_plan(GraphPlan* g, uint32_t n, uint32_t r1, uint32_t r2, uint64_t l3) 
   }
   g->jb.counters = g->alloc<unsigned long long>(kCounters);
   g->jb.triples = g->alloc<uint32_t>(3 * std::max(g->cap_t, g->cap_r));
+  if (g->tu_root.variant == 4 && std::min<uint32_t>(qroot, 64) - g->tu_root.fb >= 32) {
+    // the root's v4 sweep: A windows and the B lane-slot layout
+    const uint32_t nf4 = 1u << g->tu_root.fb;
+    const uint64_t s4 = v4_slots(g->cap_t, g->tu_root.fb);
+    g->jb.qwin = g->alloc<uint32_t>(g->cap_t + nf4 + 16);
+    g->jb.res4 = g->alloc<uint64_t>(s4);
+    g->jb.hi4 = g->alloc<uint8_t>(s4);
+    g->jb.id4 = g->alloc<uint32_t>(s4);
+    g->jb.win4 = g->alloc<uint32_t>(s4);
+    g->jb.cnt4 = g->alloc<uint32_t>(nf4 + 1);
+    g->jb.off4 = g->alloc<uint32_t>(nf4 + 1);
+    g->jb.cur4 = g->alloc<uint32_t>(nf4 + 1);
+  }
   g->cand = g->entries(g->cap_t);
   g->sort_scratch = g->alloc<uint32_t>(radix_scratch_words(g->cap_t));
   g->perm = g->alloc<uint32_t>(g->cap_t + 16);

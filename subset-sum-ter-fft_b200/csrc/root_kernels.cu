@@ -788,6 +788,340 @@ __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a)
   }
 }
 
+// ---- v4: 0/1 probe table over 14-bit windows, B laid out one bank per lane ----
+//
+// Per pair (a of family s, b of family t, carry kap into the residual): the low
+// 14 bits of the residual sum are sigma = (q_a + x_b + kap) mod 2^14, and the
+// unreduced q_a' + x_b' + kap (q', x' = residuals mod 2^14) lies in [0, 2^15).
+// A D entry with window d' matches when that value is d' or d' + 2^14.  The
+// table word v is 1 when v or v - 1 is one of those values, so a B entry that
+// adds o in {0, 1} to its window (chosen per entry by the layout) still finds
+// every match: table[q' + x' + kap + o] covers both.  The word read by a lane
+// sits in bank (q' + kap + x' + o) mod 32, the same offset for every lane of a
+// warp plus the lane's own (x' + o) mod 32, which the layout makes distinct
+// across the lanes of a row.  Survivors of the table (about 2 |D_u| / 2^14 of
+// the pairs) are resolved exactly as in v3: the 32-bit window through the
+// shared hash of D_u, then the full residual and the high bits.
+
+// Minimal forward flow on the cycle of 32 residual classes: x[c] entries of
+// class c move to bank c + 1 so that no bank holds more than R entries.
+__device__ bool flow4(const uint32_t* n, uint32_t R, uint32_t* x) {
+  for (int c = 0; c < 32; ++c) x[c] = 0u;
+  for (int lap = 0; lap < 3; ++lap) {
+    for (int b = 0; b < 32; ++b) {
+      const int64_t need = static_cast<int64_t>(n[b]) + x[(b + 31) & 31] - static_cast<int64_t>(R);
+      x[b] = need <= 0 ? 0u : (need >= static_cast<int64_t>(n[b]) ? n[b] : static_cast<uint32_t>(need));
+    }
+  }
+  for (int b = 0; b < 32; ++b)
+    if (n[b] - x[b] + x[(b + 31) & 31] > R) return false;
+  return true;
+}
+
+__global__ void k_window4(const uint64_t* __restrict__ res, Count n, uint32_t* __restrict__ win) {
+  const uint64_t m = n.get();
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    win[i] = (static_cast<uint32_t>(res[i]) & ((1u << kW4Bits) - 1u)) << 2;
+  }
+}
+
+// One warp per family: the residual classes' counts, then the fewest rows
+// (minimum plus at most kArrange4ExtraRows) over which the flow balances them;
+// a family that does not balance keeps its order (rows = the minimum).
+// mode 0: cnt4[f] = 32 * rows.  mode 1: also the layout (arrange4).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_arrange4(const uint64_t* __restrict__ res, const uint8_t* __restrict__ hi,
+                                                  const uint32_t* __restrict__ id, const uint32_t* __restrict__ off,
+                                                  const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off4,
+                                                  uint32_t nfam, uint32_t* __restrict__ cnt4,
+                                                  uint64_t* __restrict__ res4, uint8_t* __restrict__ hi4,
+                                                  uint32_t* __restrict__ id4, uint32_t* __restrict__ win4) {
+  __shared__ uint32_t counts[8][32], moved[8][32], rank[8][32], load[8][32], keep[8][32];
+  __shared__ uint32_t rows_of[8];
+  __shared__ int arranged_of[8];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t f = blockIdx.x * 8u + warp;
+  if (f >= nfam) return;  // whole warps leave together
+  const uint32_t n = cnt[f];
+  const uint64_t base = off[f];
+  counts[warp][lane] = 0u;
+  rank[warp][lane] = 0u;
+  __syncwarp();
+  const bool small = n <= kArrange4Cap;
+  if (small) {
+    for (uint32_t i = lane; i < n; i += 32u) atomicAdd(&counts[warp][static_cast<uint32_t>(res[base + i]) & 31u], 1u);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const uint32_t rmin = (n + 31u) >> 5;
+    uint32_t rows = rmin;
+    int arranged = 0;
+    if (small && n != 0) {
+      for (uint32_t extra = 0; extra <= kArrange4ExtraRows && !arranged; ++extra) {
+        if (flow4(counts[warp], rmin + extra, moved[warp])) {
+          rows = rmin + extra;
+          arranged = 1;
+        }
+      }
+    }
+    rows_of[warp] = rows;
+    arranged_of[warp] = arranged;
+  }
+  __syncwarp();
+  const uint32_t rows = rows_of[warp];
+  if (MODE == 0) {
+    if (lane == 0) cnt4[f] = 32u * rows;
+    return;
+  }
+  const bool arranged = arranged_of[warp] != 0;
+  if (arranged) {
+    const uint32_t c = lane;
+    keep[warp][c] = counts[warp][c] - moved[warp][c];
+    __syncwarp();
+    load[warp][c] = keep[warp][c] + moved[warp][(c + 31u) & 31u];
+  } else {
+    load[warp][lane] = 0u;
+  }
+  __syncwarp();
+  const uint64_t out = off4[f];
+  const uint32_t wmask = (1u << kW4Bits) - 1u;
+  for (uint32_t i = lane; i < n; i += 32u) {
+    const uint64_t r = res[base + i];
+    uint32_t pos, o = 0u;
+    if (arranged) {
+      const uint32_t c = static_cast<uint32_t>(r) & 31u;
+      const uint32_t k = atomicAdd(&rank[warp][c], 1u);
+      uint32_t bank = c, slot = k;
+      if (k >= keep[warp][c]) {  // moved on to the next bank, after that bank's own entries
+        bank = (c + 1u) & 31u;
+        slot = keep[warp][bank] + (k - keep[warp][c]);
+        o = 1u;
+      }
+      pos = slot * 32u + bank;
+    } else {
+      pos = i;
+    }
+    res4[out + pos] = r;
+    hi4[out + pos] = hi[base + i];
+    id4[out + pos] = id[base + i];
+    win4[out + pos] = ((static_cast<uint32_t>(r) & wmask) + o) << 2;
+  }
+  // empty lane slots: rows at or above the lane's bank load (arranged), or past n
+  for (uint32_t p = lane; p < 32u * rows; p += 32u) {
+    const bool hole = arranged ? (p >> 5) >= load[warp][p & 31u] : p >= n;
+    if (hole) {
+      res4[out + p] = 0ull;
+      hi4[out + p] = 0;
+      id4[out + p] = 0u;
+      win4[out + p] = kHole4;
+    }
+  }
+}
+
+__device__ __forceinline__ void build_target4(const SweepArgs& a, uint32_t yoff, uint32_t ny, uint32_t* table,
+                                              uint32_t* ywin, uint16_t* yhash, bool yshared) {
+  for (uint32_t i = threadIdx.x; i < kT4Words; i += blockDim.x) table[i] = 0u;
+  for (uint32_t i = threadIdx.x; i < (1u << kY4HashBits); i += blockDim.x) yhash[i] = 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < ny; i += blockDim.x) {
+    const uint32_t w = static_cast<uint32_t>(a.y.res[yoff + i]);  // mrb >= 32: the low 32 bits
+    const uint32_t d = w & ((1u << kW4Bits) - 1u);
+    table[d] = 1u;
+    table[d + 1u] = 1u;
+    table[d + (1u << kW4Bits)] = 1u;
+    table[d + (1u << kW4Bits) + 1u] = 1u;
+    if (yshared) {
+      ywin[i] = w;
+      uint32_t h = yhash_of<kY4HashBits>(w);
+      // at most kY4Cap entries in 2 * kY4Cap slots: an empty slot always exists
+      while (atomicCAS(reinterpret_cast<unsigned short*>(&yhash[h]), (unsigned short)0,
+                       static_cast<unsigned short>(i + 1u)) != 0) {
+        h = (h + 1u) & ((1u << kY4HashBits) - 1u);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <int R>
+__global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a) {
+  static_assert(R >= 1 && R <= 8, "at most 8 rows of B entries per chunk");
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t item_counter;
+  const uint32_t nfam = 1u << a.fb;
+  const uint32_t fmask = nfam - 1u;
+  uint32_t* table = smem;
+  uint32_t* ywin = table + kT4Words;
+  uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kY4Cap);
+  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kY4HashBits));
+  uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweep4Warps * kQueueCap);
+
+  const uint32_t nloc = nfam / a.shards;
+  const uint32_t u = a.shard + a.shards * (blockIdx.x % nloc);
+  const uint32_t part = blockIdx.x / nloc;
+  const uint32_t s_per = (nfam + a.s_split - 1u) / a.s_split;
+  const uint32_t s0 = part * s_per;
+  const uint32_t s1 = min(nfam, s0 + s_per);
+  const uint32_t ny = a.y.cnt[u];
+  if (s0 >= s1 || ny == 0u) return;  // uniform across the block
+  const uint32_t yoff = a.y.off[u];
+  const uint64_t mmask = a.mrb >= 64 ? ~0ull : ((1ull << a.mrb) - 1ull);
+  const bool yshared = ny <= kY4Cap;
+  if (threadIdx.x == 0) item_counter = 0u;
+  build_target4(a, yoff, ny, table, ywin, yhash, yshared);
+
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  uint2* wq = queues + warp * kQueueCap;
+  constexpr uint32_t kChunk = 32u * R;
+  uint32_t* xs = xstage + warp * kChunk;
+  // counters[kMaxX]: the largest B family of the lane-slot layout (a multiple of 32)
+  const uint32_t xc_max = static_cast<uint32_t>((a.counters[kMaxX] + kChunk - 1ull) / kChunk);
+  const uint32_t total_items = (s1 - s0) * xc_max;
+  unsigned long long c_surv = 0, c_fast = 0, c_fall = 0;
+  const uint32_t hi_mask = (1u << a.hi_bits) - 1u;
+  const char* tb = reinterpret_cast<const char*>(table);
+  const uint32_t two = a.two;
+
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total_items) break;
+    const uint32_t s = s0 + item / xc_max;
+    const uint32_t xc = item % xc_max;
+    const uint32_t t = (u - s) & fmask;
+    const uint32_t kap = s > u ? 1u : 0u;
+    if (a.cells != nullptr && a.cells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
+    const uint32_t nq = a.q.cnt[s];
+    const uint32_t nx = a.x.cnt[t];  // lane slots, a multiple of 32
+    const uint32_t xbase = xc * kChunk;
+    if (xbase >= nx || nq == 0u) continue;
+    const uint32_t qoff = a.q.off[s];
+    const uint32_t xoff = a.x.off[t];
+    const uint32_t rows = min(static_cast<uint32_t>(R), (nx - xbase) >> 5);
+    auto run_item = [&](auto rows_tag) {
+      constexpr int RR = decltype(rows_tag)::value;
+      constexpr int QP = ((32 / RR) & ~1) < 16 ? ((32 / RR) & ~1) : 16;
+      constexpr uint32_t kTests = QP * RR;
+      uint32_t x4[RR];
+      uint32_t vmask = kTests >= 32 ? kFull : ((1u << kTests) - 1u);
+#pragma unroll
+      for (int r = 0; r < RR; ++r) {
+        const uint32_t xi = xbase + r * 32u + lane;
+        const uint32_t xw = a.x.win[xoff + xi];
+        const bool valid = xw != kHole4;
+        // an empty slot probes its lane's own bank and never reports
+        x4[r] = valid ? xw + 4u * kap : 4u * (lane + kap);
+        xs[r * 32u + lane] = static_cast<uint32_t>(a.x.res[xoff + xi]);
+        if (!valid) {
+#pragma unroll
+          for (int e = 0; e < QP; ++e) vmask &= ~(1u << (kTests - 1u - (e * RR + r)));
+        }
+      }
+
+      uint32_t qlen = 0;
+      auto drain = [&]() {
+        __syncwarp();
+        for (uint32_t e = lane; e < qlen; e += 32u) {
+          const uint2 rec = wq[e];
+          const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
+          uint32_t mm = rec.y;
+          while (mm != 0u) {
+            const uint32_t b = __ffs(mm) - 1u;
+            mm &= mm - 1u;
+            const uint32_t k = (kTests - 1u) - b;
+            const uint32_t qi = j + k / RR;
+            const uint32_t xi = xbase + (k % RR) * 32u + ln;
+            if (qi >= nq) continue;
+            ++c_surv;
+            const uint64_t rq = a.q.res[qoff + qi];
+            const uint32_t w = static_cast<uint32_t>(rq) + kap + xs[(k % RR) * 32u + ln];
+            auto check = [&](uint32_t idx) {
+              const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
+              const uint64_t ms = sum & mmask;
+              if ((a.y.res[yoff + idx] & mmask) != ms) return;
+              ++c_fast;
+              if (a.hi_bits != 0u) {
+                const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                       static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+                if (high != a.y.hi[yoff + idx]) return;
+              }
+              const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+              if (slot < a.cap) {
+                a.triples[3 * slot] = a.q.id[qoff + qi];
+                a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+                a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+              }
+            };
+            if (yshared) {
+              uint32_t h = yhash_of<kY4HashBits>(w);
+              for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+                if (ywin[v - 1u] == w) check(v - 1u);
+                h = (h + 1u) & ((1u << kY4HashBits) - 1u);
+              }
+            } else {
+              ++c_fall;
+              for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
+            }
+          }
+        }
+        __syncwarp();
+        qlen = 0;
+      };
+
+      const uint32_t* qw = a.q.win + qoff;
+      for (uint32_t j = 0; j < nq; j += QP) {
+        uint32_t m = 0;
+#pragma unroll
+        for (int p = 0; p < QP / 2; ++p) {
+          const uint2 qq = *reinterpret_cast<const uint2*>(qw + j + 2 * p);
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const uint32_t q4 = e ? qq.y : qq.x;
+#pragma unroll
+            for (int r = 0; r < RR; ++r) {
+              const uint32_t f = *reinterpret_cast<const uint32_t*>(tb + (q4 + x4[r]));
+              m = m * two + f;
+            }
+          }
+        }
+        m &= vmask;
+        const bool has = m != 0u;
+        const uint32_t ball = __ballot_sync(kFull, has);
+        if (ball != 0u) {
+          if (qlen + __popc(ball) > kQueueCap) drain();
+          if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
+          qlen += __popc(ball);
+        }
+      }
+      drain();
+    };
+    switch (rows) {
+      case 1: run_item(RowsTag<1>{}); break;
+      case 2: run_item(RowsTag<2>{}); break;
+      case 3: run_item(RowsTag<3>{}); break;
+      case 4: run_item(RowsTag<4>{}); break;
+      case 5: run_item(RowsTag<5 <= R ? 5 : R>{}); break;
+      case 6: run_item(RowsTag<6 <= R ? 6 : R>{}); break;
+      case 7: run_item(RowsTag<7 <= R ? 7 : R>{}); break;
+      default: run_item(RowsTag<R>{}); break;
+    }
+  }
+
+  for (int d = 16; d > 0; d >>= 1) {
+    c_surv += __shfl_down_sync(kFull, c_surv, d);
+    c_fast += __shfl_down_sync(kFull, c_fast, d);
+    c_fall += __shfl_down_sync(kFull, c_fall, d);
+  }
+  if (lane == 0) {
+    if (c_surv) atomicAdd(&a.counters[kSurvivors], c_surv);
+    if (c_fast) atomicAdd(&a.counters[kFast], c_fast);
+    if (c_fall) atomicAdd(&a.counters[kFallback], c_fall);
+  }
+}
+
 // Lays every B family of at most kSortCap entries out in lane slots of 32
 // consecutive entries whose classes (residual mod 32, the bank selector of the
 // v3 probe) are distinct wherever the class counts allow: slot by slot, one
@@ -1079,6 +1413,7 @@ void prepare_root_kernels() {
   allow_max_smem(reinterpret_cast<const void*>(k_sweep2<true, 8>));
   allow_max_smem(reinterpret_cast<const void*>(k_sweep2<false, 8>));
   allow_max_smem(reinterpret_cast<const void*>(k_sweep3<8>));
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep4<8>));
   allow_max_smem(reinterpret_cast<const void*>(k_family_arrange));
   allow_max_smem(reinterpret_cast<const void*>(k_hist_priv));
   allow_max_smem(reinterpret_cast<const void*>(k_scatter_priv));
@@ -1161,6 +1496,39 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
     allow_max_smem(reinterpret_cast<const void*>(k_sweep2<false, 8>));
     k_sweep2<false, 8><<<grid, kSweepThreads, smem, st>>>(a);
   }
+}
+
+size_t sweep4_smem_bytes() {
+  return static_cast<size_t>(kT4Words) * 4 + kY4Cap * 4 + (static_cast<size_t>(1) << kY4HashBits) * 2 +
+         static_cast<size_t>(kSweep4Warps) * kQueueCap * sizeof(uint2) +
+         static_cast<size_t>(kSweep4Warps) * 32 * 8 * 4;
+}
+
+void launch_sweep4(const SweepArgs& a, cudaStream_t st) {
+  const unsigned grid = ((1u << a.fb) / a.shards) * a.s_split;
+  SweepArgs b = a;
+  b.two = 2u;
+  allow_max_smem(reinterpret_cast<const void*>(k_sweep4<8>));
+  k_sweep4<8><<<grid, kSweep4Threads, sweep4_smem_bytes(), st>>>(b);
+}
+
+void launch_window4(const uint64_t* res, Count n, uint32_t* win, cudaStream_t st) {
+  if (n.cap == 0) return;
+  k_window4<<<grid_for_count(n, 256), 256, 0, st>>>(res, n, win);
+}
+
+void launch_rows4(const uint64_t* res, const uint32_t* off, const uint32_t* cnt, uint32_t nfam,
+                  uint32_t* cnt4, cudaStream_t st) {
+  k_arrange4<0><<<(nfam + 7) / 8, 256, 0, st>>>(res, nullptr, nullptr, off, cnt, nullptr, nfam, cnt4,
+                                                nullptr, nullptr, nullptr, nullptr);
+}
+
+void launch_arrange4(const uint64_t* res, const uint8_t* hi, const uint32_t* id, const uint32_t* off,
+                     const uint32_t* cnt, const uint32_t* off4, const uint32_t* cnt4, uint32_t nfam,
+                     uint64_t* res4, uint8_t* hi4, uint32_t* id4, uint32_t* win4, cudaStream_t st) {
+  (void)cnt4;
+  k_arrange4<1><<<(nfam + 7) / 8, 256, 0, st>>>(res, hi, id, off, cnt, off4, nfam, nullptr, res4, hi4,
+                                                id4, win4);
 }
 
 void launch_sweep3(const SweepArgs& a, cudaStream_t st) {

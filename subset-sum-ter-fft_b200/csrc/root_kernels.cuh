@@ -36,12 +36,29 @@ constexpr int kSweep3Warps = kSweep3Threads / 32;
 constexpr uint32_t kY3HashBits = 12;
 constexpr uint32_t kY3Cap = 2048;
 
+// v4: one CTA of 24 warps per SM.  The probe table covers the low kW4Bits bits
+// of the residuals: word v (2^15 + 1 of them) is 1 when v or v - 1 is the sum
+// window of a D entry (each D entry sets four words), so a probe is an add, one
+// shared load and a shift-add of the loaded 0/1 into the test mask.
+constexpr uint32_t kW4Bits = 14;
+constexpr uint32_t kT4Words = (1u << (kW4Bits + 1)) + 32;
+constexpr int kSweep4Threads = 768;
+constexpr int kSweep4Warps = kSweep4Threads / 32;
+constexpr uint32_t kY4HashBits = 11;
+constexpr uint32_t kY4Cap = 1024;
+// B families of up to kArrange4Cap entries are laid out one bank per lane (at
+// most kArrange4ExtraRows rows beyond the minimum); larger ones stay in order.
+constexpr uint32_t kArrange4Cap = 4096;
+constexpr uint32_t kArrange4ExtraRows = 2;
+constexpr uint32_t kHole4 = 0xFFFFFFFFu;  // window of an empty lane slot
+
 struct ListView {
   const uint64_t* res;
   const uint8_t* hi;
   const uint32_t* id;
   const uint32_t* off;
   const uint32_t* cnt;
+  const uint32_t* win = nullptr;  // v4: 4 * (probe window [+ bank offset]) per entry, or null
 };
 
 // Counting bound in the order the reference's tiled reporter visits the
@@ -71,6 +88,7 @@ struct SweepArgs {
   uint32_t hi_bits;         // key bits above 64 (0 when Q <= 64)
   uint32_t project;         // 1: count triples on mrb residual bits only
   VisitBound visit;         // projected counts: only triples visited before this bound
+  uint32_t two;             // 2, as an opaque operand (v4 keeps its mask shift-add an IMAD)
   uint32_t* triples;        // 3 * cap
   unsigned long long cap;
   unsigned long long* counters;  // [0] triples [1] survivors [2] fast [3] projected [4] fallback
@@ -110,6 +128,26 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st);
 // value, so the bank is borrow-free; conflict-free once every B family is laid
 // out by launch_family_arrange.  Exact for any family order.
 void launch_sweep3(const SweepArgs& a, cudaStream_t st);
+// v4 (needs mrb >= 32): probe table of 0/1 words over 14-bit windows, B in the
+// lane-per-bank layout of launch_arrange4 (a.x = that layout, a.x.win its
+// windows), A windows in a.q.win.  Exact for any layout.
+void launch_sweep4(const SweepArgs& a, cudaStream_t st);
+size_t sweep4_smem_bytes();
+// win[i] = 4 * (res[i] mod 2^kW4Bits) for the n slots of a partitioned list.
+void launch_window4(const uint64_t* res, Count n, uint32_t* win, cudaStream_t st);
+// v4 layout of the B list, in two launches around a scan: rows4 writes cnt4[f] =
+// 32 * (the rows family f takes); arrange4 writes family f at off4[f] as rows of
+// 32 lane slots where the entry in lane b probes bank b (its residual class c
+// shifted by o in {0, 1}, o folded into its window, so c + o == b mod 32), and
+// marks the empty slots with the window kHole4.  Families above kArrange4Cap, or
+// whose classes do not balance within kArrange4ExtraRows more rows, keep their
+// order (same results, more bank conflicts).
+void launch_rows4(const uint64_t* res, const uint32_t* off, const uint32_t* cnt, uint32_t nfam,
+                  uint32_t* cnt4, cudaStream_t st);
+void launch_arrange4(const uint64_t* res, const uint8_t* hi, const uint32_t* id, const uint32_t* off,
+                     const uint32_t* cnt, const uint32_t* off4, const uint32_t* cnt4, uint32_t nfam,
+                     uint64_t* res4, uint8_t* hi4, uint32_t* id4, uint32_t* win4, cudaStream_t st);
+
 // Lays every B family (of at most kSortCap entries) out in lane slots of 32
 // entries with distinct residual classes mod 32 wherever the counts allow.
 void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,

@@ -30,7 +30,9 @@ thread_local std::string t_error;
 enum Slot {
   kSlotKeyLo = 0, kSlotKeyHi = 3, kSlotInId = 6, kSlotRes = 9, kSlotHi = 12, kSlotId = 15,
   kSlotCnt = 18, kSlotOff = 21, kSlotCur = 24, kSlotCells = 27, kSlotTriples = 28,
-  kSlotCounters = 29, kSlotRecords = 30, kSlotFlags = 33, kSlots = 34
+  kSlotCounters = 29, kSlotRecords = 30, kSlotFlags = 33, kSlotQWin = 34, kSlotRes4 = 35,
+  kSlotHi4 = 36, kSlotId4 = 37, kSlotWin4 = 38, kSlotCnt4 = 39, kSlotOff4 = 40, kSlotCur4 = 41,
+  kSlots = 42
 };
 
 std::mutex g_mu;
@@ -140,12 +142,20 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
                      uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards,
                      uint64_t n_q) {
   Tuning t;
-  t.variant = variant == 0 ? 3u : variant;
+  t.variant = variant == 0 ? 4u : variant;
   const bool v2 = t.variant != 1;
   uint32_t fb_max = std::min<uint32_t>(14, fast_bits - 2);
   if (projected != 0) fb_max = std::min<uint32_t>(fb_max, projected - 6);
   if (fb_req != 0) {
     t.fb = fb_req;
+  } else if (t.variant == 4) {
+    // v4: about 256 D entries per family (a table survivor rate of about
+    // 2 |D_u| / 2^14, B families of a few rows of 32)
+    const double ideal = std::log2(std::max<double>(1.0, static_cast<double>(n_d) / 256.0));
+    t.fb = static_cast<uint32_t>(std::max(6.0, std::floor(ideal + 0.5)));
+    t.fb = std::min<uint32_t>(t.fb, std::min<uint32_t>(16, fast_bits > 34 ? fast_bits - 32 : 6));
+    if (projected != 0) t.fb = std::min(t.fb, fb_max);
+    t.fb = std::max<uint32_t>(t.fb, 6);
   } else {
     const double per = v2 ? 2048.0 : 1024.0;
     const double ideal = std::log2(std::max<double>(1.0, static_cast<double>(n_d) / per));
@@ -163,8 +173,8 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   const uint64_t avg_x = std::max<uint64_t>(1, n_x >> t.fb);
   if (filter_req != 0) {
     t.wb = filter_req - 5;
-  } else if (t.variant == 3) {
-    t.wb = 15;  // the widest filter the 24-warp CTA holds: best measured at n = 72 and 108
+  } else if (t.variant == 3 || t.variant == 4) {
+    t.wb = 15;  // v3: the widest filter the 24-warp CTA holds (best measured at n = 72 and 108)
   } else if (v2) {
     t.wb = std::clamp<uint32_t>(ceil_log2(avg_x) + 3, 6, 14);
   } else {
@@ -173,7 +183,8 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   t.sort_bits = std::min<uint32_t>(t.wb, 12);
   const uint32_t nfam = 1u << t.fb;
   const uint32_t nloc = std::max<uint32_t>(1, nfam / shards);  // target families per shard
-  uint64_t target_ctas = 148 * (t.variant == 3 ? 1 : 2) * 8;  // about 8 waves of resident CTAs
+  const bool one_cta = t.variant == 3 || t.variant == 4;     // one CTA of 24 warps per SM
+  uint64_t target_ctas = 148 * (one_cta ? 1 : 2) * 8;          // about 8 waves of resident CTAs
   if (n_q != 0) {
     const double pairs = static_cast<double>(n_q) * static_cast<double>(n_x) / shards;
     target_ctas = std::min<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / (1u << 20)) + 1);
@@ -184,17 +195,22 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   // 128 families of ~144 B entries had 26 items for 24 warps: half the SM time
   // idle; 8 per warp measured 5 % more batched n = 72 attempts per second than 4)
   const uint64_t chunks = (avg_x + 255) / 256;
-  const uint64_t warps = t.variant == 3 ? kSweep3Warps : kSweepWarps;
+  const uint64_t warps = one_cta ? kSweep3Warps : kSweepWarps;
   const uint64_t most = std::max<uint64_t>(1, nfam * chunks / (8 * warps));
   t.s_split = static_cast<uint32_t>(std::min<uint64_t>(t.s_split, most));
   return t;
 }
 
-uint64_t partition_bytes(const uint64_t count[3], uint32_t fb) {
+uint64_t partition_bytes(const uint64_t count[3], uint32_t fb, uint32_t variant) {
   uint64_t b = 0;
   for (int l = 0; l < 3; ++l) {
     const uint64_t slots = count[l] + (1ull << fb) + 16;
     b += slots * (8 + 1 + 4);
+    b += 3ull * ((1ull << fb) + 1) * 4;
+  }
+  if (variant == 4) {  // A windows, the B lane-slot layout with its windows and tables
+    b += (count[0] + (1ull << fb) + 16) * 4;
+    b += v4_slots(count[1], fb) * (8 + 1 + 4 + 4);
     b += 3ull * ((1ull << fb) + 1) * 4;
   }
   return b;
@@ -206,6 +222,7 @@ bool autotune_requested(uint32_t flags) { return (flags & TERGPU_ROOT_AUTOTUNE) 
 uint32_t sweep_variant(uint32_t flags) {
   if ((flags & TERGPU_ROOT_SWEEP_V1) != 0) return 1;
   if ((flags & TERGPU_ROOT_SWEEP_V2) != 0) return 2;
+  if ((flags & TERGPU_ROOT_SWEEP_V3) != 0) return 3;
   return 0;
 }
 
@@ -239,10 +256,22 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
   launch_max_family(b.cnt[0], nfam, b.counters, kMaxQ, st);
   launch_max_family(b.cnt[1], nfam, b.counters, kMaxX, st);
   *launches += 2;
-  // v3 needs full 32-bit windows (mrb >= 32); below that the B-in-registers
-  // sweep (v2) runs, exact for any family order.
-  const uint32_t main_variant = tu.variant == 3 && F - tu.fb < 32 ? 2u : tu.variant;
-  if (main_variant == 3 && j.count[1].cap != 0) {
+  // v3 and v4 need full 32-bit windows (mrb >= 32); below that the
+  // B-in-registers sweep (v2) runs, exact for any family order.
+  uint32_t main_variant = (tu.variant == 3 || tu.variant == 4) && F - tu.fb < 32 ? 2u : tu.variant;
+  if (main_variant == 4 && b.res4 == nullptr) main_variant = 3;
+  ListView x4view{};
+  if (main_variant == 4) {
+    // A probe windows; the B list in lane slots, one bank per lane
+    launch_window4(b.res[0], Count(j.count[0].cap + nfam + 16), b.qwin, st);
+    launch_rows4(b.res[1], b.off[1], b.cnt[1], nfam, b.cnt4, st);
+    launch_scan(b.cnt4, nfam, b.off4, b.cur4, st);
+    launch_arrange4(b.res[1], b.hi[1], b.id[1], b.off[1], b.cnt[1], b.off4, b.cnt4, nfam, b.res4, b.hi4,
+                    b.id4, b.win4, st);
+    launch_max_family(b.cnt4, nfam, b.counters, kMaxX, st);
+    *launches += 5;
+    x4view = ListView{b.res4, b.hi4, b.id4, b.off4, b.cnt4, b.win4};
+  } else if (main_variant == 3 && j.count[1].cap != 0) {
     // B families in lane slots of distinct residual classes mod 32 (bank-free probes)
     launch_family_arrange(b.res[1], b.hi[1], b.id[1], b.off[1], b.cnt[1], nfam, st);
     *launches += 1;
@@ -252,7 +281,12 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
     *launches += 1;
   }
   auto sweep = [&](const SweepArgs& sa) {
-    if (main_variant == 3 && sa.mrb >= 32) {
+    if (main_variant == 4 && sa.mrb >= 32 && sa.project == 0) {
+      SweepArgs a4 = sa;
+      a4.q.win = b.qwin;
+      a4.x = x4view;
+      launch_sweep4(a4, st);
+    } else if (main_variant == 3 && sa.mrb >= 32) {
       launch_sweep3(sa, st);
     } else if (main_variant == 1) {
       launch_sweep(sa, sa.mrb < 32, st);
@@ -317,11 +351,12 @@ uint32_t size_bucket(uint64_t n) {
 
 Tuned autotune(Workspace& w, const JoinInput& in, uint64_t input_bytes, float* spent_ms) {
   const uint32_t F = std::min<uint32_t>(in.quotient_bits, 64);
-  const Tuning base = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, 0, 0, 3, 1, in.count[0]);
+  // neighbours of each variant's own size-based choice
+  (void)0;
   Tuned best;
   float best_ms = 0;
   *spent_ms = 0;
-  for (uint32_t variant : {3u, 2u}) {
+  for (uint32_t variant : {4u, 3u, 2u}) {
     for (int dfb = -1; dfb <= 1; ++dfb) {
       for (int dfl = -1; dfl <= 1; ++dfl) {
         JoinInput j = in;
@@ -331,6 +366,8 @@ Tuned autotune(Workspace& w, const JoinInput& in, uint64_t input_bytes, float* s
         j.projected_bits = 0;
         j.shard = 0;
         j.shards = 64;
+        const Tuning base = choose_tuning(in.count[1], in.count[2], F, 0, 0, 0, variant, 1, in.count[0]);
+        if (variant == 4 && dfl != 0) continue;  // v4's table has no width to tune
         j.family_bits = static_cast<uint32_t>(static_cast<int>(base.fb) + dfb);
         j.filter_bits = static_cast<uint32_t>(static_cast<int>(base.wb) + 5 + dfl);
         j.sweep_variant = variant;
@@ -395,7 +432,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     throw Failure{TERGPU_INVALID_INPUT};
   }
   const uint32_t nfam = 1u << tu.fb;
-  const uint64_t need = input_bytes + partition_bytes(in.count, tu.fb) +
+  const uint64_t need = input_bytes + partition_bytes(in.count, tu.fb, tu.variant) +
                         (in.count_only ? 0 : in.capacity * 12) + 4096 + 64;
   r.device_bytes = need;
   if (in.memory_limit_bytes != 0 && need > in.memory_limit_bytes) {
@@ -419,6 +456,18 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   }
   unsigned long long* counters = ensure<unsigned long long>(w, kSlotCounters, kCounters * 8);
   uint32_t* d_triples = ensure<uint32_t>(w, kSlotTriples, std::max<uint64_t>(in.capacity, 1) * 12);
+  JoinBuffers jb{};
+  if (tu.variant == 4 && F - tu.fb >= 32 && (!in.count_only || in.projected_bits == 0)) {
+    const uint64_t s4 = v4_slots(in.count[1], tu.fb);
+    jb.qwin = ensure<uint32_t>(w, kSlotQWin, (in.count[0] + nfam + 16) * 4);
+    jb.res4 = ensure<uint64_t>(w, kSlotRes4, s4 * 8);
+    jb.hi4 = ensure<uint8_t>(w, kSlotHi4, s4);
+    jb.id4 = ensure<uint32_t>(w, kSlotId4, s4 * 4);
+    jb.win4 = ensure<uint32_t>(w, kSlotWin4, s4 * 4);
+    jb.cnt4 = ensure<uint32_t>(w, kSlotCnt4, (nfam + 1) * 4ull);
+    jb.off4 = ensure<uint32_t>(w, kSlotOff4, (nfam + 1) * 4ull);
+    jb.cur4 = ensure<uint32_t>(w, kSlotCur4, (nfam + 1) * 4ull);
+  }
   const uint8_t* d_cells = in.cells_device;
   if (d_cells == nullptr && in.cells != nullptr) {
     uint8_t* c = ensure<uint8_t>(w, kSlotCells, 4096);
@@ -426,7 +475,6 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     d_cells = c;
   }
   check(cudaEventRecord(w.start, st), "event");
-  JoinBuffers jb{};
   for (int l = 0; l < 3; ++l) {
     jb.res[l] = res[l];
     jb.hi[l] = hi[l];
@@ -476,12 +524,18 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
       check(cudaMemcpy(hcells.data(), d_cells, 4096, cudaMemcpyDeviceToHost), "cells download");
     }
   }
+  // B sizes by t mod 64: the cell mask and the shard (shards | 64) see only that
+  const uint32_t cls = std::min<uint32_t>(nfam, 64);
+  uint64_t bsum[64] = {};
+  for (uint32_t t = 0; t < nfam; ++t) bsum[t & (cls - 1u)] += hcnt[1][t];
   for (uint32_t s = 0; s < nfam; ++s) {
-    for (uint32_t t = 0; t < nfam; ++t) {
-      if (((s + t) & (nfam - 1u) & (in.shards - 1u)) != in.shard) continue;
-      if (!hcells.empty() && hcells[((s & 63u) << 6) | (t & 63u)] == 0) continue;
-      r.pairs += static_cast<uint64_t>(hcnt[0][s]) * hcnt[1][t];
+    uint64_t b = 0;
+    for (uint32_t c = 0; c < cls; ++c) {
+      if (((s + c) & (nfam - 1u) & (in.shards - 1u)) != in.shard) continue;
+      if (!hcells.empty() && hcells[((s & 63u) << 6) | c] == 0) continue;
+      b += bsum[c];
     }
+    r.pairs += static_cast<uint64_t>(hcnt[0][s]) * b;
   }
   r.triples = hc[kTriples];
   r.survivors = hc[kSurvivors];

@@ -80,7 +80,9 @@ T* ensure(Workspace& w, int slot, size_t bytes) {
 
 struct Tuning {
   uint32_t fb = 6, wb = 12, s_split = 1, sort_bits = 0;
-  uint32_t variant = 3;  // sweep: 1 (A in registers), 2 (B in registers), 3 (v2 + bank-free probes)
+  // sweep: 1 (A in registers), 2 (B in registers), 3 (v2 + bank-free probes),
+  // 4 (0/1 probe table over 14-bit windows, B laid out one bank per lane)
+  uint32_t variant = 4;
 };
 
 // Device-resident inputs of one join: keys per list.
@@ -137,7 +139,23 @@ struct JoinBuffers {
   uint32_t *cnt[3], *off[3], *cur[3];
   unsigned long long* counters;
   uint32_t* triples;
+  // v4 (null: v4 is not run): the A list's probe windows (A slots), the B list
+  // in the lane-slot layout (v4_slots(count_B, fb) slots) with its windows, and
+  // that layout's family sizes and offsets (2^fb + 1 words each)
+  uint32_t* qwin = nullptr;
+  uint64_t* res4 = nullptr;
+  uint8_t* hi4 = nullptr;
+  uint32_t* id4 = nullptr;
+  uint32_t* win4 = nullptr;
+  uint32_t *cnt4 = nullptr, *off4 = nullptr, *cur4 = nullptr;
 };
+
+// Lane slots the v4 layout of a B list of `count` entries in 2^fb families can
+// take: every family is padded to whole rows of 32 with at most
+// kArrange4ExtraRows rows more than the minimum.
+inline uint64_t v4_slots(uint64_t count, uint32_t fb) {
+  return count + (static_cast<uint64_t>(32) * (kArrange4ExtraRows + 1)) * (uint64_t{1} << fb) + 64;
+}
 
 // The inputs of one join: keys per list with host or device counts.
 struct JoinWork {

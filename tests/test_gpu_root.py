@@ -29,8 +29,8 @@ def keys_of(oracle_mod, bits, seed, size, pool):
 
 
 def vcfg(variant):
-    """Config keywords selecting sweep variant 1, 2 or 3 (the default)."""
-    return {"sweep_v1": variant == 1, "sweep_v2": variant == 2}
+    """Config keywords selecting sweep variant 1, 2, 3 or 4 (the default)."""
+    return {"sweep_v1": variant == 1, "sweep_v2": variant == 2, "sweep_v3": variant == 3}
 
 
 def assert_digest(got, expected):
@@ -38,7 +38,7 @@ def assert_digest(got, expected):
         assert got[k] == hexint(expected[k]), (k, got[k], expected[k])
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("case", range(6))
 def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case, variant):
     from tergpu import workload
@@ -56,7 +56,7 @@ def test_synthetic_roots_match_reference(tg, oracle_mod, golden, case, variant):
     assert sub.telemetry.logical_pairs == g["subsample700"]["logical_pairs"]
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("fb,filt", [(6, 10), (6, 19), (7, 12), (8, 15), (9, 20), (10, 11)])
 def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt, variant):
     from tergpu import workload
@@ -68,7 +68,7 @@ def test_result_is_independent_of_tuning(tg, oracle_mod, golden, fb, filt, varia
     assert_digest(workload.digest(res.triples), g["brute"])
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("bits", [24, 33, 40, 47, 58, 64, 65, 69, 72])
 def test_widths_against_oracle(tg, oracle_mod, bits, variant):
     """Every key width from the n=36 root (24) to the one-byte high limit (72),
@@ -221,7 +221,7 @@ def test_large_planted_root_is_exact_and_deterministic(tg):
     assert r1.telemetry.logical_pairs == n[0] * n[1]
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("count", [2, 8, 64])
 def test_shards_union_equals_whole_root(tg, oracle_mod, golden, count, variant):
     """The multi-GPU split run shard by shard on one device: disjoint shards
@@ -272,7 +272,7 @@ def test_autotune_is_exact_and_cached(tg, oracle_mod, golden):
     second = tg.run_gpu_root(keys, tg.Config(autotune=True))
     for res in (first, second):
         assert_digest(workload.digest(res.triples), g["brute"])
-        assert res.telemetry.sweep_variant in (2, 3)
+        assert res.telemetry.sweep_variant in (2, 3, 4)
     assert first.telemetry.tune_ms > 0 and second.telemetry.tune_ms == 0
     assert (first.telemetry.family_bits, first.telemetry.filter_bits,
             first.telemetry.sweep_variant) == (second.telemetry.family_bits,
