@@ -77,7 +77,7 @@ def parse():
     p.add_argument("--filter-bits", type=int, default=0)
     p.add_argument("--sweep-v1", action="store_true", help="sweep variant 1 (A/B runs)")
     p.add_argument("--sweep-v2", action="store_true", help="sweep variant 2 (A/B runs)")
-    p.add_argument("--sweep-v3", action="store_true", help="sweep variant 3 (A/B runs)")
+    p.add_argument("--sweep-v4", action="store_true", help="sweep variant 4 (A/B runs)")
     p.add_argument("--cpu-cells", type=int, default=1,
                    help="cells per timed pass of the reference's CPU legs (per process)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -234,7 +234,7 @@ def run_tergpu(args):
         rin.flags = (_abi.ROOT_DEVICE_INPUTS if resident else 0) | \
             (_abi.ROOT_SWEEP_V1 if args.sweep_v1 else 0) | \
             (_abi.ROOT_SWEEP_V2 if args.sweep_v2 else 0) | \
-            (_abi.ROOT_SWEEP_V3 if args.sweep_v3 else 0)
+            (_abi.ROOT_SWEEP_V4 if args.sweep_v4 else 0)
         for l in range(3):
             rin.count[l] = sizes[l]
             if resident:

@@ -64,15 +64,18 @@ enum tergpu_status {
                                         variant flag is given); same results */
 #define TERGPU_ROOT_SWEEP_V2 8u      /* sweep variant 2: B in registers (families sorted by
                                         window), A broadcast.  Same results */
-#define TERGPU_ROOT_SWEEP_V3 32u     /* sweep variant 3: variant 2 with B families laid out in
-                                        lane slots of distinct residual classes and filter
-                                        words picked by the low probe bits (bank-free
-                                        shared-memory probes).  Default (no variant flag):
-                                        variant 4, a table of 0/1 words over the low 14
+#define TERGPU_ROOT_SWEEP_V4 32u     /* sweep variant 4: a table of 0/1 words over the low 14
                                         residual bits probed with one add, one shared load
                                         and one shift-add per pair, B families laid out one
-                                        bank per lane.  Variants 3 and 4 need 32 or more
-                                        residual bits, else variant 2 runs.  Same results */
+                                        bank per lane; its table passes about 2.5 % of the
+                                        pairs (the default's filter 0.16 %), which makes it
+                                        slower at n = 108.  Default (no variant flag):
+                                        variant 3, variant 2 with B families laid out in
+                                        lane slots of distinct residual classes and filter
+                                        words picked by the low probe bits (bank-free
+                                        shared-memory probes).  Variants 3 and 4 need 32 or
+                                        more residual bits, else variant 2 runs.  Same
+                                        results */
 
 /*
  * One L1 -> L0 root on full quotient keys.

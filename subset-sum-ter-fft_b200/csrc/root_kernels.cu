@@ -954,8 +954,7 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
   uint32_t* table = smem;
   uint32_t* ywin = table + kT4Words;
   uint16_t* yhash = reinterpret_cast<uint16_t*>(ywin + kY4Cap);
-  uint2* queues = reinterpret_cast<uint2*>(yhash + (1u << kY4HashBits));
-  uint32_t* xstage = reinterpret_cast<uint32_t*>(queues + kSweep4Warps * kQueueCap);
+  uint32_t* xstage = reinterpret_cast<uint32_t*>(yhash + (1u << kY4HashBits));
 
   const uint32_t nloc = nfam / a.shards;
   const uint32_t u = a.shard + a.shards * (blockIdx.x % nloc);
@@ -972,10 +971,10 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
   build_target4(a, yoff, ny, table, ywin, yhash, yshared);
 
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t lanemask_lt = (1u << lane) - 1u;
-  uint2* wq = queues + warp * kQueueCap;
   constexpr uint32_t kChunk = 32u * R;
-  uint32_t* xs = xstage + warp * kChunk;
+  uint32_t* xs = xstage + warp * (kChunk + kA4Seg + 16u + kS4Cap);  // the chunk's B windows
+  uint32_t* qs = xs + kChunk;                        // a segment of the A family's windows
+  uint32_t* sv = qs + kA4Seg + 16u;                  // survivors: A index << 8 | row << 5 | lane
   // counters[kMaxX]: the largest B family of the lane-slot layout (a multiple of 32)
   const uint32_t xc_max = static_cast<uint32_t>((a.counters[kMaxX] + kChunk - 1ull) / kChunk);
   const uint32_t total_items = (s1 - s0) * xc_max;
@@ -1010,69 +1009,80 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
 #pragma unroll
       for (int r = 0; r < RR; ++r) {
         const uint32_t xi = xbase + r * 32u + lane;
-        const uint32_t xw = a.x.win[xoff + xi];
+        // rows past the chunk's end are probed as empty slots
+        const uint32_t xw = static_cast<uint32_t>(r) < rows ? a.x.win[xoff + xi] : kHole4;
         const bool valid = xw != kHole4;
         // an empty slot probes its lane's own bank and never reports
         x4[r] = valid ? xw + 4u * kap : 4u * (lane + kap);
-        xs[r * 32u + lane] = static_cast<uint32_t>(a.x.res[xoff + xi]);
+        xs[r * 32u + lane] = valid ? static_cast<uint32_t>(a.x.res[xoff + xi]) : 0u;
         if (!valid) {
 #pragma unroll
           for (int e = 0; e < QP; ++e) vmask &= ~(1u << (kTests - 1u - (e * RR + r)));
         }
       }
+      __syncwarp();
 
-      uint32_t qlen = 0;
+      uint32_t slen = 0, seg = 0;
+      // one table survivor (A entry seg + qrel, row r, lane ln): the 32-bit
+      // window of the sum through the exact hash of D_u, then the full
+      // residual and the high bits; entries past the A family are skipped
+      auto resolve = [&](uint32_t qrel, uint32_t r, uint32_t ln) {
+        const uint32_t qi = seg + qrel;
+        if (qi >= nq) return;
+        ++c_surv;
+        const uint32_t w = qs[qrel] + kap + xs[r * 32u + ln];
+        const uint32_t xi = xbase + r * 32u + ln;
+        auto check = [&](uint32_t idx) {
+          const uint64_t rq = a.q.res[qoff + qi];
+          const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
+          const uint64_t ms = sum & mmask;
+          if ((a.y.res[yoff + idx] & mmask) != ms) return;
+          ++c_fast;
+          if (a.hi_bits != 0u) {
+            const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
+                                   static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
+            if (high != a.y.hi[yoff + idx]) return;
+          }
+          const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+          if (slot < a.cap) {
+            a.triples[3 * slot] = a.q.id[qoff + qi];
+            a.triples[3 * slot + 1] = a.x.id[xoff + xi];
+            a.triples[3 * slot + 2] = a.y.id[yoff + idx];
+          }
+        };
+        if (yshared) {
+          uint32_t h = yhash_of<kY4HashBits>(w);
+          for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
+            if (ywin[v - 1u] == w) check(v - 1u);
+            h = (h + 1u) & ((1u << kY4HashBits) - 1u);
+          }
+        } else {
+          ++c_fall;
+          for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
+        }
+      };
+      // the collected survivors, 32 at a time
       auto drain = [&]() {
         __syncwarp();
-        for (uint32_t e = lane; e < qlen; e += 32u) {
-          const uint2 rec = wq[e];
-          const uint32_t j = rec.x >> 5, ln = rec.x & 31u;
-          uint32_t mm = rec.y;
-          while (mm != 0u) {
-            const uint32_t b = __ffs(mm) - 1u;
-            mm &= mm - 1u;
-            const uint32_t k = (kTests - 1u) - b;
-            const uint32_t qi = j + k / RR;
-            const uint32_t xi = xbase + (k % RR) * 32u + ln;
-            if (qi >= nq) continue;
-            ++c_surv;
-            const uint64_t rq = a.q.res[qoff + qi];
-            const uint32_t w = static_cast<uint32_t>(rq) + kap + xs[(k % RR) * 32u + ln];
-            auto check = [&](uint32_t idx) {
-              const uint64_t sum = rq + a.x.res[xoff + xi] + kap;  // residuals < 2^58: no overflow
-              const uint64_t ms = sum & mmask;
-              if ((a.y.res[yoff + idx] & mmask) != ms) return;
-              ++c_fast;
-              if (a.hi_bits != 0u) {
-                const uint32_t high = (static_cast<uint32_t>(a.q.hi[qoff + qi]) + a.x.hi[xoff + xi] +
-                                       static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
-                if (high != a.y.hi[yoff + idx]) return;
-              }
-              const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
-              if (slot < a.cap) {
-                a.triples[3 * slot] = a.q.id[qoff + qi];
-                a.triples[3 * slot + 1] = a.x.id[xoff + xi];
-                a.triples[3 * slot + 2] = a.y.id[yoff + idx];
-              }
-            };
-            if (yshared) {
-              uint32_t h = yhash_of<kY4HashBits>(w);
-              for (uint32_t v = yhash[h]; v != 0u; v = yhash[h]) {
-                if (ywin[v - 1u] == w) check(v - 1u);
-                h = (h + 1u) & ((1u << kY4HashBits) - 1u);
-              }
-            } else {
-              ++c_fall;
-              for (uint32_t idx = 0; idx < ny; ++idx) check(idx);
-            }
-          }
+        for (uint32_t e = lane; e < slen; e += 32u) {
+          const uint32_t rec = sv[e];
+          resolve(rec >> 8, (rec >> 5) & 7u, rec & 31u);
         }
         __syncwarp();
-        qlen = 0;
+        slen = 0;
       };
 
       const uint32_t* qw = a.q.win + qoff;
-      for (uint32_t j = 0; j < nq; j += QP) {
+      // segments of whole masks (QP entries), so no mask straddles two segments
+      constexpr uint32_t kSeg = (kA4Seg / QP) * QP;
+      for (seg = 0; seg < nq; seg += kSeg) {
+      // the segment's 32-bit A windows (and up to 15 entries past it, for the
+      // last mask; entries past the family are skipped by their index)
+      const uint32_t seg_end = min(nq, seg + kSeg);
+      for (uint32_t i = lane; i < seg_end - seg + 16u; i += 32u)
+        qs[i] = static_cast<uint32_t>(a.q.res[qoff + seg + i]);
+      __syncwarp();
+      for (uint32_t j = seg; j < seg_end; j += QP) {
         uint32_t m = 0;
 #pragma unroll
         for (int p = 0; p < QP / 2; ++p) {
@@ -1088,26 +1098,42 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
           }
         }
         m &= vmask;
-        const bool has = m != 0u;
-        const uint32_t ball = __ballot_sync(kFull, has);
-        if (ball != 0u) {
-          if (qlen + __popc(ball) > kQueueCap) drain();
-          if (has) wq[qlen + __popc(ball & lanemask_lt)] = make_uint2((j << 5) | lane, m);
-          qlen += __popc(ball);
+        // table survivors: compacted one per record (a warp prefix sum of the
+        // mask popcounts), resolved 32 at a time by drain()
+        const uint32_t mine = __popc(m);
+        uint32_t incl = mine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t o = __shfl_up_sync(kFull, incl, d);
+          if (lane >= static_cast<uint32_t>(d)) incl += o;
         }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        if (total == 0u) continue;
+        if (slen + total > kS4Cap) drain();
+        if (total > kS4Cap) {  // more than the buffer holds (a dense D family): each lane its own
+          while (m != 0u) {
+            const uint32_t b = __ffs(m) - 1u;
+            m &= m - 1u;
+            const uint32_t k = (kTests - 1u) - b;
+            resolve(j - seg + k / RR, k % RR, lane);
+          }
+          __syncwarp();
+          continue;
+        }
+        uint32_t at = slen + incl - mine;
+        while (m != 0u) {
+          const uint32_t b = __ffs(m) - 1u;
+          m &= m - 1u;
+          const uint32_t k = (kTests - 1u) - b;
+          sv[at++] = ((j - seg + k / RR) << 8) | ((k % RR) << 5) | lane;
+        }
+        slen += total;
       }
       drain();
+      }
     };
-    switch (rows) {
-      case 1: run_item(RowsTag<1>{}); break;
-      case 2: run_item(RowsTag<2>{}); break;
-      case 3: run_item(RowsTag<3>{}); break;
-      case 4: run_item(RowsTag<4>{}); break;
-      case 5: run_item(RowsTag<5 <= R ? 5 : R>{}); break;
-      case 6: run_item(RowsTag<6 <= R ? 6 : R>{}); break;
-      case 7: run_item(RowsTag<7 <= R ? 7 : R>{}); break;
-      default: run_item(RowsTag<R>{}); break;
-    }
+    // one body for every row count: a single hot code path
+    run_item(RowsTag<R>{});
   }
 
   for (int d = 16; d > 0; d >>= 1) {
@@ -1500,8 +1526,7 @@ void launch_sweep2(const SweepArgs& a, bool aligned, cudaStream_t st) {
 
 size_t sweep4_smem_bytes() {
   return static_cast<size_t>(kT4Words) * 4 + kY4Cap * 4 + (static_cast<size_t>(1) << kY4HashBits) * 2 +
-         static_cast<size_t>(kSweep4Warps) * kQueueCap * sizeof(uint2) +
-         static_cast<size_t>(kSweep4Warps) * 32 * 8 * 4;
+         static_cast<size_t>(kSweep4Warps) * (32 * 8 + kA4Seg + 16 + kS4Cap) * 4;
 }
 
 void launch_sweep4(const SweepArgs& a, cudaStream_t st) {

@@ -46,6 +46,11 @@ constexpr int kSweep4Threads = 768;
 constexpr int kSweep4Warps = kSweep4Threads / 32;
 constexpr uint32_t kY4HashBits = 11;
 constexpr uint32_t kY4Cap = 1024;
+// A entries whose 32-bit windows a warp stages at once (its buffer holds 16 more:
+// the last mask of a segment reads up to 15 entries past it)
+constexpr uint32_t kA4Seg = 256;
+// table survivors a warp collects before resolving them (one per 32-bit record)
+constexpr uint32_t kS4Cap = 256;
 // B families of up to kArrange4Cap entries are laid out one bank per lane (at
 // most kArrange4ExtraRows rows beyond the minimum); larger ones stay in order.
 constexpr uint32_t kArrange4Cap = 4096;

@@ -142,7 +142,7 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
                      uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards,
                      uint64_t n_q) {
   Tuning t;
-  t.variant = variant == 0 ? 4u : variant;
+  t.variant = variant == 0 ? 3u : variant;
   const bool v2 = t.variant != 1;
   uint32_t fb_max = std::min<uint32_t>(14, fast_bits - 2);
   if (projected != 0) fb_max = std::min<uint32_t>(fb_max, projected - 6);
@@ -222,7 +222,7 @@ bool autotune_requested(uint32_t flags) { return (flags & TERGPU_ROOT_AUTOTUNE) 
 uint32_t sweep_variant(uint32_t flags) {
   if ((flags & TERGPU_ROOT_SWEEP_V1) != 0) return 1;
   if ((flags & TERGPU_ROOT_SWEEP_V2) != 0) return 2;
-  if ((flags & TERGPU_ROOT_SWEEP_V3) != 0) return 3;
+  if ((flags & TERGPU_ROOT_SWEEP_V4) != 0) return 4;
   return 0;
 }
 
@@ -356,7 +356,7 @@ Tuned autotune(Workspace& w, const JoinInput& in, uint64_t input_bytes, float* s
   Tuned best;
   float best_ms = 0;
   *spent_ms = 0;
-  for (uint32_t variant : {4u, 3u, 2u}) {
+  for (uint32_t variant : {3u, 2u}) {
     for (int dfb = -1; dfb <= 1; ++dfb) {
       for (int dfl = -1; dfl <= 1; ++dfl) {
         JoinInput j = in;

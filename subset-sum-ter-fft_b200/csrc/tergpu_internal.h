@@ -82,7 +82,7 @@ struct Tuning {
   uint32_t fb = 6, wb = 12, s_split = 1, sort_bits = 0;
   // sweep: 1 (A in registers), 2 (B in registers), 3 (v2 + bank-free probes),
   // 4 (0/1 probe table over 14-bit windows, B laid out one bank per lane)
-  uint32_t variant = 4;
+  uint32_t variant = 3;
 };
 
 // Device-resident inputs of one join: keys per list.

@@ -41,7 +41,7 @@ ABI_VERSION = 3  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
 ROOT_SWEEP_V1 = 4
 ROOT_SWEEP_V2 = 8
 ROOT_AUTOTUNE = 16
-ROOT_SWEEP_V3 = 32
+ROOT_SWEEP_V4 = 32
 MAX_QUOTIENT_BITS = 72
 # tergpu_attempt_in.root_policy: the numerics of ter::RootOutputPolicy
 ROOT_POLICY_FIRST_WITNESS = 0

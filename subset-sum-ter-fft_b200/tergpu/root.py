@@ -48,8 +48,8 @@ class Config:
     count_only: bool = False
     capacity: int = 1 << 16
     sweep_v1: bool = False  # sweep variant 1 (A in registers)
-    sweep_v2: bool = False  # sweep variant 2 (B in registers, windows sorted)
-    sweep_v3: bool = False  # sweep variant 3 (bank-free bitmap probes); default: variant 4
+    sweep_v2: bool = False  # sweep variant 2 (B in registers, windows sorted); default: variant 3
+    sweep_v4: bool = False  # sweep variant 4 (0/1 probe table, one bank per lane)
     autotune: bool = False  # pick fb / filter bits / variant per shape by timing a 1/64 sample
     shard_index: int = 0
     shard_count: int = 1  # power of two <= 64: join only D entries with key_d == index (mod count)
@@ -122,7 +122,7 @@ def run_gpu_root(keys: RootKeys, config: Config | None = None,
     rin.flags = (_abi.ROOT_COUNT_ONLY if config.count_only else 0) | \
         (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
         (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0) | \
-        (_abi.ROOT_SWEEP_V3 if config.sweep_v3 else 0) | \
+        (_abi.ROOT_SWEEP_V4 if config.sweep_v4 else 0) | \
         (_abi.ROOT_AUTOTUNE if config.autotune else 0)
     for l in range(3):
         rin.count[l] = len(lo[l])
@@ -166,7 +166,7 @@ def run_gpu_root_records(snap, config: Config | None = None,
     rin.flags = (_abi.ROOT_COUNT_ONLY if config.count_only else 0) | \
         (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
         (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0) | \
-        (_abi.ROOT_SWEEP_V3 if config.sweep_v3 else 0) | \
+        (_abi.ROOT_SWEEP_V4 if config.sweep_v4 else 0) | \
         (_abi.ROOT_AUTOTUNE if config.autotune else 0)
     rin.record_bytes = snap.record_bytes
     recs = [np.ascontiguousarray(r, dtype=np.uint8) for r in snap.records]

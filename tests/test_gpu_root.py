@@ -29,8 +29,8 @@ def keys_of(oracle_mod, bits, seed, size, pool):
 
 
 def vcfg(variant):
-    """Config keywords selecting sweep variant 1, 2, 3 or 4 (the default)."""
-    return {"sweep_v1": variant == 1, "sweep_v2": variant == 2, "sweep_v3": variant == 3}
+    """Config keywords selecting sweep variant 1, 2, 3 (the default) or 4."""
+    return {"sweep_v1": variant == 1, "sweep_v2": variant == 2, "sweep_v4": variant == 4}
 
 
 def assert_digest(got, expected):
@@ -272,7 +272,7 @@ def test_autotune_is_exact_and_cached(tg, oracle_mod, golden):
     second = tg.run_gpu_root(keys, tg.Config(autotune=True))
     for res in (first, second):
         assert_digest(workload.digest(res.triples), g["brute"])
-        assert res.telemetry.sweep_variant in (2, 3, 4)
+        assert res.telemetry.sweep_variant in (2, 3)
     assert first.telemetry.tune_ms > 0 and second.telemetry.tune_ms == 0
     assert (first.telemetry.family_bits, first.telemetry.filter_bits,
             first.telemetry.sweep_variant) == (second.telemetry.family_bits,
@@ -280,3 +280,53 @@ def test_autotune_is_exact_and_cached(tg, oracle_mod, golden):
                                                second.telemetry.sweep_variant)
     plain = tg.run_gpu_root(keys, tg.Config(sweep_v1=True))
     assert plain.telemetry.sweep_variant == 1 and plain.telemetry.tune_ms == 0
+
+
+def test_v4_large_a_families_and_ragged_rows(tg):
+    """Variant 4 with A families of several staged segments (about 940 entries
+    at 6 family bits) and B families of every row count: the same triples as
+    variant 2 on the same keys."""
+    from tergpu import workload
+
+    keys = workload.synthetic_root(sizes=(60_000, 9_000, 9_000), quotient_bits=69, seed=0xA4,
+                                   planted=24)
+    want = tg.run_gpu_root(keys, tg.Config(sweep_v2=True, family_bits=6))
+    for fb in (6, 7, 9):
+        got = tg.run_gpu_root(keys, tg.Config(family_bits=fb, sweep_v4=True))
+        assert got.telemetry.sweep_variant == 4
+        assert workload.digest(got.triples) == workload.digest(want.triples)
+        assert got.telemetry.logical_pairs == want.telemetry.logical_pairs
+
+
+def test_v4_dense_target_family(tg):
+    """Every A + B sum on one 14-bit window that a dense D family holds: every
+    probe passes the table, so a warp's survivors overflow its buffer and
+    resolve in place; one class of B entries (no balanced layout: the family
+    keeps its order) and A families of many staged segments.  The result
+    equals variant 2's, including planted exact sums."""
+    import numpy as np
+
+    import tergpu
+    from tergpu import workload
+
+    rng = np.random.default_rng(5)
+    Q, fb = 69, 6
+    low_b = (0x1357 << fb) | 5
+    mask = (1 << Q) - 1
+
+    def keys(n, low):
+        return [(int(v) << 20 | low) & mask for v in rng.integers(0, 1 << 49, n, dtype=np.uint64)]
+
+    a, b = keys(3_000, 0), keys(3_000, low_b)
+    d = keys(500, low_b) + keys(1_000, int(rng.integers(0, 1 << 20)))
+    d += [(a[int(i)] + b[int(j)]) & mask for i, j in rng.integers(0, 3_000, (10, 2))]
+    lists = [a, b, d]
+    k = tergpu.RootKeys(quotient_bits=Q,
+                        lo=[np.array([v & ((1 << 64) - 1) for v in l], dtype=np.uint64) for l in lists],
+                        hi=[np.array([v >> 64 for v in l], dtype=np.uint8) for l in lists])
+    want = tg.run_gpu_root(k, tg.Config(sweep_v2=True, family_bits=fb))
+    got = tg.run_gpu_root(k, tg.Config(family_bits=fb, sweep_v4=True))
+    assert got.telemetry.sweep_variant == 4
+    assert got.telemetry.filter_survivors >= 3_000 * 3_000
+    assert len(want.triples) >= 10
+    assert workload.digest(got.triples) == workload.digest(want.triples)
