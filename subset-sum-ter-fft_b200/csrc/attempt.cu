@@ -17,7 +17,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <functional>
+#include <thread>
 #include <vector>
 
 namespace tergpu {
@@ -171,6 +173,34 @@ void cancelled_check(const tergpu_attempt_in* in) {
   }
 }
 
+// Mirrors the caller's host cancel flag into the workspace's cancel word while
+// the call runs, so the sweep kernels (which read only device-visible memory)
+// stop within a few work items of a cancel instead of at the next stage.
+class CancelMirror {
+ public:
+  CancelMirror(const volatile int32_t* src, volatile int* dst) : src_(src), dst_(dst) {
+    if (src_ == nullptr || dst_ == nullptr) return;
+    thread_ = std::thread([this] {
+      while (!done_.load(std::memory_order_relaxed)) {
+        if (*src_ != 0) *dst_ = 1;
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+      }
+    });
+  }
+  ~CancelMirror() {
+    done_.store(true);
+    if (thread_.joinable()) thread_.join();
+  }
+  CancelMirror(const CancelMirror&) = delete;
+  CancelMirror& operator=(const CancelMirror&) = delete;
+
+ private:
+  const volatile int32_t* src_;
+  volatile int* dst_;
+  std::atomic<bool> done_{false};
+  std::thread thread_;
+};
+
 double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
 }
@@ -223,6 +253,7 @@ struct GraphPlan {
   uint64_t* rk_lo[3]{};
   uint8_t* rk_hi[3]{};
   uint8_t* aflags = nullptr;
+  const volatile int* cancel = nullptr;  // the workspace's cancel word (device view)
   GraphParams* d_params = nullptr;
   GraphParams* h_params = nullptr;  // pinned
   GraphCounts* d_counts = nullptr;
@@ -457,6 +488,7 @@ void capture_attempt(GraphPlan& g, cudaStream_t st) {
     jw.cap = g.cap_t;
     jw.main_sweep = true;
     jw.projected_bits = 0;
+    jw.cancel = g.cancel;
     enqueue_join(g.jb, jw, g.tu_l2, nullptr, st, &launches);
     launch_copy_count(&g.jb.counters[kTriples], &dc->l2_triples[grp], st);
     launch_l1_parents(g.jb.triples, Count(g.cap_t, &g.jb.counters[kTriples]), as_const(g.l2all),
@@ -497,6 +529,7 @@ void capture_attempt(GraphPlan& g, cudaStream_t st) {
   jr.cap = g.cap_r;
   jr.main_sweep = true;
   jr.projected_bits = 0;
+  jr.cancel = g.cancel;
   enqueue_join(g.jb, jr, g.tu_root, nullptr, st, &launches);
   check(cudaMemsetAsync(dc->auth, 0, sizeof dc->auth, st), "memset");
   AuthorityArgs au{};
@@ -625,6 +658,8 @@ GraphPlan* graph_plan(Workspace& w, uint32_t n, uint32_t r1, uint32_t r2, uint64
   check(cudaMallocHost(&g->h_triples, g->cap_r * 12), "cudaMallocHost");
   check(cudaMallocHost(&g->h_aflags, g->cap_r), "cudaMallocHost");
   // capture (the kernels' shared-memory limits are set before, outside the capture)
+  cancel_word(w);
+  g->cancel = w.cancel_dev;
   prepare_root_kernels();
   prepare_attempt_kernels();
   check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
@@ -780,6 +815,9 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   check(cudaSetDevice(w.device), "cudaSetDevice");
   cudaStream_t st = w.stream;
   w.alloc_stream = st;
+  cancel_word(w);
+  const CancelMirror mirror(in->cancel, w.cancel_host);
+  const volatile int* dcancel = w.cancel_dev;
 
   // ---- level 3 (once per call): both halves, lexicographic k-subsets
   std::vector<uint64_t> weights(2 * n, 0);
@@ -843,6 +881,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     bool graphed = false;
     if (plan != nullptr) {
       graphed = graph_attempt(*plan, w, tg, T, policy, &stat, &root, st);
+      cancelled_check(in);  // a cancel during the graph cut its sweeps short
       if (!graphed) {  // a capacity overflowed: this attempt runs stage by stage
         root = RootOutcome{};
         std::memset(&stat, 0, sizeof stat);
@@ -933,10 +972,13 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       j.stream = st;
       const double est = (double)j.count[0] * j.count[1] * j.count[2] / std::ldexp(1.0, qbits);
       j.capacity = (uint64_t)(est * 1.25) + 4096;
+      j.cancel = dcancel;
       JoinResult jr = run_join(w, j, 0);
+      cancelled_check(in);
       if (jr.triples > j.capacity) {
         j.capacity = jr.triples + 16;
         jr = run_join(w, j, 0);
+        cancelled_check(in);
       }
       stat.l2_modular += jr.triples;
       EntryArrays cand = entry_slot(w, S_CAND, jr.triples);
@@ -1019,10 +1061,13 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     }
     j.stream = st;
     j.capacity = 4096;
+    j.cancel = dcancel;
     JoinResult jr = run_join(w, j, 0);
+    cancelled_check(in);  // a cancel during the sweep cut it short: nothing is reported
     if (jr.triples > j.capacity) {
       j.capacity = jr.triples + 16;
       jr = run_join(w, j, 0);
+      cancelled_check(in);
     }
     stat.root_pairs = jr.pairs;
     std::vector<uint32_t> htrip;
@@ -1066,6 +1111,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
                               root.stop.b, root.stop.c};
       }
       const JoinResult pr = run_join(w, jp, 0);
+      cancelled_check(in);
       stat.root_low_prefilter = pr.projected + (root.stopped ? 1 : 0);
     }
     stat.root_ms = ms_since(t_root);

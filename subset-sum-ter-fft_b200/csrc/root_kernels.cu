@@ -250,9 +250,14 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
 
   for (;;) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    int stop = 0;
+    if (lane == 0) {
+      item = atomicAdd(&item_counter, 1u);
+      // the caller's cancel word, read every 8th work item of the CTA
+      if (a.cancel != nullptr && (item & 7u) == 0u) stop = *a.cancel;
+    }
     item = __shfl_sync(kFull, item, 0);
-    if (item >= total_items) break;
+    if (item >= total_items || __shfl_sync(kFull, stop, 0) != 0) break;
     const uint32_t s = s0 + item / qc_max;
     const uint32_t qc = item % qc_max;
     const uint32_t t = (u - s) & fmask;
@@ -430,9 +435,14 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
 
   for (;;) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    int stop = 0;
+    if (lane == 0) {
+      item = atomicAdd(&item_counter, 1u);
+      // the caller's cancel word, read every 8th work item of the CTA
+      if (a.cancel != nullptr && (item & 7u) == 0u) stop = *a.cancel;
+    }
     item = __shfl_sync(kFull, item, 0);
-    if (item >= total_items) break;
+    if (item >= total_items || __shfl_sync(kFull, stop, 0) != 0) break;
     const uint32_t s = s0 + item / xc_max;
     const uint32_t xc = item % xc_max;
     const uint32_t t = (u - s) & fmask;
@@ -646,9 +656,14 @@ __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a)
 
   for (;;) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    int stop = 0;
+    if (lane == 0) {
+      item = atomicAdd(&item_counter, 1u);
+      // the caller's cancel word, read every 8th work item of the CTA
+      if (a.cancel != nullptr && (item & 7u) == 0u) stop = *a.cancel;
+    }
     item = __shfl_sync(kFull, item, 0);
-    if (item >= total_items) break;
+    if (item >= total_items || __shfl_sync(kFull, stop, 0) != 0) break;
     const uint32_t s = s0 + item / xc_max;
     const uint32_t xc = item % xc_max;
     const uint32_t t = (u - s) & fmask;
@@ -985,9 +1000,14 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
 
   for (;;) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&item_counter, 1u);
+    int stop = 0;
+    if (lane == 0) {
+      item = atomicAdd(&item_counter, 1u);
+      // the caller's cancel word, read every 8th work item of the CTA
+      if (a.cancel != nullptr && (item & 7u) == 0u) stop = *a.cancel;
+    }
     item = __shfl_sync(kFull, item, 0);
-    if (item >= total_items) break;
+    if (item >= total_items || __shfl_sync(kFull, stop, 0) != 0) break;
     const uint32_t s = s0 + item / xc_max;
     const uint32_t xc = item % xc_max;
     const uint32_t t = (u - s) & fmask;

@@ -81,6 +81,18 @@ std::unique_ptr<Workspace> make_workspace(int device, bool blocking) {
   return w;
 }
 
+void cancel_word(Workspace& w) {
+  if (w.cancel_host == nullptr) {
+    void* h = nullptr;
+    check(cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc");
+    void* d = nullptr;
+    check(cudaHostGetDevicePointer(&d, h, 0), "cudaHostGetDevicePointer");
+    w.cancel_host = static_cast<volatile int*>(h);
+    w.cancel_dev = static_cast<const volatile int*>(d);
+  }
+  *w.cancel_host = 0;
+}
+
 void sync_stream(Workspace& w, cudaStream_t st, const char* what) {
   if (w.sync_event != nullptr) {
     check(cudaEventRecord(w.sync_event, st), what);
@@ -107,6 +119,9 @@ void destroy_workspace(Workspace& w) {
   if (w.stop) cudaEventDestroy(w.stop);
   if (w.sync_event) cudaEventDestroy(w.sync_event);
   if (w.stream) cudaStreamDestroy(w.stream);
+  if (w.cancel_host) cudaFreeHost(const_cast<int*>(w.cancel_host));
+  w.cancel_host = nullptr;
+  w.cancel_dev = nullptr;
   w.start = w.mid = w.stop = w.sync_event = nullptr;
   w.stream = nullptr;
 }
@@ -311,6 +326,7 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
   a.triples = b.triples;
   a.cap = j.cap;
   a.counters = b.counters;
+  a.cancel = j.cancel;
   if (j.main_sweep) {
     a.project = 0;
     a.mrb = F - tu.fb;
@@ -500,6 +516,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   jw.main_sweep = !in.count_only || in.projected_bits == 0;
   jw.projected_bits = in.projected_bits;
   jw.visit = in.visit;
+  jw.cancel = in.cancel;
   r.tuning.variant = enqueue_join(jb, jw, tu, w.mid, st, &r.launches);
   check(cudaGetLastError(), "sweep launch");
   check(cudaEventRecord(w.stop, st), "event");

@@ -48,7 +48,14 @@ struct Workspace {
   // calls and across release_buffers, freed by destroy_workspace
   std::map<uint32_t, std::shared_ptr<void>> plans;
   std::mutex mu;
+  // cancel word of this workspace's calls: pinned host memory the sweep reads
+  // through its device mapping (cancel_word() allocates it on first use)
+  volatile int* cancel_host = nullptr;
+  const volatile int* cancel_dev = nullptr;
 };
+
+// The workspace's cancel word (host and device views), cleared.
+void cancel_word(Workspace& w);
 
 // Waits until the work queued so far on `st` is done (see Workspace::sync_event).
 void sync_stream(Workspace& w, cudaStream_t st, const char* what);
@@ -104,6 +111,7 @@ struct JoinInput {
   uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
   cudaStream_t stream;
   VisitBound visit{};      // projected counts only before this bound (root_kernels.cuh)
+  const volatile int* cancel = nullptr;  // device view of a cancel word, or null
 };
 
 struct JoinResult {
@@ -170,6 +178,7 @@ struct JoinWork {
   bool main_sweep;       // the full-width sweep (false: projected counts only)
   uint32_t projected_bits;
   VisitBound visit{};
+  const volatile int* cancel = nullptr;
 };
 
 // The join's device work on `st` -- partition, family layout, sweep(s) -- with

@@ -204,9 +204,11 @@ def merge_digests(rows: list) -> dict:
 
 def whole_roots(tmp: Path):
     """The reference's frozen ARWLF over every cell of unplanted n=108 roots
-    (seeds WHOLE_ROOT_SEEDS_108, attempt 0) with 32-bit projected counts: each
-    root runs as WHOLE_ROOT_SLICES disjoint cell slices in parallel processes
-    (about 3 hours of one core per root), merged with merge_digests."""
+    (seeds WHOLE_ROOT_SEEDS_108, attempt 0) at its default projection (its
+    check bits give 51-bit projected counts; 32-bit counts cost about 40 s per
+    cell, so they are taken on the 16-cell samples of seed_roots): each root
+    runs as WHOLE_ROOT_SLICES disjoint cell slices in parallel processes (about
+    3 hours of one core per root), merged with merge_digests."""
     from concurrent.futures import ThreadPoolExecutor
 
     with ThreadPoolExecutor(max_workers=JOBS) as pool:
@@ -214,13 +216,14 @@ def whole_roots(tmp: Path):
         specs = [f"mod:{WHOLE_ROOT_SLICES}:{i}:4096" for i in range(WHOLE_ROOT_SLICES)]
         jobs = [(snap, spec) for snap, _ in captures for spec in specs]
         rows = list(pool.map(
-            lambda job: O.ref_run("snaproot", job[0], "arwlf", job[1], 32, timeout=8 * 3600)[0],
+            lambda job: O.ref_run("snaproot", job[0], "arwlf", job[1], 0, timeout=8 * 3600)[0],
             jobs))
     out = []
     for k, (seed, (snap, cap)) in enumerate(zip(WHOLE_ROOT_SEEDS_108, captures)):
         part = rows[k * WHOLE_ROOT_SLICES:(k + 1) * WHOLE_ROOT_SLICES]
         out.append({"seed": seed, "attempt": 0, "level1": cap["level1"],
                     "checksums": _snap_checksums(snap), "slices": WHOLE_ROOT_SLICES,
+                    "projected_bits": part[0]["projected_bits"],
                     "slice_ms": [r["ms"] for r in part], "arwlf": merge_digests(part)})
         snap.unlink()
     return out

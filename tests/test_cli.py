@@ -163,3 +163,18 @@ def test_time_limit_cancels():
             "--memory-limit-mib=65536")
     assert p.returncode == 1
     assert "Cancelled" in p.stderr
+
+
+@pytest.mark.gpu
+def test_time_limit_cancels_inside_the_n108_root():
+    """--time-limit-ms at n=108 lands inside the root sweep (one launch of about
+    7.6 s): the run ends Cancelled within about a second of the limit."""
+    import time
+
+    t0 = time.perf_counter()
+    p = run("--n=108", "--attempt-limit=1", "--warmup=0", "--repeat=1", "--time-limit-ms=2000",
+            "--memory-limit-mib=65536")
+    elapsed = time.perf_counter() - t0
+    assert p.returncode == 1
+    assert "Cancelled" in p.stderr
+    assert elapsed < 6.0, elapsed

@@ -184,3 +184,28 @@ def test_graph_attempts_equal_stage_by_stage(n, seed, first, count):
     _, staged = _attempt(n, seed, first, count, no_graph=True)
     assert batch.same_result(graphed, staged)
     assert graphed.attempts and graphed.attempts[0]["level1"] == staged.attempts[0]["level1"]
+
+
+def test_cancel_reaches_the_running_n108_sweep():
+    """A cancel raised while the n=108 root sweep runs (about 7.6 s of device
+    work) stops it within a few work items: the attempt returns Cancelled soon
+    after the flag is set, with no witness."""
+    import ctypes
+    import threading
+    import time
+
+    from tergpu import _abi, attempt, instance
+
+    inst = instance.benchmark_instance(108, 0x1001)
+    flag = ctypes.c_int32(0)
+    timer = threading.Timer(1.5, lambda: setattr(flag, "value", 1))
+    t0 = time.perf_counter()
+    timer.start()
+    res = attempt.solve_full_ter(inst, attempt.FullTerConfig(seed=0x1001, attempt_limit=1,
+                                                             memory_limit_bytes=64 << 30),
+                                 cancel=flag)
+    elapsed = time.perf_counter() - t0
+    timer.cancel()
+    assert res.status == _abi.CANCELLED
+    assert res.witness is None
+    assert elapsed < 4.0, elapsed
