@@ -96,6 +96,9 @@ def parse():
                    help="attempt budgets uniform in [1, max]: 16 for --batch, 64 for --serve")
     p.add_argument("--shard-root", action="store_true",
                    help="N>1: split one root over the ranks (strong scaling) instead of replicas")
+    p.add_argument("--n72", action="store_true",
+                   help="config 2: the n=72 whole roots (anchor, 0x7201 / 0x7203 / 0x7207 attempt 0) on "
+                        "the device against the reference's K2, K2_WIDE, ARWLF and DISPATCH on one core")
     p.add_argument("--synthetic", action="store_true",
                    help="uniform seeded keys (+8 planted triples) instead of the authentic root")
     return p.parse_args()
@@ -586,6 +589,98 @@ def run_reference(args):
     print(json.dumps(base), flush=True)
 
 
+N72_ROOTS = ((19797034556212562, 0), (0x7201, 0), (0x7203, 0), (0x7207, 0))
+
+
+def run_n72(args):
+    """Config 2: each n=72 whole root (L1 lists from the device attempt
+    pipeline, byte-identical to the reference's capture) joined on the device
+    (CUDA events, keys resident) and by the reference's frozen CPU backends on
+    one pinned core over the same root read by its load_snapshot_workload
+    (1 warm-up + 3 timed passes each, median; backends in rotated order)."""
+    import torch
+
+    import tergpu
+    from tergpu import _abi, attempt, instance, snapshot
+
+    torch.cuda.set_device(0)
+    binary, build = ref_binary()
+    lib = _abi.load()
+    backends = ["k2", "k2wide", "arwlf", "dispatch"]
+    rows = []
+    for k, (seed, att) in enumerate(N72_ROOTS):
+        inst = instance.benchmark_instance(72, seed)
+        res = attempt.solve_full_ter(inst, attempt.FullTerConfig(seed=seed, attempt_first=att,
+                                                                 attempt_limit=1, capture_only=True,
+                                                                 export_l1_capacity=200_000))
+        snap = res.snapshot
+        q, lo, hi, _ = snapshot.root_keys(snap)
+        keys = tergpu.RootKeys(quotient_bits=q, lo=lo, hi=hi)
+        d_lo = [torch.from_numpy(a.view(np.int64)).cuda() for a in keys.lo]
+        d_hi = [torch.from_numpy(h).cuda() for h in keys.hi]
+        stream = torch.cuda.current_stream()
+        rin = _abi.RootIn()
+        rin.quotient_bits = q
+        rin.flags = _abi.ROOT_DEVICE_INPUTS
+        for l in range(3):
+            rin.count[l] = len(keys.lo[l])
+            rin.key_lo[l] = ctypes.cast(d_lo[l].data_ptr(), _abi._u64p)
+            rin.key_hi[l] = ctypes.cast(d_hi[l].data_ptr(), _abi._u8p)
+        rin.device = 0
+        rin.stream = ctypes.c_void_p(stream.cuda_stream)
+        trip = np.zeros(4096 * 3, dtype=np.uint32)
+
+        def call():
+            out = _abi.RootOut()
+            out.triples = trip.ctypes.data_as(_abi._u32p)
+            out.capacity = 4096
+            st = lib.tergpu_root_run(ctypes.byref(rin), ctypes.byref(out))
+            if st != _abi.COMPLETED:
+                raise RuntimeError(f"tergpu_root_run status {st}: {_abi.last_error()}")
+            return out
+
+        for _ in range(max(3, args.warmup)):
+            call()
+        torch.cuda.synchronize()
+        steps = max(10, args.steps)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        outs = [call() for _ in range(steps)]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        pairs = int(outs[-1].logical_pairs)
+        row = {"seed": seed, "attempt": att, "level1": [len(a) for a in keys.lo], "pairs": pairs,
+               "gpu": {"ms": ms, "pairs_per_s": pairs / (ms / 1000.0),
+                       "sweep_ms": statistics.median(o.sweep_ms for o in outs),
+                       "partition_ms": statistics.median(o.partition_ms for o in outs),
+                       "family_bits": int(outs[-1].family_bits), "full_q_triples": int(outs[-1].triples_count)},
+               "cpu": {}}
+        if binary.exists():
+            with tempfile.TemporaryDirectory() as d:
+                path = Path(d) / "root.snap"
+                snapshot.save(snap, path, git_commit="reference")
+                order = backends[k % 4:] + backends[:k % 4]
+                for b in order:
+                    r = rows_of(snaptime(binary, path, b, 4096, 4, 0, 0, core=0))
+                    t = statistics.median(x["ms"] for x in r[1:])
+                    row["cpu"][b] = {"ms": t, "pairs_per_s": pairs / (t / 1000.0),
+                                     "full_q": r[-1]["full_q"], "residue": r[-1]["residue"]}
+                    if b == "dispatch":
+                        row["cpu"][b]["ran"] = r[-1].get("ran")
+            best = max(row["cpu"].items(), key=lambda kv: kv[1]["pairs_per_s"])
+            row["best_cpu"] = best[0]
+            row["gpu_vs_best_cpu_core"] = row["gpu"]["pairs_per_s"] / best[1]["pairs_per_s"]
+        rows.append(row)
+    line = {"metric": "n=72 root pairs/s", "unit": "pairs/s", "impl": "tergpu", "n_gpus": 1,
+            "value": statistics.median(r["gpu"]["pairs_per_s"] for r in rows),
+            "config": {"workload": "n=72 whole authentic roots (benchmark instance, attempt 0): "
+                                   + ", ".join(f"{s:#x}" for s, _ in N72_ROOTS),
+                       "cpu": cpu_model(), "cpu_build": build, "cpu_cores": 1},
+            "roots": rows}
+    print(json.dumps(line), flush=True)
+
+
 def solve_requests(args, serve: bool):
     """Seeded request mix of the batch (config 4) or served (config 5) workload."""
     from tergpu import attempt, batch, instance
@@ -670,6 +765,8 @@ def main():
         run_reference(args)
     elif args.batch or args.serve:
         run_batch_modes(args)
+    elif args.n72:
+        run_n72(args)
     else:
         run_tergpu(args)
 

@@ -33,7 +33,7 @@
 //   terref report SNAP POLICY
 //       report_full_ter_root (src/full_ter.cpp:3722) on the capture held by SNAP
 //       (POLICY = first | count | canon), plus count_full_ter_root (:3861).
-// BACKEND: arwlf | k2wide | k2 | hash | gpu | brute
+// BACKEND: arwlf | k2wide | k2 | dispatch | hash | gpu | brute
 
 #include "ter_a64_chqr.hpp"
 #include "ter_arwlf.hpp"
@@ -216,6 +216,15 @@ std::string run_backend(const std::string& backend, const mr8::Dataset& data, rg
     rg::run_k2(data, sink);
     *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
     o << "\"backend_status\":\"Completed\"";
+  } else if (backend == "dispatch") {
+    // the reference's probe-and-choose dispatcher (QUEUE_DENSE / ARWLF /
+    // K2_WIDE), with radix tables kept for the process as its runner keeps them
+    static rg::RadixTables tables;
+    if (tables.sources.empty()) tables.allocate();
+    const aw::Dispatch d = aw::dispatch_and_run(data, index, keys, &tables, sink);
+    *ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();
+    o << "\"backend_status\":\"Completed\",\"chosen\":\"" << aw::backend_label(d.chosen)
+      << "\",\"ran\":\"" << aw::backend_label(d.ran) << "\",\"probe_ms\":" << d.probe_ms;
   } else if (backend == "hash") {
     hj::Telemetry t;
     const hj::Status st = hj::run_hash_join(data, index, keys, hj::Config{}, sink, &t);
