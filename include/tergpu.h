@@ -263,6 +263,11 @@ typedef struct {
                                           join), every stage's output_fingerprint (the
                                           canonical lists are downloaded and hashed on the
                                           host) and out->fingerprint.  Runs stage by stage */
+#define TERGPU_ATTEMPT_BACKGROUND 16u  /* run on the workspace's lowest-priority stream, so
+                                          work of higher priority on the device (the other
+                                          slots of tergpu_attempt_batch, which sets this flag
+                                          for n >= 108) takes SMs first as this attempt's
+                                          sweep blocks finish.  Same results */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return

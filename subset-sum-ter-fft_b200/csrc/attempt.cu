@@ -813,7 +813,8 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     }
   } held{w, out};
   check(cudaSetDevice(w.device), "cudaSetDevice");
-  cudaStream_t st = w.stream;
+  cudaStream_t st = (in->flags & TERGPU_ATTEMPT_BACKGROUND) != 0 && w.stream_low != nullptr ? w.stream_low
+                                                                                             : w.stream;
   w.alloc_stream = st;
   cancel_word(w);
   const CancelMirror mirror(in->cancel, w.cancel_host);

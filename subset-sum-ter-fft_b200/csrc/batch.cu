@@ -176,6 +176,8 @@ void worker_main(Engine* e) {
     tergpu_attempt_in one = e->in->jobs[u.req];
     one.device = e->in->device;
     if (!e->graphs) one.flags |= TERGPU_ATTEMPT_NO_GRAPH;
+    // the largest attempts (n = 108: seconds of sweep) yield SMs to the others
+    if (one.n >= 108) one.flags |= TERGPU_ATTEMPT_BACKGROUND;
     one.attempt_first += u.k;
     one.attempt_count = 1;
     tergpu_attempt_out* dst = &e->in->outs[u.req];

@@ -70,7 +70,15 @@ std::unique_ptr<Workspace> make_workspace(int device, bool blocking) {
     uint64_t keep = ~0ull;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (blocking) {
+    // batch slots: small requests' work ahead of background (n >= 108) attempts
+    int least = 0, greatest = 0;
+    check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+    check(cudaStreamCreateWithPriority(&w->stream, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+    check(cudaStreamCreateWithPriority(&w->stream_low, cudaStreamNonBlocking, least), "cudaStreamCreate");
+  } else {
+    check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  }
   check(cudaEventCreate(&w->start), "cudaEventCreate");
   check(cudaEventCreate(&w->mid), "cudaEventCreate");
   check(cudaEventCreate(&w->stop), "cudaEventCreate");
@@ -119,6 +127,11 @@ void destroy_workspace(Workspace& w) {
   if (w.stop) cudaEventDestroy(w.stop);
   if (w.sync_event) cudaEventDestroy(w.sync_event);
   if (w.stream) cudaStreamDestroy(w.stream);
+  if (w.stream_low) {
+    cudaStreamSynchronize(w.stream_low);
+    cudaStreamDestroy(w.stream_low);
+  }
+  w.stream_low = nullptr;
   if (w.cancel_host) cudaFreeHost(const_cast<int*>(w.cancel_host));
   w.cancel_host = nullptr;
   w.cancel_dev = nullptr;
@@ -203,6 +216,10 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   if (n_q != 0) {
     const double pairs = static_cast<double>(n_q) * static_cast<double>(n_x) / shards;
     target_ctas = std::min<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / (1u << 20)) + 1);
+    // very large joins: blocks of about 2^29 pairs (some 25 ms), so SMs come free
+    // often for work of higher priority on the device (no measurable cost: a
+    // block's filter build is microseconds)
+    target_ctas = std::max<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / (1u << 29)));
   }
   t.s_split = static_cast<uint32_t>(std::clamp<uint64_t>((target_ctas + nloc - 1) / nloc, 1, nfam));
   // every CTA gets at least about 8 work items (A family x chunk of 256 B entries)

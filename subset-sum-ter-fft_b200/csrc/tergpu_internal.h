@@ -38,6 +38,9 @@ struct Buffer {
 struct Workspace {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // batch slots: `stream` has the device's highest priority and stream_low its
+  // lowest (TERGPU_ATTEMPT_BACKGROUND); null elsewhere
+  cudaStream_t stream_low = nullptr;
   cudaStream_t alloc_stream = nullptr;  // the stream the current call launches on
   cudaEvent_t start = nullptr, mid = nullptr, stop = nullptr;
   // batch slots wait on a blocking-sync event (the host thread sleeps instead of
