@@ -82,6 +82,8 @@ def parse():
                    help="cells per timed pass of the reference's CPU legs (per process)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-batch", action="store_true",
+                   help="leave the batch / serve sub-measurements out of the root line")
     p.add_argument("--batch", action="store_true",
                    help="batched attempts (256 instances, n from {36,48,60,72}, 1-16 attempts): "
                         "solves/s batched vs one at a time")
@@ -429,6 +431,14 @@ def run_tergpu(args):
                                                 "authentic roots only (not --synthetic)"}
         else:
             result["cpu_baseline"] = cpu_baseline(snap_obj, args)
+    # configs 4 and 5 beside the root line (N=1 only): batched and served
+    # admitted solves/s against one-at-a-time GPU solves
+    if rank == 0 and world == 1 and not args.no_batch:
+        result["batch"] = batch_measure(args, False, 256, args.rate, args.serve_n)
+        result["serve"] = batch_measure(args, True, 400, 200.0, "36,48,60,72,84,96")
+        result["serve"]["note"] = ("n = 108 requests (seconds of sweep per attempt, up to 64 "
+                                   "attempts) are measured apart: bench.py --serve "
+                                   "--serve-n 36,48,60,72,84,96,108")
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -701,61 +711,74 @@ def solve_requests(args, serve: bool):
     return reqs
 
 
-def run_batch_modes(args):
-    """--batch / --serve: the same requests one at a time (one pipeline, in
-    order) and through the continuous-batching engine; every result must be
-    bit-identical between the two; prints one JSON line."""
-    import torch
-
+def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -> dict:
+    """One batch (config 4) or served (config 5) measurement: the same seeded
+    requests one at a time (one pipeline, in order) and through the
+    continuous-batching engine; every result must be bit-identical between the
+    two.  The headline is admitted solves/s: requests the preflight refuses
+    (36 does not divide n) complete at once and are counted apart."""
     from tergpu import batch
 
-    torch.cuda.set_device(0)
-    serve = args.serve
-    reqs = solve_requests(args, serve)
+    a = argparse.Namespace(**vars(args))
+    a.requests, a.rate, a.serve_n = requests, rate, serve_n
+    reqs = solve_requests(a, serve)
     # warm both paths: module load, and every slot's workspace with its captured
     # attempt graphs (the engine keeps its slots between calls, as a server would)
     batch.solve_batch(reqs, slots=args.slots)
     one = batch.solve_batch(reqs, slots=1, served=serve)
     many = batch.solve_batch(reqs, slots=args.slots, served=serve)
-    for i, (a, b) in enumerate(zip(one.results, many.results)):
-        if not batch.same_result(a, b):
+    for i, (x, y) in enumerate(zip(one.results, many.results)):
+        if not batch.same_result(x, y):
             print(f"request {i} (n={reqs[i].instance.n}, seed={reqs[i].config.seed:#x}, "
-                  f"budget {reqs[i].config.attempt_limit}): one at a time {a.status_name} "
-                  f"{[t['level1'] for t in a.attempts][:3]}, batched {b.status_name} "
-                  f"{[t['level1'] for t in b.attempts][:3]}", file=sys.stderr)
+                  f"budget {reqs[i].config.attempt_limit}): one at a time {x.status_name}, "
+                  f"batched {y.status_name}", file=sys.stderr)
             raise RuntimeError("a request's result differs between one-at-a-time and batched runs")
     statuses = [r.status for r in many.results]
-    found = [i for i, s in enumerate(statuses) if s == 1]
-    admitted = [i for i, s in enumerate(statuses) if s in (1, 3)]
+    found = [i for i, st in enumerate(statuses) if st == 1]
+    admitted = [i for i, st in enumerate(statuses) if st in (1, 3)]
 
     def pct(v, q):
         return float(np.percentile(v, q)) if len(v) else None
 
     def summary(res):
         lat = res.latency_ms
-        return {"solves_per_s": len(reqs) / (res.total_ms / 1000.0),
-                "admitted_solves_per_s": len(admitted) / (res.total_ms / 1000.0),
+        return {"admitted_solves_per_s": len(admitted) / (res.total_ms / 1000.0),
+                "all_requests_per_s": len(reqs) / (res.total_ms / 1000.0),
                 "wall_ms": res.total_ms, "peak_running": res.peak_running,
                 "latency_p50_ms": pct(lat[admitted], 50), "latency_p99_ms": pct(lat[admitted], 99),
                 "time_to_found_p50_ms": pct(lat[found], 50),
                 "time_to_found_p99_ms": pct(lat[found], 99)}
 
     s1, sb = summary(one), summary(many)
-    attempts = sum(len(r.attempts) for r in many.results)
-    line = {
-        "metric": "served solves/s" if serve else "batched solves/s",
-        "value": sb["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
-        "n_gpus": 1, "impl": "tergpu",
-        "vs_one_at_a_time": sb["solves_per_s"] / s1["solves_per_s"],
-        "config": {"workload": ("served stream" if serve else "batched attempts"),
-                   "requests": len(reqs), "slots": args.slots, "seed": args.seed,
-                   "n": sorted({r.instance.n for r in reqs}),
+    by_n = {}
+    for r, st in zip(reqs, statuses):
+        d = by_n.setdefault(str(r.instance.n), {"requests": 0, "found": 0, "refused": 0})
+        d["requests"] += 1
+        d["found"] += st == 1
+        d["refused"] += st not in (1, 3)
+    return {
+        "metric": "served admitted solves/s" if serve else "batched admitted solves/s",
+        "value": sb["admitted_solves_per_s"], "unit": "solves/s",
+        "vs_one_at_a_time": sb["admitted_solves_per_s"] / s1["admitted_solves_per_s"],
+        "config": {"workload": "served stream (Poisson arrivals)" if serve else "batched attempts",
+                   "requests": len(reqs), "admitted": len(admitted), "refused": many.refused,
+                   "found": len(found), "slots": args.slots, "seed": args.seed,
+                   "n": sorted({r.instance.n for r in reqs}), "by_n": by_n,
                    "max_attempts": args.max_attempts or (64 if serve else 16),
-                   "arrival_rate_per_s": args.rate if serve else None,
-                   "refused": many.refused, "found": len(found), "attempts_run": attempts,
+                   "arrival_rate_per_s": rate if serve else None,
+                   "attempts_run": sum(len(r.attempts) for r in many.results),
                    "identical_results": True},
         "batched": sb, "one_at_a_time": s1,
     }
+
+
+def run_batch_modes(args):
+    """--batch / --serve: one measurement as its own JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    line = batch_measure(args, args.serve, args.requests, args.rate, args.serve_n)
+    line.update({"higher_is_better": True, "n_gpus": 1, "impl": "tergpu"})
     print(json.dumps(line), flush=True)
 
 
