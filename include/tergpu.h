@@ -322,7 +322,8 @@ typedef struct {
   uint64_t fingerprint;         /* TERGPU_ATTEMPT_TELEMETRY: FullTerTelemetry::fingerprint
                                    (src/full_ter.cpp:2532-2577) over the attempts this call ran
                                    and the witness; the reference's value when attempt_first = 0 */
-  double level3_ms;             /* wall time of the level-3 enumeration */
+  double level3_ms;             /* TERGPU_ATTEMPT_TELEMETRY: wall time of the level-3
+                                   enumeration (0 without it) */
 } tergpu_attempt_out;
 
 /* Replaces: solve_full_ter's attempt loop (src/full_ter.cpp:3125-3515) and

@@ -657,9 +657,11 @@ GraphPlan* graph_plan(Workspace& w, uint32_t n, uint32_t r1, uint32_t r2, uint64
   check(cudaMallocHost(&g->h_counts, sizeof(GraphCounts)), "cudaMallocHost");
   check(cudaMallocHost(&g->h_triples, g->cap_r * 12), "cudaMallocHost");
   check(cudaMallocHost(&g->h_aflags, g->cap_r), "cudaMallocHost");
-  // capture (the kernels' shared-memory limits are set before, outside the capture)
-  cancel_word(w);
-  g->cancel = w.cancel_dev;
+  // capture (the kernels' shared-memory limits are set before, outside the capture).
+  // The graph's sweeps take no cancel word: an attempt at these sizes lasts
+  // milliseconds, so the checks between stages suffice, and a read of host-mapped
+  // memory in every captured sweep costs the batched path several times its time
+  g->cancel = nullptr;
   prepare_root_kernels();
   prepare_attempt_kernels();
   check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
@@ -816,9 +818,13 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   cudaStream_t st = (in->flags & TERGPU_ATTEMPT_BACKGROUND) != 0 && w.stream_low != nullptr ? w.stream_low
                                                                                              : w.stream;
   w.alloc_stream = st;
-  cancel_word(w);
+  // the sweeps read the cancel word only when the caller can cancel
+  const volatile int* dcancel = nullptr;
+  if (in->cancel != nullptr) {
+    cancel_word(w);
+    dcancel = w.cancel_dev;
+  }
   const CancelMirror mirror(in->cancel, w.cancel_host);
-  const volatile int* dcancel = w.cancel_dev;
 
   // ---- level 3 (once per call): both halves, lexicographic k-subsets
   std::vector<uint64_t> weights(2 * n, 0);
@@ -864,8 +870,10 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     check(cudaGetLastError(), "level 3");
   };
   if (plan == nullptr) dynamic_level3();
-  sync_stream(w, st, "level 3");
-  out->level3_ms = ms_since(t_l3);
+  if (telemetry) {  // the level-3 time of the reference's row (one more wait)
+    sync_stream(w, st, "level 3");
+    out->level3_ms = ms_since(t_l3);
+  }
   std::vector<tergpu_attempt_stats> run;  // every attempt's stats (the run fingerprint)
 
   int status = TERGPU_ATTEMPT_LIMIT_REACHED;

@@ -96,7 +96,8 @@ struct SweepArgs {
   uint32_t two;             // 2, as an opaque operand (v4 keeps its mask shift-add an IMAD)
   const volatile int* cancel;  // device-visible word (host-mapped) or null: when it reads
                                // nonzero, warps stop taking work items (the counts are then
-                               // incomplete and the caller discards them)
+                               // incomplete and the caller discards them).  Each read crosses
+                               // PCIe: pass it only to long sweeps a caller may cancel
   uint32_t* triples;        // 3 * cap
   unsigned long long cap;
   unsigned long long* counters;  // [0] triples [1] survivors [2] fast [3] projected [4] fallback
