@@ -10,6 +10,8 @@ hand.
 """
 from __future__ import annotations
 
+import contextlib
+import fcntl
 import json
 import os
 import sys
@@ -160,24 +162,49 @@ def _capture_108(tmp: Path, seed: int) -> tuple[Path, dict]:
     return snap, cap
 
 
+@contextlib.contextmanager
+def _golden_update():
+    """Read-modify-write of the golden file under an exclusive lock: the long
+    sections write every finished item at once (several generator processes may
+    run side by side), so an interrupted run resumes where it stopped."""
+    target = HERE / "reference_golden.json"
+    with open(target, "r+") as f:
+        fcntl.flock(f, fcntl.LOCK_EX)
+        golden = json.loads(f.read())
+        yield golden
+        f.seek(0)
+        f.write(json.dumps(golden, indent=1, sort_keys=True) + "\n")
+        f.truncate()
+
+
 def seed_roots(tmp: Path):
     """Config 3's 32 n=108 roots (benchmark instance, attempt 0): per seed the
     reference's capture sizes, the three L1 list checksums of its .snap header
     and its frozen ARWLF over the declared 16-cell sample with 32-bit projected
-    counts (about 3.5 minutes of one core per seed; seeds run in parallel)."""
+    counts (about 17 minutes of one core per seed; seeds run in parallel).  Each
+    finished seed is written at once; seeds already written are skipped."""
     from concurrent.futures import ThreadPoolExecutor
+
+    order = PUBLISHED_SEEDS_108 + FRESH_SEEDS_108
+    with _golden_update() as g:
+        done = {r["seed"] for r in g.get("seed_roots", []) if "checksums" in r}
 
     def one(seed):
         snap, cap = _capture_108(tmp, seed)
         row = O.ref_run("snaproot", snap, "arwlf", 16, 32, timeout=3600)[0]
         sums = _snap_checksums(snap)
         snap.unlink()
-        return {"seed": seed, "published": seed in PUBLISHED_SEEDS_108, "level1": cap["level1"],
-                "level2": cap["level2"], "file_bytes": cap["file_bytes"], "checksums": sums,
-                "arwlf16": {k: row[k] for k in _DIGEST_KEEP}}
+        new = {"seed": seed, "published": seed in PUBLISHED_SEEDS_108, "level1": cap["level1"],
+               "level2": cap["level2"], "file_bytes": cap["file_bytes"], "checksums": sums,
+               "arwlf16": {k: row[k] for k in _DIGEST_KEEP}}
+        with _golden_update() as g:
+            rows = [r for r in g.get("seed_roots", []) if r["seed"] != seed] + [new]
+            rows.sort(key=lambda r: order.index(r["seed"]) if r["seed"] in order else len(order))
+            g["seed_roots"] = rows
+        print("seed_roots: wrote seed", hex(seed), flush=True)
 
     with ThreadPoolExecutor(max_workers=JOBS) as pool:
-        return list(pool.map(one, PUBLISHED_SEEDS_108 + FRESH_SEEDS_108))
+        list(pool.map(one, [s for s in order if s not in done]))
 
 
 def merge_digests(rows: list) -> dict:
@@ -202,31 +229,56 @@ def merge_digests(rows: list) -> dict:
     return out
 
 
+_SLICE_KEEP = ("triples", "triple_sum", "triple_xor", "triple_sum2", "full_q", "residue",
+               "residue_sum", "structural", "witnesses", "pairs", "projected_hits", "cells",
+               "projected_bits", "ms")
+
+
 def whole_roots(tmp: Path):
     """The reference's frozen ARWLF over every cell of unplanted n=108 roots
     (seeds WHOLE_ROOT_SEEDS_108, attempt 0) at its default projection (its
     check bits give 51-bit projected counts; 32-bit counts cost about 40 s per
     cell, so they are taken on the 16-cell samples of seed_roots): each root
     runs as WHOLE_ROOT_SLICES disjoint cell slices in parallel processes (about
-    3 hours of one core per root), merged with merge_digests."""
+    4 hours of one core per root), merged with merge_digests once all its slices
+    are in.  Each finished slice is written at once; slices already written are
+    skipped."""
     from concurrent.futures import ThreadPoolExecutor
 
+    with _golden_update() as g:
+        have = {e["seed"]: set(e.get("slice_rows", {})) for e in g.get("whole_roots", [])}
+    todo = {seed: [i for i in range(WHOLE_ROOT_SLICES) if str(i) not in have.get(seed, set())]
+            for seed in WHOLE_ROOT_SEEDS_108}
+    todo = {seed: slices for seed, slices in todo.items() if slices}
+    if not todo:
+        return
     with ThreadPoolExecutor(max_workers=JOBS) as pool:
-        captures = list(pool.map(lambda seed: _capture_108(tmp, seed), WHOLE_ROOT_SEEDS_108))
-        specs = [f"mod:{WHOLE_ROOT_SLICES}:{i}:4096" for i in range(WHOLE_ROOT_SLICES)]
-        jobs = [(snap, spec) for snap, _ in captures for spec in specs]
-        rows = list(pool.map(
-            lambda job: O.ref_run("snaproot", job[0], "arwlf", job[1], 0, timeout=8 * 3600)[0],
-            jobs))
-    out = []
-    for k, (seed, (snap, cap)) in enumerate(zip(WHOLE_ROOT_SEEDS_108, captures)):
-        part = rows[k * WHOLE_ROOT_SLICES:(k + 1) * WHOLE_ROOT_SLICES]
-        out.append({"seed": seed, "attempt": 0, "level1": cap["level1"],
-                    "checksums": _snap_checksums(snap), "slices": WHOLE_ROOT_SLICES,
-                    "projected_bits": part[0]["projected_bits"],
-                    "slice_ms": [r["ms"] for r in part], "arwlf": merge_digests(part)})
+        captures = dict(zip(todo, pool.map(lambda seed: _capture_108(tmp, seed), todo)))
+
+        def one(job):
+            seed, i = job
+            snap, cap = captures[seed]
+            row = O.ref_run("snaproot", snap, "arwlf", f"mod:{WHOLE_ROOT_SLICES}:{i}:4096", 0,
+                            timeout=8 * 3600)[0]
+            with _golden_update() as g:
+                entries = g.setdefault("whole_roots", [])
+                entry = next((e for e in entries if e["seed"] == seed), None)
+                if entry is None:
+                    entry = {"seed": seed, "attempt": 0, "level1": cap["level1"],
+                             "checksums": _snap_checksums(snap), "slices": WHOLE_ROOT_SLICES,
+                             "slice_rows": {}}
+                    entries.append(entry)
+                    entries.sort(key=lambda e: WHOLE_ROOT_SEEDS_108.index(e["seed"]))
+                entry["slice_rows"][str(i)] = {k: row[k] for k in _SLICE_KEEP}
+                if len(entry["slice_rows"]) == WHOLE_ROOT_SLICES:
+                    part = [entry["slice_rows"][str(k)] for k in range(WHOLE_ROOT_SLICES)]
+                    entry["projected_bits"] = part[0]["projected_bits"]
+                    entry["arwlf"] = merge_digests(part)
+            print("whole_roots: wrote seed", hex(seed), "slice", i, flush=True)
+
+        list(pool.map(one, [(seed, i) for seed, slices in todo.items() for i in slices]))
+    for snap, _ in captures.values():
         snap.unlink()
-    return out
 
 
 def attempt_telemetry(tmp: Path):
@@ -316,10 +368,11 @@ def main():
     with tempfile.TemporaryDirectory(dir=os.environ.get("TERGPU_GOLDEN_TMP")) as d:
         for name in wanted:
             section = SECTIONS[name](Path(d))
-            # re-read right before writing: another run may have written other sections
-            golden = json.loads(target.read_text()) if target.exists() else {}
-            golden[name] = section
-            target.write_text(json.dumps(golden, indent=1, sort_keys=True) + "\n")
+            if section is None:  # written item by item
+                print("complete", target, "section", name, flush=True)
+                continue
+            with _golden_update() as golden:
+                golden[name] = section
             print("wrote", target, "section", name, flush=True)
 
 
