@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import dataclasses
 import json
 import os
 import statistics
@@ -96,6 +97,9 @@ def parse():
                    help="--serve dimensions (108 makes one attempt ~9 s; add it explicitly)")
     p.add_argument("--max-attempts", type=int, default=0,
                    help="attempt budgets uniform in [1, max]: 16 for --batch, 64 for --serve")
+    p.add_argument("--max-attempts-108", type=int, default=0,
+                   help="--serve: budgets of n=108 requests uniform in [1, max] (one n=108 attempt "
+                        "holds the device for ~7.7 s; 0 = the same as --max-attempts)")
     p.add_argument("--shard-root", action="store_true",
                    help="N>1: split one root over the ranks (strong scaling) instead of replicas")
     p.add_argument("--n72", action="store_true",
@@ -447,24 +451,26 @@ def run_tergpu(args):
 
 
 def ref_binary():
-    """The reference harness for timing: the -march=native build when this host's
-    CPU has every flag of the CPU that built it, else the portable build."""
-    plain = ROOT / "oracle" / "_ref" / "terref"
-    native = ROOT / "oracle" / "_ref" / "terref_native"
-    flags = ROOT / "oracle" / "_ref" / "native_flags.txt"
-    if native.exists() and flags.exists():
-        need = set(flags.read_text().split())
-        have = set()
-        for line in Path("/proc/cpuinfo").read_text().splitlines():
-            if line.startswith("flags"):
-                have = set(line.split(":", 1)[1].split())
-                break
-        if need <= have:
-            return native, "g++ -O2 -march=native"
-        missing = " ".join(sorted(need - have)[:12])
-        return plain, (f"g++ -O2 -march=x86-64-v3 (this host lacks CPU flags of the native build: "
-                       f"{missing})")
-    return plain, "g++ -O2 -march=x86-64-v3"
+    """The reference harness for timing: the widest of its builds whose CPU flags
+    this host has -- -march=native (the CPU that built it), then x86-64-v4
+    (AVX-512), then the portable x86-64-v3."""
+    ref = ROOT / "oracle" / "_ref"
+    have = set()
+    for line in Path("/proc/cpuinfo").read_text().splitlines():
+        if line.startswith("flags"):
+            have = set(line.split(":", 1)[1].split())
+            break
+    skipped = []
+    for exe, flags, name in (("terref_native", "native_flags.txt", "native"),
+                             ("terref_v4", "v4_flags.txt", "x86-64-v4")):
+        if (ref / exe).exists() and (ref / flags).exists():
+            missing = set((ref / flags).read_text().split()) - have
+            if not missing:
+                note = f" (native build lacks: {skipped[0]})" if skipped else ""
+                return ref / exe, f"g++ -O2 -march={name}{note}"
+            skipped.append(" ".join(sorted(missing)[:8]))
+    note = f" (wider builds need CPU flags this host lacks: {'; '.join(skipped)})" if skipped else ""
+    return ref / "terref", f"g++ -O2 -march=x86-64-v3{note}"
 
 
 def cpu_model() -> str:
@@ -555,7 +561,9 @@ def run_reference(args):
         print(json.dumps(base), flush=True)
         return
     procs_n = max(1, min(os.cpu_count() or 1, 64))
-    cells = max(1, args.cpu_cells)
+    # at least 256 distinct timed cells (successive windows of a shuffled order, so
+    # every one of the 64 target families is all but certain to appear)
+    cells = max(1, args.cpu_cells, -(-256 // (procs_n * max(1, args.steps))))
     reps = max(1, args.steps + args.warmup)
     with tempfile.TemporaryDirectory() as d:
         snap = Path(d) / "root.snap"
@@ -709,15 +717,18 @@ def solve_requests(args, serve: bool):
     rng = np.random.default_rng(args.seed)
     ns = [36, 48, 60, 72] if not serve else [int(v) for v in args.serve_n.split(",")]
     max_att = args.max_attempts or (64 if serve else 16)
+    max_108 = getattr(args, "max_attempts_108", 0) or max_att
     reqs, t = [], 0.0
     for _ in range(args.requests):
         n = int(rng.choice(ns))
         seed = int(rng.integers(1, 1 << 62))
         if serve:
             t += float(rng.exponential(1000.0 / args.rate))
+        budget = int(rng.integers(1, max_att + 1))
+        if n >= 108 and max_108 < max_att:
+            budget = 1 + (budget - 1) * max_108 // max_att    # same draw, scaled to [1, max_108]
         reqs.append(batch.Request(instance.build_instance(n, seed),
-                                  attempt.FullTerConfig(seed=seed,
-                                                        attempt_limit=int(rng.integers(1, max_att + 1))),
+                                  attempt.FullTerConfig(seed=seed, attempt_limit=budget),
                                   arrival_ms=t))
     return reqs
 
@@ -734,8 +745,14 @@ def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -
     a.requests, a.rate, a.serve_n = requests, rate, serve_n
     reqs = solve_requests(a, serve)
     # warm both paths: module load, and every slot's workspace with its captured
-    # attempt graphs (the engine keeps its slots between calls, as a server would)
-    batch.solve_batch(reqs, slots=args.slots)
+    # attempt graphs (the engine keeps its slots between calls, as a server would);
+    # n=108 requests warm with one of them at one attempt (their cost is the sweep)
+    big = [r for r in reqs if r.instance.n >= 108]
+    warm = [r for r in reqs if r.instance.n < 108]
+    if big:
+        r0 = big[0]
+        warm.append(batch.Request(r0.instance, dataclasses.replace(r0.config, attempt_limit=1)))
+    batch.solve_batch(warm, slots=args.slots)
     one = batch.solve_batch(reqs, slots=1, served=serve)
     many = batch.solve_batch(reqs, slots=args.slots, served=serve)
     for i, (x, y) in enumerate(zip(one.results, many.results)):
@@ -767,6 +784,12 @@ def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -
         d["requests"] += 1
         d["found"] += st == 1
         d["refused"] += st not in (1, 3)
+    for key, d in by_n.items():
+        idx = [i for i in admitted if str(reqs[i].instance.n) == key]
+        if idx:
+            for name, res in (("batched", many), ("one_at_a_time", one)):
+                d[name] = {"latency_p50_ms": pct(res.latency_ms[idx], 50),
+                           "latency_p99_ms": pct(res.latency_ms[idx], 99)}
     return {
         "metric": "served admitted solves/s" if serve else "batched admitted solves/s",
         "value": sb["admitted_solves_per_s"], "unit": "solves/s",
@@ -776,6 +799,8 @@ def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -
                    "found": len(found), "slots": args.slots, "seed": args.seed,
                    "n": sorted({r.instance.n for r in reqs}), "by_n": by_n,
                    "max_attempts": args.max_attempts or (64 if serve else 16),
+                   "max_attempts_n108": (getattr(args, "max_attempts_108", 0) or None)
+                   if any(r.instance.n >= 108 for r in reqs) else None,
                    "arrival_rate_per_s": rate if serve else None,
                    "attempts_run": sum(len(r.attempts) for r in many.results),
                    "identical_results": True},
