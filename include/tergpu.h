@@ -267,7 +267,9 @@ typedef struct {
                                           work of higher priority on the device (the other
                                           slots of tergpu_attempt_batch, which sets this flag
                                           for n >= 108) takes SMs first as this attempt's
-                                          sweep blocks finish.  Same results */
+                                          sweep blocks finish; its joins use blocks of about
+                                          2^25 pairs (about 2 ms of one SM) instead of 2^29,
+                                          so SMs come free often.  Same results */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return

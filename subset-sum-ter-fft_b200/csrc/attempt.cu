@@ -825,6 +825,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     dcancel = w.cancel_dev;
   }
   const CancelMirror mirror(in->cancel, w.cancel_host);
+  const bool background = (in->flags & TERGPU_ATTEMPT_BACKGROUND) != 0;
 
   // ---- level 3 (once per call): both halves, lexicographic k-subsets
   std::vector<uint64_t> weights(2 * n, 0);
@@ -982,6 +983,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       const double est = (double)j.count[0] * j.count[1] * j.count[2] / std::ldexp(1.0, qbits);
       j.capacity = (uint64_t)(est * 1.25) + 4096;
       j.cancel = dcancel;
+      j.background = background;
       JoinResult jr = run_join(w, j, 0);
       cancelled_check(in);
       if (jr.triples > j.capacity) {
@@ -1071,6 +1073,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     j.stream = st;
     j.capacity = 4096;
     j.cancel = dcancel;
+    j.background = background;
     JoinResult jr = run_join(w, j, 0);
     cancelled_check(in);  // a cancel during the sweep cut it short: nothing is reported
     if (jr.triples > j.capacity) {

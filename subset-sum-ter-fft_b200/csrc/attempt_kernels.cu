@@ -10,10 +10,13 @@
 #include "attempt_kernels.cuh"
 #include "root_kernels.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 namespace tergpu {
 namespace {
+
+namespace cg = cooperative_groups;
 
 typedef unsigned __int128 u128;
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -472,7 +475,12 @@ __global__ void k_l1_parents(const uint32_t* __restrict__ triples, Count ntc, Co
     }
     const u128 s = ((((u128)x.res_hi[a] << 64) | x.res_lo[a]) + (((u128)y.res_hi[b] << 64) | y.res_lo[b]) +
                     (((u128)z.res_hi[c] << 64) | z.res_lo[c])) & nm;
-    const unsigned long long at = atomicAdd(count, 1ull);
+    // the kept parents of the warp's current step take consecutive slots with one
+    // atomic (their order is free: the canonical sort follows)
+    const cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long at = 0;
+    if (g.thread_rank() == 0) at = atomicAdd(count, static_cast<unsigned long long>(g.size()));
+    at = g.shfl(at, 0) + g.thread_rank();
     out.pos0[at] = p0;
     out.pos1[at] = p1;
     out.res_lo[at] = (uint64_t)s;

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include "root_kernels.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -20,6 +21,8 @@
 #include <utility>
 
 namespace tergpu {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -45,6 +48,17 @@ __device__ __forceinline__ bool visit_counts(const SweepArgs& a, uint32_t s, uin
   if (ia != v.a) return ia < v.a;
   if (ib != v.b) return ib < v.b;
   return ic > v.c;
+}
+
+// One output slot per calling thread: the threads of the warp that reach this
+// call together take consecutive slots with one atomic.  The L2 -> L1 joins emit
+// about 10^5 candidates (10^6 at n = 108) into one counter; one atomic per
+// candidate serialised them on that address.
+__device__ __forceinline__ unsigned long long take_triple_slot(unsigned long long* counter) {
+  const cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(counter, static_cast<unsigned long long>(g.size()));
+  return g.shfl(base, 0) + g.thread_rank();
 }
 
 template <bool ALIGNED>
@@ -303,7 +317,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_sweep(const SweepArgs a) {
                                    static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
             if (high != a.y.hi[yoff + idx]) return;
           }
-          const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+          const unsigned long long slot = take_triple_slot(&a.counters[kTriples]);
           if (slot < a.cap) {
             a.triples[3 * slot] = a.q.id[qoff + qi];
             a.triples[3 * slot + 1] = a.x.id[xoff + xi];
@@ -504,7 +518,7 @@ __global__ void __launch_bounds__(kSweepThreads, 3) k_sweep2(const SweepArgs a) 
                                        static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
                 if (high != a.y.hi[yoff + idx]) return;
               }
-              const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+              const unsigned long long slot = take_triple_slot(&a.counters[kTriples]);
               if (slot < a.cap) {
                 a.triples[3 * slot] = a.q.id[qoff + qi];
                 a.triples[3 * slot + 1] = a.x.id[xoff + xi];
@@ -727,7 +741,7 @@ __global__ void __launch_bounds__(kSweep3Threads, 1) k_sweep3(const SweepArgs a)
                                        static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
                 if (high != a.y.hi[yoff + idx]) return;
               }
-              const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+              const unsigned long long slot = take_triple_slot(&a.counters[kTriples]);
               if (slot < a.cap) {
                 a.triples[3 * slot] = a.q.id[qoff + qi];
                 a.triples[3 * slot + 1] = a.x.id[xoff + xi];
@@ -1063,7 +1077,7 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
                                    static_cast<uint32_t>(sum >> a.rb)) & hi_mask;
             if (high != a.y.hi[yoff + idx]) return;
           }
-          const unsigned long long slot = atomicAdd(&a.counters[kTriples], 1ull);
+          const unsigned long long slot = take_triple_slot(&a.counters[kTriples]);
           if (slot < a.cap) {
             a.triples[3 * slot] = a.q.id[qoff + qi];
             a.triples[3 * slot + 1] = a.x.id[xoff + xi];

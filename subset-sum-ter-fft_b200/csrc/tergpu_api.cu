@@ -168,7 +168,7 @@ uint32_t ceil_log2(uint64_t v) {
 // n=108, false-pass rate ~ 0.16 %).
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
                      uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards,
-                     uint64_t n_q) {
+                     uint64_t n_q, uint32_t block_log2) {
   Tuning t;
   t.variant = variant == 0 ? 3u : variant;
   const bool v2 = t.variant != 1;
@@ -216,10 +216,10 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   if (n_q != 0) {
     const double pairs = static_cast<double>(n_q) * static_cast<double>(n_x) / shards;
     target_ctas = std::min<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / (1u << 20)) + 1);
-    // very large joins: blocks of about 2^29 pairs (some 25 ms), so SMs come free
-    // often for work of higher priority on the device (no measurable cost: a
-    // block's filter build is microseconds)
-    target_ctas = std::max<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / (1u << 29)));
+    // very large joins: blocks of about 2^block_log2 pairs, so SMs come free
+    // often for work of higher priority on the device (a block's filter build
+    // is microseconds)
+    target_ctas = std::max<uint64_t>(target_ctas, static_cast<uint64_t>(pairs / std::ldexp(1.0, block_log2)));
   }
   t.s_split = static_cast<uint32_t>(std::clamp<uint64_t>((target_ctas + nloc - 1) / nloc, 1, nfam));
   // every CTA gets at least about 8 work items (A family x chunk of 256 B entries)
@@ -456,7 +456,8 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
   const uint32_t Q = in.quotient_bits;
   const uint32_t F = std::min<uint32_t>(Q, 64);
   r.tuning = choose_tuning(in.count[1], in.count[2], F, in.projected_bits, in.family_bits,
-                           in.filter_bits, in.sweep_variant, in.shards, in.count[0]);
+                           in.filter_bits, in.sweep_variant, in.shards, in.count[0],
+                           in.background ? kBackgroundBlockLog2 : kJoinBlockLog2);
   const Tuning& tu = r.tuning;
   checked_shards(in.shard, in.shards);
   if (tu.fb < 6 || tu.fb > 16 || tu.fb + 2 > F || tu.wb < 5 || tu.wb > 15 ||

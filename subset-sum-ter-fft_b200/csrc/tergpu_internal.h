@@ -111,6 +111,8 @@ struct JoinInput {
   bool count_only;
   uint32_t sweep_variant;  // 0: default (3), else 1, 2 or 3
   bool autotune = false;   // pick fb / filter bits / variant by timing a sample first
+  bool background = false; // CTAs of about 2^kBackgroundBlockLog2 pairs (work of higher
+                           // priority on the device gets SMs sooner)
   uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
   cudaStream_t stream;
   VisitBound visit{};      // projected counts only before this bound (root_kernels.cuh)
@@ -132,13 +134,20 @@ struct JoinResult {
 // power of two in [1, 64] and the index is below it.
 uint32_t checked_shards(uint32_t index, uint32_t count);
 
+// Pairs per sweep CTA of a very large join, as a power of two: about 25 ms of
+// one SM in the foreground, about 2 ms for background work (an n = 108 attempt
+// beside short requests: an SM comes free every ~10 us on average).
+constexpr uint32_t kJoinBlockLog2 = 29;
+constexpr uint32_t kBackgroundBlockLog2 = 25;
+
 // Family bits, filter bits, CTAs per family and variant of one join from its
 // list sizes (requested values win when not zero).  With the A list size n_q,
 // small joins get fewer CTAs (about 2^20 pairs each at least), so a join of a
-// few million pairs does not occupy every SM with CTAs that mostly build filters.
+// few million pairs does not occupy every SM with CTAs that mostly build filters,
+// and very large joins get CTAs of at most about 2^block_log2 pairs.
 Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t projected,
                      uint32_t fb_req, uint32_t filter_req, uint32_t variant, uint32_t shards,
-                     uint64_t n_q = 0);
+                     uint64_t n_q = 0, uint32_t block_log2 = kJoinBlockLog2);
 
 // Device buffers of one join, sized by the caller for the lists' count bounds:
 // per list res / hi / id (bound + 2^fb + 16 entries), cnt / off / cur
