@@ -79,6 +79,8 @@ def parse():
     p.add_argument("--sweep-v1", action="store_true", help="sweep variant 1 (A/B runs)")
     p.add_argument("--sweep-v2", action="store_true", help="sweep variant 2 (A/B runs)")
     p.add_argument("--sweep-v4", action="store_true", help="sweep variant 4 (A/B runs)")
+    p.add_argument("--partition-one-pass", action="store_true",
+                   help="one scattered pass per list instead of the staged two (A/B runs)")
     p.add_argument("--cpu-cells", type=int, default=1,
                    help="cells per timed pass of the reference's CPU legs (per process)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -243,7 +245,8 @@ def run_tergpu(args):
         rin.flags = (_abi.ROOT_DEVICE_INPUTS if resident else 0) | \
             (_abi.ROOT_SWEEP_V1 if args.sweep_v1 else 0) | \
             (_abi.ROOT_SWEEP_V2 if args.sweep_v2 else 0) | \
-            (_abi.ROOT_SWEEP_V4 if args.sweep_v4 else 0)
+            (_abi.ROOT_SWEEP_V4 if args.sweep_v4 else 0) | \
+            (_abi.ROOT_PARTITION_ONE_PASS if args.partition_one_pass else 0)
         for l in range(3):
             rin.count[l] = sizes[l]
             if resident:
@@ -374,7 +377,10 @@ def run_tergpu(args):
         sweep_bytes = sum(sizes) * 8
         sweep_kernel = {1: "k_sweep", 2: "k_sweep2", 3: "k_sweep3", 4: "k_sweep4"}.get(
             int(outs[-1].sweep_variant), "k_sweep3")
-        part_bytes = sum(sizes) * (2 * 9 + 8 + 13 + 4)  # hist read, scatter read + write
+        # algorithmic partition bytes: every entry read once (8 B key + 1 B high byte) and
+        # written once in its family (8 B residual, 1 B high byte, 4 B id), and the B list
+        # read and written once more by the lane-slot arrangement of its families
+        part_bytes = sum(sizes) * (9 + 13) + sizes[1] * 26
         int32_peak = INT32_LANES * sm_mhz * 1e6  # INT32 ops/s
         sweep_pairs_s = local_pairs / (sweep_ms / 1000.0)
         design_peak = INT32_LANES * sm_mhz * 1e6 / DESIGN_OPS_PER_PAIR
@@ -419,8 +425,12 @@ def run_tergpu(args):
                                "ops_per_pair": DESIGN_OPS_PER_PAIR, "sm_mhz": sm_mhz,
                                "note": "secondary: the probe design's instructions per pair"},
             "partition_roofline": {"bound": "hbm", "unit": "GB/s",
+                                   "kernels": "histogram, scan, scatter (staged two-pass unless "
+                                              "--partition-one-pass), family maxima, B arrangement",
                                    "achieved": part_bytes / (part_ms / 1000.0) / 1e9, "peak": hbm,
                                    "frac": part_bytes / (part_ms / 1000.0) / 1e9 / hbm,
+                                   "algorithmic_bytes": part_bytes, "partition_ms": part_ms,
+                                   "one_pass": bool(args.partition_one_pass),
                                    "peak_source": peak_src},
             "gpu_launches": launches,
             "clocks": clk,

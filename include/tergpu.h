@@ -76,6 +76,12 @@ enum tergpu_status {
                                         shared-memory probes).  Variants 3 and 4 need 32 or
                                         more residual bits, else variant 2 runs.  Same
                                         results */
+#define TERGPU_ROOT_PARTITION_ONE_PASS 64u /* lists of 2^20 or more entries go to their families
+                                        in one pass of scattered stores, as shorter lists
+                                        always do.  Default: two staged passes (high family
+                                        digit into buckets, then low digit into families),
+                                        each sorting a tile of 4,096 entries by digit in
+                                        shared memory so stores form runs.  Same results */
 
 /*
  * One L1 -> L0 root on full quotient keys.

@@ -787,7 +787,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   const double l1_est = cand_est * 0.6;
   const double rec = 16.0 * w64 + 4.0 * w32;
   double predicted = 2.0 * (2 * l3 * 32.0 + 9 * l2_est * 32 + l2_est * 120 + cand_est * (32 + 12 + 60) +
-                            3 * l1_est * (32 + rec + 40));
+                            3 * l1_est * (32 + rec + 40) + l1_est * 13);  // + the staged scatter's temp copy
   // the graph plan's fixed buffers sit beside the stage-by-stage ones (its fallback)
   if (graph_shape(n) && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) predicted += (double)plan_bytes(n, r1, r2, l3);
   out->device_bytes = (uint64_t)predicted;

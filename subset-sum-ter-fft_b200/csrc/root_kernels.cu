@@ -98,8 +98,20 @@ __global__ void __launch_bounds__(256) k_hist_priv(const uint64_t* __restrict__ 
   __syncthreads();
   uint64_t b, e;
   chunk_of(count.get(), &b, &e);
-  for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-    atomicAdd(&hbins[static_cast<uint32_t>(key[i]) & fmask], 1u);
+  // eight independent loads per thread before their counts: keeps enough
+  // bytes in flight to stream the list at HBM speed
+  constexpr int kLoads = 8;
+  for (uint64_t i0 = b + threadIdx.x; i0 < e; i0 += static_cast<uint64_t>(kLoads) * blockDim.x) {
+    uint32_t f[kLoads];
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      const uint64_t i = i0 + static_cast<uint64_t>(j) * blockDim.x;
+      f[j] = i < e ? (static_cast<uint32_t>(key[i]) & fmask) : 0xffffffffu;
+    }
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      if (f[j] != 0xffffffffu) atomicAdd(&hbins[f[j]], 1u);
+    }
   }
   __syncthreads();
   for (uint32_t f = threadIdx.x; f < nfam; f += blockDim.x) {
@@ -122,8 +134,20 @@ __global__ void __launch_bounds__(256) k_scatter_priv(
   __syncthreads();
   uint64_t b, e;
   chunk_of(count.get(), &b, &e);
-  for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-    atomicAdd(&rank[static_cast<uint32_t>(key_lo[i]) & fmask], 1u);
+  // eight entries per thread and step, loads first (many bytes in flight)
+  constexpr int kLoads = 8;
+  const uint64_t step = static_cast<uint64_t>(kLoads) * blockDim.x;
+  for (uint64_t i0 = b + threadIdx.x; i0 < e; i0 += step) {
+    uint32_t f[kLoads];
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      const uint64_t i = i0 + static_cast<uint64_t>(j) * blockDim.x;
+      f[j] = i < e ? (static_cast<uint32_t>(key_lo[i]) & fmask) : 0xffffffffu;
+    }
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      if (f[j] != 0xffffffffu) atomicAdd(&rank[f[j]], 1u);
+    }
   }
   __syncthreads();
   for (uint32_t f = threadIdx.x; f < nfam; f += blockDim.x) {
@@ -132,13 +156,31 @@ __global__ void __launch_bounds__(256) k_scatter_priv(
     rank[f] = 0u;
   }
   __syncthreads();
-  for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-    const uint64_t k = key_lo[i] & fast_mask;
-    const uint32_t f = static_cast<uint32_t>(k) & fmask;
-    const uint32_t pos = base[f] + atomicAdd(&rank[f], 1u);
-    res[pos] = k >> fb;
-    hi[pos] = key_hi != nullptr ? static_cast<uint8_t>(key_hi[i] & hi_mask) : 0;
-    out_id[pos] = id != nullptr ? id[i] : static_cast<uint32_t>(i);
+  for (uint64_t i0 = b + threadIdx.x; i0 < e; i0 += step) {
+    uint64_t k[kLoads];
+    uint32_t h[kLoads], v[kLoads];
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      const uint64_t i = i0 + static_cast<uint64_t>(j) * blockDim.x;
+      k[j] = 0;
+      h[j] = 0;
+      v[j] = 0;
+      if (i < e) {
+        k[j] = key_lo[i] & fast_mask;
+        h[j] = key_hi != nullptr ? (key_hi[i] & hi_mask) : 0u;
+        v[j] = id != nullptr ? id[i] : static_cast<uint32_t>(i);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+      if (i0 + static_cast<uint64_t>(j) * blockDim.x < e) {
+        const uint32_t f = static_cast<uint32_t>(k[j]) & fmask;
+        const uint32_t pos = base[f] + atomicAdd(&rank[f], 1u);
+        res[pos] = k[j] >> fb;
+        hi[pos] = static_cast<uint8_t>(h[j]);
+        out_id[pos] = v[j];
+      }
+    }
   }
 }
 
@@ -192,6 +234,203 @@ __global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __
     res[pos] = k >> fb;
     hi[pos] = key_hi != nullptr ? static_cast<uint8_t>(key_hi[i] & hi_mask) : 0;
     out_id[pos] = id != nullptr ? id[i] : static_cast<uint32_t>(i);
+  }
+}
+
+// ---- staged two-pass scatter ----
+//
+// A list of n entries goes to 2^fb families in two passes over digits of the
+// family f = key mod 2^fb: pass 1 by the high digit f >> lb into 2^(fb - lb)
+// buckets (a temp copy of the list; bucket h occupies [off[h << lb], +its
+// count), inside the range its families take in the output), pass 2 by the low
+// digit f mod 2^lb from each bucket into the families.  Every pass takes tiles
+// of kStageTile consecutive entries: each thread loads kStagePer of them at
+// once (the loads are independent, so many are in flight), ranks them by digit
+// with shared-memory counters, the tile reserves one output range per digit
+// with a global atomic, stages its entries in shared memory in digit order and
+// writes each digit's run to consecutive slots -- stores of consecutive threads
+// land in consecutive slots (about 64 entries per digit and tile).  Within a
+// family, entries keep no particular order (the sweep needs none).
+//
+// table (u32): [0,128) bucket cursors, [128,256) bucket starts, [256,384)
+// bucket sizes, [384,513) tile prefix over the buckets.
+
+struct StageArgs {
+  const uint64_t* key;      // pass reading the caller's lists: keys, high bytes, ids
+  const uint8_t* khi;       //   (khi, kid may be null)
+  const uint32_t* kid;
+  uint64_t n;
+  uint64_t fast_mask;
+  uint32_t hi_mask;
+  uint64_t* tkey;           // the bucketed temp copy (masked key, high byte, id)
+  uint8_t* thi;
+  uint32_t* tid;
+  uint32_t* table;
+  uint32_t nb;              // buckets
+  uint64_t* res;            // output: residual, high byte, id; family cursors
+  uint8_t* hi;
+  uint32_t* id;
+  uint32_t* cur;
+  uint32_t fb, lb;
+};
+
+constexpr uint32_t kStageBins = 128;
+constexpr uint32_t kStageTabStart = 128, kStageTabSize = 256, kStageTabTiles = 384;
+
+__global__ void k_bucket_init(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
+                              uint32_t fb, uint32_t lb, uint32_t* __restrict__ table) {
+  __shared__ uint32_t tiles[kStageBins];
+  const uint32_t nb = 1u << (fb - lb), h = threadIdx.x;
+  if (h < nb) {
+    uint32_t s = 0;
+    for (uint32_t l = 0; l < (1u << lb); ++l) s += cnt[(h << lb) + l];
+    table[h] = off[h << lb];
+    table[kStageTabStart + h] = off[h << lb];
+    table[kStageTabSize + h] = s;
+    tiles[h] = (s + kStageTile - 1) / kStageTile;
+  }
+  __syncthreads();
+  if (h == 0) {
+    uint32_t run = 0;
+    for (uint32_t i = 0; i < nb; ++i) {
+      table[kStageTabTiles + i] = run;
+      run += tiles[i];
+    }
+    table[kStageTabTiles + nb] = run;
+  }
+}
+
+// FROM_INPUT: tiles of the caller's list (else: tiles of the temp buckets).
+// TO_FINAL: digit = low family digit, into the families (else: high digit,
+// into the temp buckets).
+template <bool FROM_INPUT, bool TO_FINAL>
+__global__ void __launch_bounds__(kStageThreads, 3) k_stage_scatter(const StageArgs a) {
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  uint64_t* skey = reinterpret_cast<uint64_t*>(stage_smem);
+  uint32_t* sid = reinterpret_cast<uint32_t*>(skey + kStageTile);
+  uint8_t* shi = reinterpret_cast<uint8_t*>(sid + kStageTile);
+  __shared__ uint32_t bin_cnt[kStageBins], bin_off[kStageBins], bin_base[kStageBins];
+  const uint32_t fmask = (1u << a.fb) - 1u, lmask = (1u << a.lb) - 1u;
+  const uint32_t nbins = TO_FINAL ? (1u << a.lb) : (1u << (a.fb - a.lb));
+  const uint64_t tiles = FROM_INPUT ? (a.n + kStageTile - 1) / kStageTile : a.table[kStageTabTiles + a.nb];
+  auto digit = [&](uint64_t k) -> uint32_t {
+    const uint32_t f = static_cast<uint32_t>(k) & fmask;
+    return TO_FINAL ? (f & lmask) : (f >> a.lb);
+  };
+  for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    uint64_t b, e;
+    uint32_t bucket = 0;
+    if (FROM_INPUT) {
+      b = tile * kStageTile;
+      e = b + kStageTile < a.n ? b + kStageTile : a.n;
+    } else {
+      // the bucket whose tiles hold this one: tpre[h] <= tile < tpre[h + 1]
+      const uint32_t* tpre = a.table + kStageTabTiles;
+      uint32_t lo = 0, hi = a.nb;
+      while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tpre[mid] <= tile) {
+          lo = mid;
+        } else {
+          hi = mid;
+        }
+      }
+      bucket = lo;
+      const uint64_t start = a.table[kStageTabStart + bucket];
+      const uint64_t end = start + a.table[kStageTabSize + bucket];
+      b = start + (tile - tpre[bucket]) * kStageTile;
+      e = b + kStageTile < end ? b + kStageTile : end;
+    }
+    const uint32_t cnt = static_cast<uint32_t>(e - b);
+    for (uint32_t i = threadIdx.x; i < nbins; i += kStageThreads) bin_cnt[i] = 0u;
+    __syncthreads();
+    uint64_t k[kStagePer];
+    uint32_t idv[kStagePer], meta[kStagePer];  // meta: high byte | digit << 8 | rank << 16
+#pragma unroll
+    for (int j = 0; j < static_cast<int>(kStagePer); ++j) {
+      const uint32_t p = threadIdx.x + j * kStageThreads;
+      k[j] = 0;
+      idv[j] = 0;
+      meta[j] = 0;
+      if (p < cnt) {
+        const uint64_t i = b + p;
+        if (FROM_INPUT) {
+          k[j] = a.key[i] & a.fast_mask;
+          meta[j] = a.khi != nullptr ? (a.khi[i] & a.hi_mask) : 0u;
+          idv[j] = a.kid != nullptr ? a.kid[i] : static_cast<uint32_t>(i);
+        } else {
+          k[j] = a.tkey[i];
+          meta[j] = a.thi[i];
+          idv[j] = a.tid[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < static_cast<int>(kStagePer); ++j) {
+      const uint32_t p = threadIdx.x + j * kStageThreads;
+      if (p < cnt) {
+        const uint32_t d = digit(k[j]);
+        const uint32_t r = atomicAdd(&bin_cnt[d], 1u);
+        meta[j] |= (d << 8) | (r << 16);
+      }
+    }
+    __syncthreads();
+    // digit offsets inside the tile, and one output range per digit
+    if (threadIdx.x < 32) {
+      const uint32_t lane = threadIdx.x;
+      uint32_t c[4], s = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t bin = 4u * lane + q;
+        c[q] = bin < nbins ? bin_cnt[bin] : 0u;
+        s += c[q];
+      }
+      uint32_t incl = s;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(kFull, incl, d);
+        if (lane >= static_cast<uint32_t>(d)) incl += o;
+      }
+      uint32_t run = incl - s;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t bin = 4u * lane + q;
+        if (bin < nbins) {
+          bin_off[bin] = run;
+          if (c[q] != 0u) {
+            uint32_t* target = TO_FINAL ? &a.cur[(bucket << a.lb) + bin] : &a.table[bin];
+            bin_base[bin] = atomicAdd(target, c[q]);
+          }
+          run += c[q];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < static_cast<int>(kStagePer); ++j) {
+      const uint32_t p = threadIdx.x + j * kStageThreads;
+      if (p < cnt) {
+        const uint32_t q = bin_off[(meta[j] >> 8) & 127u] + (meta[j] >> 16);
+        skey[q] = k[j];
+        sid[q] = idv[j];
+        shi[q] = static_cast<uint8_t>(meta[j]);
+      }
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < cnt; q += kStageThreads) {
+      const uint64_t kk = skey[q];
+      const uint32_t d = digit(kk);
+      const uint32_t pos = bin_base[d] + (q - bin_off[d]);
+      if (TO_FINAL) {
+        a.res[pos] = kk >> a.fb;
+        a.hi[pos] = shi[q];
+        a.id[pos] = sid[q];
+      } else {
+        a.tkey[pos] = kk;
+        a.thi[pos] = shi[q];
+        a.tid[pos] = sid[q];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1477,6 +1716,9 @@ void prepare_root_kernels() {
   allow_max_smem(reinterpret_cast<const void*>(k_family_arrange));
   allow_max_smem(reinterpret_cast<const void*>(k_hist_priv));
   allow_max_smem(reinterpret_cast<const void*>(k_scatter_priv));
+  allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<true, true>));
+  allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<true, false>));
+  allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<false, true>));
   allow_max_smem(reinterpret_cast<const void*>(k_family_sort<true>));
   allow_max_smem(reinterpret_cast<const void*>(k_family_sort<false>));
 }
@@ -1488,11 +1730,11 @@ bool use_priv(const Count& n, uint32_t nfam) {
   return nfam <= kPrivFamilies && n.dev == nullptr && n.cap >= (1u << 20);
 }
 
-// CTAs of a privatized partition pass: chunks of at least 8,192 entries, at most
-// two CTAs per SM.
+// CTAs of a privatized partition pass: chunks of at least 16,384 entries, at
+// most four CTAs per SM.
 int priv_grid(const Count& n) {
-  const uint64_t g = (n.cap + 8191) / 8192;
-  return static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(g, 1), 148 * 2));
+  const uint64_t g = (n.cap + 16383) / 16384;
+  return static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(g, 1), 148 * 4));
 }
 
 void launch_hist(const uint64_t* key, Count n, uint32_t fmask, uint32_t* cnt, cudaStream_t st) {
@@ -1522,6 +1764,54 @@ void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_
   }
   k_scatter<<<grid_for_count(n, 256), 256, 0, st>>>(key_lo, key_hi, id, n, fb, fast_mask, hi_mask, cursor,
                                              res, hi, out_id);
+}
+
+bool staged_partition(const Count& n, uint32_t fb) {
+  return n.dev == nullptr && n.cap >= (1u << 20) && fb >= 1 && fb <= 14;
+}
+
+uint32_t staged_table_words(uint32_t) { return kStageTabTiles + kStageBins + 1; }
+
+uint32_t launch_scatter_staged(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, Count n,
+                               uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, const uint32_t* cnt,
+                               const uint32_t* off, uint32_t* cursor, const StageBuffers& tmp, uint64_t* res,
+                               uint8_t* hi, uint32_t* out_id, cudaStream_t st) {
+  if (n.cap == 0) return 0;
+  StageArgs a{};
+  a.key = key_lo;
+  a.khi = key_hi;
+  a.kid = id;
+  a.n = n.cap;
+  a.fast_mask = fast_mask;
+  a.hi_mask = hi_mask;
+  a.tkey = tmp.key;
+  a.thi = tmp.hi;
+  a.tid = tmp.id;
+  a.table = tmp.table;
+  a.res = res;
+  a.hi = hi;
+  a.id = out_id;
+  a.cur = cursor;
+  a.fb = fb;
+  const uint64_t tiles = (n.cap + kStageTile - 1) / kStageTile;
+  const size_t smem = static_cast<size_t>(kStageTile) * (8 + 4 + 1);
+  constexpr uint64_t kResident = 148 * 3;
+  if (fb <= 7) {  // one pass: every family is a digit
+    a.lb = fb;
+    a.nb = 1;
+    allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<true, true>));
+    k_stage_scatter<true, true><<<static_cast<int>(std::min(tiles, kResident)), kStageThreads, smem, st>>>(a);
+    return 1;
+  }
+  a.lb = fb / 2;
+  a.nb = 1u << (fb - a.lb);
+  k_bucket_init<<<1, kStageBins, 0, st>>>(cnt, off, fb, a.lb, tmp.table);
+  allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<true, false>));
+  allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<false, true>));
+  k_stage_scatter<true, false><<<static_cast<int>(std::min(tiles, kResident)), kStageThreads, smem, st>>>(a);
+  k_stage_scatter<false, true>
+      <<<static_cast<int>(std::min(tiles + a.nb, kResident)), kStageThreads, smem, st>>>(a);
+  return 3;
 }
 
 void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters, int slot,

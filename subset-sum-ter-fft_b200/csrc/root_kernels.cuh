@@ -126,6 +126,31 @@ void launch_scatter(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_
                     uint64_t* res, uint8_t* hi, uint32_t* out_id, cudaStream_t st);
 void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters, int slot,
                        cudaStream_t st);
+
+// Staged two-pass scatter for long lists with a host count (staged_partition):
+// pass 1 moves every entry into the bucket of its high family digit (a temp
+// copy of the list), pass 2 moves it from there into its family; each pass
+// sorts a tile of kStageTile entries by digit in shared memory first, so every
+// store is part of a run of consecutive entries.  The temp arrays hold
+// count + 2^fb + 16 slots like the output arrays; the table holds
+// staged_table_words(fb) words.
+constexpr uint32_t kStageThreads = 256;
+constexpr uint32_t kStagePer = 16;
+constexpr uint32_t kStageTile = kStageThreads * kStagePer;
+struct StageBuffers {
+  uint64_t* key = nullptr;
+  uint8_t* hi = nullptr;
+  uint32_t* id = nullptr;
+  uint32_t* table = nullptr;
+};
+bool staged_partition(const Count& n, uint32_t fb);
+uint32_t staged_table_words(uint32_t fb);
+// The scatter of launch_scatter through the two staged passes (cursor and off
+// as the scan left them).  Returns the kernels launched.
+uint32_t launch_scatter_staged(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, Count n,
+                               uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, const uint32_t* cnt,
+                               const uint32_t* off, uint32_t* cursor, const StageBuffers& tmp, uint64_t* res,
+                               uint8_t* hi, uint32_t* out_id, cudaStream_t st);
 size_t sweep_smem_bytes(uint32_t wb);
 // v1: A windows in registers, B broadcast (any family order).
 void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st);

@@ -32,7 +32,7 @@ enum Slot {
   kSlotCnt = 18, kSlotOff = 21, kSlotCur = 24, kSlotCells = 27, kSlotTriples = 28,
   kSlotCounters = 29, kSlotRecords = 30, kSlotFlags = 33, kSlotQWin = 34, kSlotRes4 = 35,
   kSlotHi4 = 36, kSlotId4 = 37, kSlotWin4 = 38, kSlotCnt4 = 39, kSlotOff4 = 40, kSlotCur4 = 41,
-  kSlots = 42
+  kSlotStageKey = 42, kSlotStageHi = 43, kSlotStageId = 44, kSlotStageTab = 45, kSlots = 46
 };
 
 std::mutex g_mu;
@@ -233,7 +233,16 @@ Tuning choose_tuning(uint64_t n_x, uint64_t n_d, uint32_t fast_bits, uint32_t pr
   return t;
 }
 
-uint64_t partition_bytes(const uint64_t count[3], uint32_t fb, uint32_t variant) {
+// Slots of the staged scatter's temp copy: the longest list that takes it (0: none).
+uint64_t staged_slots(const uint64_t count[3], uint32_t fb) {
+  uint64_t m = 0;
+  for (int l = 0; l < 3; ++l) {
+    if (staged_partition(Count(count[l]), fb)) m = std::max<uint64_t>(m, count[l] + (1ull << fb) + 16);
+  }
+  return m;
+}
+
+uint64_t partition_bytes(const uint64_t count[3], uint32_t fb, uint32_t variant, bool one_pass) {
   uint64_t b = 0;
   for (int l = 0; l < 3; ++l) {
     const uint64_t slots = count[l] + (1ull << fb) + 16;
@@ -245,6 +254,8 @@ uint64_t partition_bytes(const uint64_t count[3], uint32_t fb, uint32_t variant)
     b += v4_slots(count[1], fb) * (8 + 1 + 4 + 4);
     b += 3ull * ((1ull << fb) + 1) * 4;
   }
+  const uint64_t staged = one_pass ? 0 : staged_slots(count, fb);
+  if (staged != 0) b += staged * (8 + 1 + 4) + staged_table_words(fb) * 4ull;
   return b;
 }
 
@@ -280,10 +291,18 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
     check(cudaMemsetAsync(b.cnt[l], 0, nfam * 4ull, st), "memset");
     launch_hist(j.key_lo[l], j.count[l], nfam - 1, b.cnt[l], st);
     launch_scan(b.cnt[l], nfam, b.off[l], b.cur[l], st);
-    launch_scatter(j.key_lo[l], j.key_hi[l], j.id[l], j.count[l], tu.fb, fast_mask,
-                   hi_bits ? ((1u << hi_bits) - 1u) : 0u, b.cur[l], b.res[l], b.hi[l], b.id[l], st);
+    const uint32_t hi_mask = hi_bits ? ((1u << hi_bits) - 1u) : 0u;
+    if (b.stage.key != nullptr && staged_partition(j.count[l], tu.fb)) {
+      *launches += launch_scatter_staged(j.key_lo[l], j.key_hi[l], j.id[l], j.count[l], tu.fb, fast_mask,
+                                         hi_mask, b.cnt[l], b.off[l], b.cur[l], b.stage, b.res[l], b.hi[l],
+                                         b.id[l], st);
+    } else {
+      launch_scatter(j.key_lo[l], j.key_hi[l], j.id[l], j.count[l], tu.fb, fast_mask, hi_mask, b.cur[l],
+                     b.res[l], b.hi[l], b.id[l], st);
+      *launches += j.count[l].cap != 0 ? 1 : 0;
+    }
     views[l] = ListView{b.res[l], b.hi[l], b.id[l], b.off[l], b.cnt[l]};
-    *launches += (j.count[l].cap != 0 ? 2 : 0) + 1;
+    *launches += (j.count[l].cap != 0 ? 1 : 0) + 1;
   }
   launch_max_family(b.cnt[0], nfam, b.counters, kMaxQ, st);
   launch_max_family(b.cnt[1], nfam, b.counters, kMaxX, st);
@@ -466,7 +485,7 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     throw Failure{TERGPU_INVALID_INPUT};
   }
   const uint32_t nfam = 1u << tu.fb;
-  const uint64_t need = input_bytes + partition_bytes(in.count, tu.fb, tu.variant) +
+  const uint64_t need = input_bytes + partition_bytes(in.count, tu.fb, tu.variant, in.one_pass) +
                         (in.count_only ? 0 : in.capacity * 12) + 4096 + 64;
   r.device_bytes = need;
   if (in.memory_limit_bytes != 0 && need > in.memory_limit_bytes) {
@@ -501,6 +520,13 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     jb.cnt4 = ensure<uint32_t>(w, kSlotCnt4, (nfam + 1) * 4ull);
     jb.off4 = ensure<uint32_t>(w, kSlotOff4, (nfam + 1) * 4ull);
     jb.cur4 = ensure<uint32_t>(w, kSlotCur4, (nfam + 1) * 4ull);
+  }
+  const uint64_t staged = in.one_pass ? 0 : staged_slots(in.count, tu.fb);
+  if (staged != 0) {
+    jb.stage.key = ensure<uint64_t>(w, kSlotStageKey, staged * 8);
+    jb.stage.hi = ensure<uint8_t>(w, kSlotStageHi, staged);
+    jb.stage.id = ensure<uint32_t>(w, kSlotStageId, staged * 4);
+    jb.stage.table = ensure<uint32_t>(w, kSlotStageTab, staged_table_words(tu.fb) * 4ull);
   }
   const uint8_t* d_cells = in.cells_device;
   if (d_cells == nullptr && in.cells != nullptr) {
@@ -698,6 +724,7 @@ int root_run_body(const void* vin, void* vout) {
   j.count_only = count_only;
   j.sweep_variant = sweep_variant(in->flags);
   j.autotune = autotune_requested(in->flags) && j.sweep_variant == 0;
+  j.one_pass = (in->flags & TERGPU_ROOT_PARTITION_ONE_PASS) != 0;
   j.shard = in->shard_index;
   j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);
@@ -830,6 +857,7 @@ int root_records_body(const void* vin, void* vout) {
   j.count_only = count_only;
   j.sweep_variant = sweep_variant(in->flags);
   j.autotune = autotune_requested(in->flags) && j.sweep_variant == 0;
+  j.one_pass = (in->flags & TERGPU_ROOT_PARTITION_ONE_PASS) != 0;
   j.shard = in->shard_index;
   j.shards = checked_shards(in->shard_index, in->shard_count);
   const JoinResult res = run_join(w, j, input_bytes);

@@ -111,6 +111,7 @@ struct JoinInput {
   bool count_only;
   uint32_t sweep_variant;  // 0: default (3), else 1, 2 or 3
   bool autotune = false;   // pick fb / filter bits / variant by timing a sample first
+  bool one_pass = false;   // no staged two-pass scatter for long lists
   bool background = false; // CTAs of about 2^kBackgroundBlockLog2 pairs (work of higher
                            // priority on the device gets SMs sooner)
   uint32_t shard = 0, shards = 1;  // join only target families u == shard (mod shards)
@@ -168,6 +169,9 @@ struct JoinBuffers {
   uint32_t* id4 = nullptr;
   uint32_t* win4 = nullptr;
   uint32_t *cnt4 = nullptr, *off4 = nullptr, *cur4 = nullptr;
+  // temp copy for the staged two-pass scatter (null: every list takes the
+  // one-pass scatter); sized for the longest staged list
+  StageBuffers stage{};
 };
 
 // Lane slots the v4 layout of a B list of `count` entries in 2^fb families can

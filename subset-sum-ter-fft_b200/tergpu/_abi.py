@@ -42,6 +42,7 @@ ROOT_SWEEP_V1 = 4
 ROOT_SWEEP_V2 = 8
 ROOT_AUTOTUNE = 16
 ROOT_SWEEP_V4 = 32
+ROOT_PARTITION_ONE_PASS = 64
 MAX_QUOTIENT_BITS = 72
 # tergpu_attempt_in.root_policy: the numerics of ter::RootOutputPolicy
 ROOT_POLICY_FIRST_WITNESS = 0

@@ -51,6 +51,7 @@ class Config:
     sweep_v2: bool = False  # sweep variant 2 (B in registers, windows sorted); default: variant 3
     sweep_v4: bool = False  # sweep variant 4 (0/1 probe table, one bank per lane)
     autotune: bool = False  # pick fb / filter bits / variant per shape by timing a 1/64 sample
+    one_pass_partition: bool = False  # long lists: one scattered pass instead of two staged ones
     shard_index: int = 0
     shard_count: int = 1  # power of two <= 64: join only D entries with key_d == index (mod count)
 
@@ -123,7 +124,8 @@ def run_gpu_root(keys: RootKeys, config: Config | None = None,
         (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
         (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0) | \
         (_abi.ROOT_SWEEP_V4 if config.sweep_v4 else 0) | \
-        (_abi.ROOT_AUTOTUNE if config.autotune else 0)
+        (_abi.ROOT_AUTOTUNE if config.autotune else 0) | \
+        (_abi.ROOT_PARTITION_ONE_PASS if config.one_pass_partition else 0)
     for l in range(3):
         rin.count[l] = len(lo[l])
         rin.key_lo[l] = _p(lo[l], ctypes.c_uint64)
@@ -167,7 +169,8 @@ def run_gpu_root_records(snap, config: Config | None = None,
         (_abi.ROOT_SWEEP_V1 if config.sweep_v1 else 0) | \
         (_abi.ROOT_SWEEP_V2 if config.sweep_v2 else 0) | \
         (_abi.ROOT_SWEEP_V4 if config.sweep_v4 else 0) | \
-        (_abi.ROOT_AUTOTUNE if config.autotune else 0)
+        (_abi.ROOT_AUTOTUNE if config.autotune else 0) | \
+        (_abi.ROOT_PARTITION_ONE_PASS if config.one_pass_partition else 0)
     rin.record_bytes = snap.record_bytes
     recs = [np.ascontiguousarray(r, dtype=np.uint8) for r in snap.records]
     targets = [np.ascontiguousarray(t, dtype=np.uint32) for t in snap.child_targets]
