@@ -332,15 +332,18 @@ def test_v4_dense_target_family(tg):
     assert workload.digest(got.triples) == workload.digest(want.triples)
 
 
-@pytest.mark.parametrize("fb", [6, 7, 8, 11, 12, 13, 14])
+@pytest.mark.parametrize("fb", [6, 7, 8, 9, 10, 12, 14])
 def test_staged_partition_equals_one_pass(tg, fb):
     """Lists of 2^20 or more entries go to their families through the staged
     two-pass scatter (one staged pass at 7 family bits or fewer); on the same
-    keys every count and the triple multiset equal the one-pass scatter's (the
-    shorter B list takes the one-pass path either way)."""
+    keys every count and the triple multiset equal the one-pass scatter's.  A
+    (1.1 M entries) is always staged; D holds about 1,500 entries per family
+    (the sweep's exact lookup takes 2,048), so it is staged from 10 family bits
+    on; B stays short."""
     from tergpu import workload
 
-    keys = workload.synthetic_root(sizes=(1_100_000, 300_000, 1_200_000), quotient_bits=69,
+    n_d = min(1_200_000, 1500 << fb)
+    keys = workload.synthetic_root(sizes=(1_100_000, 40_000, n_d), quotient_bits=69,
                                    seed=0x5EED + fb, planted=40)
     cfg = dict(family_bits=fb, projected_bits=fb + 20)
     staged = tg.run_gpu_root(keys, tg.Config(**cfg))
@@ -349,8 +352,9 @@ def test_staged_partition_equals_one_pass(tg, fb):
     assert workload.digest(staged.triples) == workload.digest(plain.triples)
     for k in ("logical_pairs", "filter_survivors", "fast_hits", "full_hits", "projected_hits"):
         assert getattr(staged.telemetry, k) == getattr(plain.telemetry, k), k
-    if fb >= 8:  # bucket table + two passes instead of one, for A and D
-        assert staged.telemetry.kernel_launches == plain.telemetry.kernel_launches + 4
+    if fb >= 8:  # a bucket table and two passes instead of one, per staged list
+        extra = 2 * sum(1 for n in (1_100_000, 40_000, n_d) if n >= 1 << 20)
+        assert staged.telemetry.kernel_launches == plain.telemetry.kernel_launches + extra
 
 
 def test_staged_partition_with_empty_buckets_and_no_high_byte(tg):
@@ -361,14 +365,14 @@ def test_staged_partition_with_empty_buckets_and_no_high_byte(tg):
     import tergpu
     from tergpu import workload
 
-    keys = workload.synthetic_root(sizes=(1_300_000, 200_000, 1_100_000), quotient_bits=47,
-                                   seed=0xE3, planted=16)
     rng = np.random.default_rng(3)
-    low = np.array([0, 5, 4077], dtype=np.uint64)[rng.integers(0, 3, len(keys.lo[0]))]
-    lo_a = (keys.lo[0] & ~np.uint64(0xFFF)) | low
-    skew = tergpu.RootKeys(quotient_bits=47, lo=[lo_a, keys.lo[1], keys.lo[2]], hi=keys.hi)
     for fb in (7, 12):
-        cfg = dict(family_bits=fb, projected_bits=fb + 14)
+        keys = workload.synthetic_root(sizes=(1_300_000, 30_000, 1200 << fb if fb < 10 else 1_100_000),
+                                       quotient_bits=47, seed=0xE3 + fb, planted=16)
+        low = np.array([0, 5, 4077], dtype=np.uint64)[rng.integers(0, 3, len(keys.lo[0]))]
+        lo_a = (keys.lo[0] & ~np.uint64(0xFFF)) | low
+        skew = tergpu.RootKeys(quotient_bits=47, lo=[lo_a, keys.lo[1], keys.lo[2]], hi=keys.hi)
+        cfg = dict(family_bits=fb, projected_bits=fb + 18)
         staged = tg.run_gpu_root(skew, tg.Config(**cfg))
         plain = tg.run_gpu_root(skew, tg.Config(one_pass_partition=True, **cfg))
         assert staged.telemetry.projected_hits > 0
