@@ -252,8 +252,9 @@ __global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __
 // land in consecutive slots (about 64 entries per digit and tile).  Within a
 // family, entries keep no particular order (the sweep needs none).
 //
-// table (u32): [0,128) bucket cursors, [128,256) bucket starts, [256,384)
-// bucket sizes, [384,513) tile prefix over the buckets.
+// table (u32): bucket cursors at [32 h] (one 128-byte line each, so the tiles'
+// reservations spread over L2 slices instead of queueing on one), then bucket
+// starts, bucket sizes and the tile prefix over the buckets.
 
 struct StageArgs {
   const uint64_t* key;      // pass reading the caller's lists: keys, high bytes, ids
@@ -275,7 +276,9 @@ struct StageArgs {
 };
 
 constexpr uint32_t kStageBins = 128;
-constexpr uint32_t kStageTabStart = 128, kStageTabSize = 256, kStageTabTiles = 384;
+constexpr uint32_t kStageCurStride = 32;
+constexpr uint32_t kStageTabStart = kStageBins * kStageCurStride, kStageTabSize = kStageTabStart + kStageBins,
+                   kStageTabTiles = kStageTabSize + kStageBins;
 
 __global__ void k_bucket_init(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
                               uint32_t fb, uint32_t lb, uint32_t* __restrict__ table) {
@@ -284,7 +287,7 @@ __global__ void k_bucket_init(const uint32_t* __restrict__ cnt, const uint32_t* 
   if (h < nb) {
     uint32_t s = 0;
     for (uint32_t l = 0; l < (1u << lb); ++l) s += cnt[(h << lb) + l];
-    table[h] = off[h << lb];
+    table[h * kStageCurStride] = off[h << lb];
     table[kStageTabStart + h] = off[h << lb];
     table[kStageTabSize + h] = s;
     tiles[h] = (s + kStageTile - 1) / kStageTile;
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(kStageThreads, 3) k_stage_scatter(const StageA
         if (bin < nbins) {
           bin_off[bin] = run;
           if (c[q] != 0u) {
-            uint32_t* target = TO_FINAL ? &a.cur[(bucket << a.lb) + bin] : &a.table[bin];
+            uint32_t* target = TO_FINAL ? &a.cur[(bucket << a.lb) + bin] : &a.table[bin * kStageCurStride];
             bin_base[bin] = atomicAdd(target, c[q]);
           }
           run += c[q];
