@@ -59,17 +59,46 @@ Workspace& workspace(int device) {
   return *g_ws.back();
 }
 
+std::mutex g_pool_mu;
+std::map<int, cudaMemPool_t> g_pools;
+
+// The library's stream-ordered memory pool of `device`, created on first use.
+// It keeps freed memory instead of returning it at every synchronization
+// (workspaces grow and shrink across calls), and it never reuses a block whose
+// free is still pending on another stream by making the allocating stream wait
+// for that stream: with the default pool's internal dependencies, a short
+// request's allocation could wait for a whole n = 108 sweep launched on another
+// slot's stream.  Such a block stays unused until its free has completed.
+cudaMemPool_t library_pool(int device) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  auto it = g_pools.find(device);
+  if (it != g_pools.end()) return it->second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+  uint64_t keep = ~0ull;
+  check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+  int off = 0;
+  check(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &off),
+        "cudaMemPoolSetAttribute");
+  g_pools[device] = pool;
+  return pool;
+}
+
+void trim_library_pools() {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  for (auto& kv : g_pools) cudaMemPoolTrimTo(kv.second, 0);
+}
+
 std::unique_ptr<Workspace> make_workspace(int device, bool blocking) {
   auto w = std::make_unique<Workspace>();
   w->device = device;
   check(cudaSetDevice(device), "cudaSetDevice");
-  // keep freed stream-ordered memory in the device pool instead of returning it
-  // at every synchronization (workspaces grow and shrink across calls)
-  cudaMemPool_t pool = nullptr;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-    uint64_t keep = ~0ull;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
+  w->pool = library_pool(device);
   if (blocking) {
     // batch slots: small requests' work ahead of background (n >= 108) attempts
     int least = 0, greatest = 0;
@@ -147,7 +176,7 @@ void* ensure_bytes(Workspace& w, int slot, size_t bytes) {
     if (b.ptr != nullptr) check(cudaFreeAsync(b.ptr, s), "cudaFreeAsync");
     b.ptr = nullptr;
     b.bytes = 0;
-    check(cudaMallocAsync(&b.ptr, bytes, s), "cudaMallocAsync");
+    check(cudaMallocFromPoolAsync(&b.ptr, bytes, w.pool, s), "cudaMallocFromPoolAsync");
     b.bytes = bytes;
   }
   return b.ptr;
@@ -940,10 +969,9 @@ void tergpu_release(void) {
   for (auto& w : tergpu::g_ws) {
     std::lock_guard<std::mutex> inner(w->mu);
     tergpu::destroy_workspace(*w);
-    cudaMemPool_t pool = nullptr;
-    if (cudaDeviceGetDefaultMemPool(&pool, w->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   }
   tergpu::g_ws.clear();
+  tergpu::trim_library_pools();
 }
 
 const char* tergpu_last_error(void) { return tergpu::t_error.c_str(); }

@@ -32,8 +32,9 @@ struct Buffer {
 };
 
 // Device buffers, a stream and timing events for one call at a time.  Buffers
-// are stream-ordered allocations (cudaMallocAsync / cudaFreeAsync on
-// alloc_stream, or on `stream` when that is null), so growing one workspace
+// are stream-ordered allocations from the library's own pool of the device
+// (library_pool: no reuse that would make one stream wait for another's work),
+// on alloc_stream, or on `stream` when that is null, so growing one workspace
 // never waits for work that other workspaces have in flight on the device.
 struct Workspace {
   int device = 0;
@@ -54,6 +55,7 @@ struct Workspace {
   // cancel word of this workspace's calls: pinned host memory the sweep reads
   // through its device mapping (cancel_word() allocates it on first use)
   volatile int* cancel_host = nullptr;
+  cudaMemPool_t pool = nullptr;  // library_pool(device)
   const volatile int* cancel_dev = nullptr;
 };
 
