@@ -798,8 +798,11 @@ def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -
         idx = [i for i in admitted if str(reqs[i].instance.n) == key]
         if idx:
             for name, res in (("batched", many), ("one_at_a_time", one)):
+                wait = res.admit_ms[idx] - res.arrival_ms[idx]
+                service = res.finish_ms[idx] - res.admit_ms[idx]
                 d[name] = {"latency_p50_ms": pct(res.latency_ms[idx], 50),
-                           "latency_p99_ms": pct(res.latency_ms[idx], 99)}
+                           "latency_p99_ms": pct(res.latency_ms[idx], 99),
+                           "admit_wait_p50_ms": pct(wait, 50), "service_p50_ms": pct(service, 50)}
     return {
         "metric": "served admitted solves/s" if serve else "batched admitted solves/s",
         "value": sb["admitted_solves_per_s"], "unit": "solves/s",
