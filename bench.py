@@ -44,6 +44,10 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "subset-sum-ter-fft_b200"))
+# 32 hardware work queues for this process's CUDA context (the batch / serve
+# measurements run 32 streams; with CUDA's default of 8 a short request's kernel
+# waits behind a long sweep queued on another stream); before any CUDA call
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "n=108 root pairs/s"
 UNIT = "pairs/s"

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -57,6 +58,16 @@ Workspace& workspace(int device) {
   }
   g_ws.push_back(make_workspace(device));
   return *g_ws.back();
+}
+
+// Loading the library asks the CUDA context this process will create for 32
+// hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS; CUDA's default is 8 and it
+// maps streams onto them in order): the batch engine runs two streams per slot,
+// and with fewer queues than streams a short request's kernel waits behind an
+// n = 108 sweep queued earlier on another slot's stream.  A value the caller set
+// is kept; a context created before the library is loaded keeps its own count.
+__attribute__((constructor)) void ask_for_work_queues() {
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
 }
 
 std::mutex g_pool_mu;
