@@ -575,9 +575,10 @@ def run_reference(args):
         print(json.dumps(base), flush=True)
         return
     procs_n = max(1, min(os.cpu_count() or 1, 64))
-    # at least 256 distinct timed cells (successive windows of a shuffled order, so
-    # every one of the 64 target families is all but certain to appear)
-    cells = max(1, args.cpu_cells, -(-256 // (procs_n * max(1, args.steps))))
+    # at least 512 distinct timed cells (successive windows of a shuffled order:
+    # 63.99 of the 64 target families appear on average; 256 cells left 61 of 64
+    # in one run)
+    cells = max(1, args.cpu_cells, -(-512 // (procs_n * max(1, args.steps))))
     reps = max(1, args.steps + args.warmup)
     with tempfile.TemporaryDirectory() as d:
         snap = Path(d) / "root.snap"
