@@ -1,37 +1,57 @@
-"""n=108 roots of the six published seeds against the reference.
+"""Config 3: n=108 roots of 32 seeds against the reference.
 
-For every seed the device attempt pipeline makes the authentic attempt-0 L1
-lists of the benchmark instance and the device runs the records root (keys
-derived on the device, join, authority) over the reference's declared 16-cell
-sample; the reference's own capture and frozen ARWLF on the same sample
-(golden seed_roots, printed by the reference harness) must agree on the level
-sizes, the full-Q triple multiset (count and the three sink hashes), the
-residue-exact and structural counts, the witnesses, the logical pairs and the
-32-bit projected hits (about 1.6e8 per seed: the strong check, since the full-Q
-outputs of a 16-cell sample are almost always empty).
+For every seed (the six published ones and 26 fresh ones) the device attempt
+pipeline makes the authentic attempt-0 L1 lists of the benchmark instance.
+The reference's own capture of the same attempt (golden seed_roots, printed by
+the reference harness) fixes:
+
+* the level sizes and the three per-list FNV-1a-64 checksums of its .snap
+  header (ter2_root/frozen/ter_root_snapshot.cpp:94-101) -- the device lists
+  must be byte-identical record for record, not only equal in size;
+* frozen ARWLF over the reference's declared 16-cell sample: the full-Q triple
+  multiset (count and the three sink hashes), residue-exact count, witnesses,
+  logical pairs and 32-bit projected hits (about 1.6e8 per seed: the strong
+  check, since the full-Q outputs of a 16-cell sample are almost always empty).
+
+For two unplanted seeds (golden whole_roots) frozen ARWLF ran over all 4,096
+cells (2.5e13 pairs per root, merged from cell slices): the device's whole
+root must give the same triple multiset, residue counts, witnesses and
+projected count at ARWLF's own check width.
 """
+import json
+
 import pytest
 
-from conftest import hexint
+from conftest import GOLDEN_DIR, hexint
 
 pytestmark = pytest.mark.gpu
 
 CELLS = 16
+_G = json.loads((GOLDEN_DIR / "reference_golden.json").read_text())
+SEEDS = [g["seed"] for g in _G["seed_roots"]]
+WHOLE = [g["seed"] for g in _G.get("whole_roots", []) if "arwlf" in g]
 
 
-@pytest.mark.parametrize("index", range(6))
-def test_seed_root_sample_matches_reference_arwlf(oracle_mod, golden, index):
-    import tergpu
-    from tergpu import attempt, instance, workload
+def _device_capture(seed):
+    from tergpu import attempt, instance
 
-    g = golden["seed_roots"][index]
-    seed = g["seed"]
     inst = instance.benchmark_instance(108, seed)
-    res = attempt.solve_full_ter(inst, attempt.FullTerConfig(seed=seed, attempt_limit=1,
-                                                             capture_only=True,
-                                                             export_l1_capacity=7_500_000))
+    return attempt.solve_full_ter(inst, attempt.FullTerConfig(seed=seed, attempt_limit=1,
+                                                              capture_only=True,
+                                                              export_l1_capacity=7_500_000))
+
+
+@pytest.mark.parametrize("seed", SEEDS, ids=hex)
+def test_seed_root_sample_matches_reference_arwlf(oracle_mod, golden, seed):
+    import tergpu
+    from tergpu import snapshot, workload
+
+    g = next(r for r in golden["seed_roots"] if r["seed"] == seed)
+    res = _device_capture(seed)
     assert res.attempts[0]["level1"] == g["level1"]
     assert res.attempts[0]["level2"] == g["level2"]
+    sums = [f"0x{snapshot.fnv1a(res.snapshot.records[l]):016x}" for l in range(3)]
+    assert sums == g["checksums"], hex(seed)
     root = tergpu.run_gpu_root_records(res.snapshot, tergpu.Config(projected_bits=32),
                                        cells=oracle_mod.select_cells(CELLS))
     ref = g["arwlf16"]
@@ -40,5 +60,25 @@ def test_seed_root_sample_matches_reference_arwlf(oracle_mod, golden, index):
         assert got[k] == hexint(ref[k]), (hex(seed), k)
     assert root.telemetry.logical_pairs == ref["pairs"]
     assert root.telemetry.projected_hits == ref["projected_hits"] > 0
+    assert root.residue_exact == ref["residue"]
+    assert sorted(map(list, root.triples[root.flags & 1 == 1].tolist())) == ref["witnesses"]
+
+
+@pytest.mark.parametrize("seed", WHOLE, ids=hex)
+def test_whole_unplanted_root_matches_reference_arwlf(golden, seed):
+    import tergpu
+    from tergpu import snapshot, workload
+
+    g = next(r for r in golden["whole_roots"] if r["seed"] == seed)
+    res = _device_capture(seed)
+    assert res.attempts[0]["level1"] == g["level1"]
+    assert [f"0x{snapshot.fnv1a(res.snapshot.records[l]):016x}" for l in range(3)] == g["checksums"]
+    ref = g["arwlf"]
+    root = tergpu.run_gpu_root_records(res.snapshot, tergpu.Config(projected_bits=g["projected_bits"]))
+    got = workload.digest(root.triples)
+    for k in ("triples", "triple_sum", "triple_xor", "triple_sum2"):
+        assert got[k] == hexint(ref[k]), (hex(seed), k)
+    assert root.telemetry.logical_pairs == ref["pairs"]
+    assert root.telemetry.projected_hits == ref["projected_hits"]
     assert root.residue_exact == ref["residue"]
     assert sorted(map(list, root.triples[root.flags & 1 == 1].tolist())) == ref["witnesses"]
