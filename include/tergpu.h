@@ -25,8 +25,9 @@ extern "C" {
  * 3: tergpu_attempt_in gained root_policy, tergpu_attempt_stats the reference's
  *    per-stage counters and output fingerprints, tergpu_attempt_out the run
  *    fingerprint and the level-3 time.
+ * 4: tergpu_attempt_stats gained audited_stages (TERGPU_ATTEMPT_AUDIT).
  * Callers compiled against another version must not call in (the adapter checks). */
-#define TERGPU_ABI_VERSION 3
+#define TERGPU_ABI_VERSION 4
 
 enum tergpu_status {
   TERGPU_COMPLETED = 0,
@@ -255,6 +256,11 @@ typedef struct {
   uint64_t l1_fingerprint;     /* ... of the three L1 lists */
   uint64_t l0_fingerprint;     /* ... of the retained L0 parents */
   double verification_ms;      /* host verification of the witness */
+  uint32_t audited_stages;     /* TERGPU_ATTEMPT_AUDIT: stages checked against the scalar
+                                  oracles (the nine L3 -> L2 merges, the three L2 -> L1
+                                  merges and the root, where the oracle's work is at most
+                                  10^6 pairs or triples) */
+  uint32_t reserved_audit;
 } tergpu_attempt_stats;
 
 /* tergpu_attempt_in.flags */
@@ -276,6 +282,16 @@ typedef struct {
                                           sweep blocks finish; its joins use blocks of about
                                           2^25 pairs (about 2 ms of one SM) instead of 2^29,
                                           so SMs come free often.  Same results */
+#define TERGPU_ATTEMPT_AUDIT 32u      /* the reference's audit mode (FullTerConfig::audit,
+                                          src/full_ter.cpp:3186-3222, 3318-3334, 3449-3465):
+                                          every stage whose scalar oracle needs at most 10^6
+                                          pairs or triples (every stage at n = 36, the
+                                          L3 -> L2 merges at n = 72) is recomputed on the host
+                                          by plain enumeration and compared with the device's
+                                          output and provenance; a difference returns
+                                          TERGPU_INVARIANT_VIOLATION.  Runs stage by stage and
+                                          reports the root as FullCanonicalOutput, as the
+                                          reference's audit does */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return

@@ -12,7 +12,8 @@
 //                                      bytes, no device work
 // A solve is one call of attempt_limit attempts on the reference's benchmark
 // instance (the planted support fixed to the first n/4 coordinates of each
-// half, bench/ter_full_bench.cpp:218-245).  --fixture, --guided, --audit and
+// half, bench/ter_full_bench.cpp:218-245).  --audit checks every stage whose
+// scalar oracle fits against it (TERGPU_ATTEMPT_AUDIT).  --fixture, --guided and
 // --family=paper-rounded select reference paths the device does not implement;
 // they are refused with a message and exit status 2.
 #include "tergpu.h"
@@ -72,6 +73,7 @@ struct Options {
   Mode mode = Mode::AttemptCost;
   bool preflight = false;
   bool require_found = false;
+  bool audit = false;
   bool unsupported = false;
   std::string unsupported_what;
   uint32_t attempt_limit = 1;
@@ -127,7 +129,8 @@ int parse_options(int argc, char** argv, Options* o) {
     auto has_prefix = [&](std::string_view prefix) { return v.substr(0, prefix.size()) == prefix; };
     if (v == "--preflight") { o->preflight = true; continue; }
     if (v == "--require-found") { o->require_found = true; continue; }
-    if (v == "--audit" || v == "--guided" || v == "--fixture") {
+    if (v == "--audit") { o->audit = true; continue; }
+    if (v == "--guided" || v == "--fixture") {
       o->unsupported = true;
       o->unsupported_what = std::string(v);
       continue;
@@ -348,7 +351,7 @@ Solve solve(const Options& o, const Instance& inst, uint64_t seed, uint64_t time
   in.memory_limit_bytes = o.memory_limit_bytes;
   in.cancel = &cancel;
   in.device = o.device;
-  in.flags = telemetry ? TERGPU_ATTEMPT_TELEMETRY : 0u;
+  in.flags = (telemetry ? TERGPU_ATTEMPT_TELEMETRY : 0u) | (o.audit ? TERGPU_ATTEMPT_AUDIT : 0u);
   // the reference's bench keeps FirstWitness (include/ter/full_ter.hpp:105)
   in.root_policy = TERGPU_ROOT_POLICY_FIRST_WITNESS;
   s.out.stats = s.stats.data();
@@ -385,7 +388,8 @@ void print_metadata(const Options& o, const std::string& command, uint64_t execu
             << " attempts_executed=" << executed << " warmup=" << o.warmup
             << " repeat=" << o.repeat << " time_limit_ms=" << o.time_limit_ms
             << " memory_limit_bytes=" << o.memory_limit_bytes << " seed=" << o.seed
-            << " execution_mode=FullTer target=Random audit=off family=FiniteSanity"
+            << " execution_mode=FullTer target=Random audit=" << (o.audit ? "on" : "off")
+            << " family=FiniteSanity"
             << " command=\"" << command << "\"\n";
 }
 

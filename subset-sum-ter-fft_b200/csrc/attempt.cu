@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <tuple>
 #include <atomic>
 #include <functional>
 #include <thread>
@@ -430,6 +431,130 @@ RootOutcome pick_root(uint32_t n, uint32_t Q, uint32_t policy, const uint32_t* t
   return o;
 }
 
+// ---- audit (TERGPU_ATTEMPT_AUDIT): the reference's scalar oracles per stage
+// (binary_oracle and ternary_oracle, src/full_ter.cpp:2061-2160, compared with
+// the optimized stages at :3186-3222, :3318-3334 and :3449-3465).  Where a
+// stage's oracle work is at most kAuditCap pairs or triples (the reference's
+// kCubicCandidateTripleCap, include/ter/limitations.hpp:89), its device output
+// is recomputed on the host by plain enumeration of the stage's inputs and
+// compared: the canonical output list and the provenance -- which children
+// made each output (the L3 -> L2 merge's raw parents, the ternary merges' and
+// the root's index triples with their decisions).  A difference is
+// InvariantViolation, as in the reference.
+constexpr uint64_t kAuditCap = 1000000;
+
+struct HostEntry {
+  uint64_t p0, p1;
+  u128 res;
+  bool operator<(const HostEntry& o) const {
+    if (p0 != o.p0) return p0 < o.p0;
+    if (p1 != o.p1) return p1 < o.p1;
+    return res < o.res;
+  }
+  bool operator==(const HostEntry& o) const { return p0 == o.p0 && p1 == o.p1 && res == o.res; }
+};
+
+std::vector<HostEntry> host_entries(Workspace& w, const EntryArrays& e, uint64_t m, cudaStream_t st) {
+  std::vector<uint64_t> p0(m), p1(m), rl(m), rh(m);
+  if (m != 0) {
+    check(cudaMemcpyAsync(p0.data(), e.pos0, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(p1.data(), e.pos1, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(rl.data(), e.res_lo, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(rh.data(), e.res_hi, m * 8, cudaMemcpyDeviceToHost, st), "d2h");
+    sync_stream(w, st, "audit download");
+  }
+  std::vector<HostEntry> v(m);
+  for (uint64_t i = 0; i < m; ++i) v[i] = HostEntry{p0[i], p1[i], ((u128)rh[i] << 64) | rl[i]};
+  return v;
+}
+
+// Canonical order (digit words ascending, pos0 first) without repeated digits.
+std::vector<HostEntry> canonical_entries(std::vector<HostEntry> v) {
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end(),
+                      [](const HostEntry& a, const HostEntry& b) { return a.p0 == b.p0 && a.p1 == b.p1; }),
+          v.end());
+  return v;
+}
+
+[[noreturn]] void audit_failed(const char* what) {
+  t_error = std::string("audit: ") + what + " disagrees with the scalar oracle";
+  throw Failure{TERGPU_INVARIANT_VIOLATION};
+}
+
+// L3 -> L2 merge: every pair (a of the left half, b of the right half) with
+// res_a + res_b = t (mod 2^r2), binary digits (disjoint supports) and n/18 ones.
+// The device's raw parents (one per matching pair) and its canonical list.
+void audit_binary(uint32_t n, uint32_t r2, u128 t, const std::vector<HostEntry>& left,
+                  const std::vector<HostEntry>& right, std::vector<HostEntry> raw_dev,
+                  const std::vector<HostEntry>& canon_dev) {
+  const u128 nm = mask128(n), m2 = mask128(r2);
+  std::vector<HostEntry> raw;
+  for (const HostEntry& a : left) {
+    for (const HostEntry& b : right) {
+      const u128 s = (a.res + b.res) & nm;
+      if (((s - t) & m2) != 0) continue;
+      if (((a.p0 & b.p0) | (a.p1 & b.p1)) != 0) continue;
+      const uint64_t p0 = a.p0 | b.p0, p1 = a.p1 | b.p1;
+      if ((uint32_t)(__builtin_popcountll(p0) + __builtin_popcountll(p1)) != n / 18) continue;
+      raw.push_back(HostEntry{p0, p1, s});
+    }
+  }
+  std::sort(raw.begin(), raw.end());
+  std::sort(raw_dev.begin(), raw_dev.end());
+  if (raw != raw_dev) audit_failed("an L3 -> L2 merge's parents (provenance)");
+  if (canonical_entries(std::move(raw)) != canon_dev) audit_failed("an L3 -> L2 list");
+}
+
+struct Triple {
+  uint32_t a, b, c;
+  bool operator<(const Triple& o) const {
+    return std::tie(a, b, c) < std::tie(o.a, o.b, o.c);
+  }
+  bool operator==(const Triple& o) const { return a == o.a && b == o.b && c == o.c; }
+};
+
+// A ternary merge: every triple with res_a + res_b + res_c = t (mod 2^bits)
+// (the candidates), and among them those with disjoint supports (else a
+// structural reject) and `ones` ones (else a distribution reject): the parents.
+struct TernaryOracle {
+  std::vector<Triple> candidates;
+  std::vector<uint8_t> decision;  // 0 parent, 1 structural reject, 2 distribution reject
+  std::vector<HostEntry> parents;
+};
+
+TernaryOracle ternary_oracle(uint32_t n, uint32_t bits, u128 t, uint32_t ones, const std::vector<HostEntry>& A,
+                             const std::vector<HostEntry>& B, const std::vector<HostEntry>& C) {
+  const u128 nm = mask128(n), mb = mask128(bits);
+  TernaryOracle o;
+  for (uint32_t i = 0; i < A.size(); ++i) {
+    for (uint32_t j = 0; j < B.size(); ++j) {
+      const u128 ab = A[i].res + B[j].res;
+      for (uint32_t k = 0; k < C.size(); ++k) {
+        const u128 s = (ab + C[k].res) & nm;
+        if (((s - t) & mb) != 0) continue;
+        o.candidates.push_back(Triple{i, j, k});
+        const uint64_t two0 = (A[i].p0 & B[j].p0) | (A[i].p0 & C[k].p0) | (B[j].p0 & C[k].p0);
+        const uint64_t two1 = (A[i].p1 & B[j].p1) | (A[i].p1 & C[k].p1) | (B[j].p1 & C[k].p1);
+        const uint64_t p0 = A[i].p0 | B[j].p0 | C[k].p0, p1 = A[i].p1 | B[j].p1 | C[k].p1;
+        if ((two0 | two1) != 0) {
+          o.decision.push_back(1);
+        } else if ((uint32_t)(__builtin_popcountll(p0) + __builtin_popcountll(p1)) != ones) {
+          o.decision.push_back(2);
+        } else {
+          o.decision.push_back(0);
+          o.parents.push_back(HostEntry{p0, p1, s});
+        }
+      }
+    }
+  }
+  return o;
+}
+
+bool cubic_fits(uint64_t a, uint64_t b, uint64_t c) {
+  return a == 0 || b == 0 || c == 0 || (a * b <= kAuditCap && a * b * c <= kAuditCap);
+}
+
 // stage_fingerprint of the retained L0 parents: each parent's digits and the
 // root target as its residue (every retained parent is residue-exact).
 uint64_t l0_fingerprint(uint32_t n, const std::vector<std::array<uint64_t, 2>>& parents, u128 T) {
@@ -837,14 +962,17 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   const bool exporting = (in->flags & TERGPU_ATTEMPT_CAPTURE_ONLY) != 0 || out->l1_records[0] != nullptr ||
                          out->l1_records[1] != nullptr || out->l1_records[2] != nullptr;
   const bool telemetry = (in->flags & TERGPU_ATTEMPT_TELEMETRY) != 0;
-  const uint32_t policy = in->root_policy;
-  if (policy > TERGPU_ROOT_POLICY_FULL_CANONICAL) {
+  // audit: every stage checked against the scalar oracles where they fit (the
+  // root then reports FullCanonicalOutput, as the reference's audit does)
+  const bool audit = (in->flags & TERGPU_ATTEMPT_AUDIT) != 0;
+  const uint32_t policy = audit ? TERGPU_ROOT_POLICY_FULL_CANONICAL : in->root_policy;
+  if (in->root_policy > TERGPU_ROOT_POLICY_FULL_CANONICAL) {
     t_error = "root_policy must be FirstWitness (0), CountOnly (1) or FullCanonicalOutput (2)";
     return TERGPU_INVALID_CONFIGURATION;
   }
   const auto t_l3 = std::chrono::steady_clock::now();
   GraphPlan* plan = nullptr;
-  if (!exporting && !telemetry && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
+  if (!exporting && !telemetry && !audit && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
     plan = graph_plan(w, n, r1, r2, l3, st);
     held.plan = plan;
     if (plan != nullptr) graph_level3(*plan, weights, st);
@@ -940,6 +1068,14 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     }
     for (int i = 0; i < 9; ++i) stat.level2_sizes[i] = l2n[i];
     stat.l3_survivors = stat.l3_modular;
+    if (audit && l3 * l3 <= kAuditCap) {
+      const std::vector<HostEntry> hl = host_entries(w, left, l3, st), hr = host_entries(w, right, l3, st);
+      for (int i = 0; i < 9; ++i) {
+        audit_binary(n, r2, tg.t2[i] & mask128(r2), hl, hr, host_entries(w, view(raw, hb[i]), sg.cnt[i], st),
+                     host_entries(w, l2[i], l2n[i], st));
+        ++stat.audited_stages;
+      }
+    }
     check(cudaGetLastError(), "L3 -> L2");
     if (telemetry) stat.l2_fingerprint = lists_fingerprint(w, n, l2.data(), l2n.data(), 9, st);
     stat.l2_ms = ms_since(t_att);
@@ -1006,6 +1142,24 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       l1[g] = entry_slot(w, S_L1 + 4 * g, ncand);
       l1n[g] = canonicalize(w, cand, ncand, l1[g], st);
       stat.level1_sizes[g] = l1n[g];
+      if (audit && cubic_fits(l2n[3 * g], l2n[3 * g + 1], l2n[3 * g + 2])) {
+        const TernaryOracle o =
+            ternary_oracle(n, b1, t1, n / 6, host_entries(w, l2[3 * g], l2n[3 * g], st),
+                           host_entries(w, l2[3 * g + 1], l2n[3 * g + 1], st),
+                           host_entries(w, l2[3 * g + 2], l2n[3 * g + 2], st));
+        std::vector<uint32_t> ht(jr.triples * 3);
+        if (jr.triples != 0) download(w, ht.data(), jr.d_triples, ht.size(), st);
+        std::vector<Triple> dev(jr.triples), want = o.candidates;
+        for (uint64_t i = 0; i < jr.triples; ++i) dev[i] = Triple{ht[3 * i], ht[3 * i + 1], ht[3 * i + 2]};
+        std::sort(dev.begin(), dev.end());
+        std::sort(want.begin(), want.end());
+        if (dev != want) audit_failed("an L2 -> L1 merge's candidate triples (provenance)");
+        const uint64_t s_rej = std::count(o.decision.begin(), o.decision.end(), 1);
+        const uint64_t d_rej = std::count(o.decision.begin(), o.decision.end(), 2);
+        if (s_rej != lc[2] || d_rej != lc[3]) audit_failed("an L2 -> L1 merge's rejects");
+        if (canonical_entries(o.parents) != host_entries(w, l1[g], l1n[g], st)) audit_failed("an L1 list");
+        ++stat.audited_stages;
+      }
     }
     check(cudaGetLastError(), "L2 -> L1");
     if (telemetry) stat.l1_fingerprint = lists_fingerprint(w, n, l1.data(), l1n.data(), 3, st);
@@ -1110,6 +1264,27 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       sync_stream(w, st, "sync");
     }
     root = pick_root(n, Q, policy, htrip.data(), hflags.data(), jr.triples, j.key_lo[0], j.key_lo[1], recs, rb);
+    if (audit && cubic_fits(l1n[0], l1n[1], l1n[2])) {
+      const TernaryOracle o = ternary_oracle(n, n, T & nmask, n / 2, host_entries(w, l1[0], l1n[0], st),
+                                             host_entries(w, l1[1], l1n[1], st), host_entries(w, l1[2], l1n[2], st));
+      std::vector<std::pair<Triple, uint8_t>> dev, want;
+      for (uint64_t i = 0; i < jr.triples; ++i) {
+        if ((hflags[i] & 1) == 0) continue;
+        const uint8_t d = (hflags[i] & 8) != 0 ? 1 : (hflags[i] & 16) != 0 ? 2 : (hflags[i] & 4) != 0 ? 0 : 3;
+        dev.push_back({Triple{htrip[3 * i], htrip[3 * i + 1], htrip[3 * i + 2]}, d});
+      }
+      for (size_t i = 0; i < o.candidates.size(); ++i) want.push_back({o.candidates[i], o.decision[i]});
+      auto by_triple = [](const std::pair<Triple, uint8_t>& x, const std::pair<Triple, uint8_t>& y) {
+        return x.first < y.first || (x.first == y.first && x.second < y.second);
+      };
+      std::sort(dev.begin(), dev.end(), by_triple);
+      std::sort(want.begin(), want.end(), by_triple);
+      if (dev != want) audit_failed("the root's residue-exact triples or their decisions (provenance)");
+      std::vector<std::array<uint64_t, 2>> parents;
+      for (const HostEntry& e : canonical_entries(o.parents)) parents.push_back({e.p0, e.p1});
+      if (parents != root.parents) audit_failed("the root's parents");
+      ++stat.audited_stages;
+    }
     if (telemetry) {
       // the reporter's low-prefilter candidates: triples equal on the low p
       // bits, counted up to the FirstWitness stop when there is one

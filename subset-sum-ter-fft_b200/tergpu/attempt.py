@@ -37,6 +37,7 @@ class AttemptStats(ctypes.Structure):
         ("root_policy", ctypes.c_uint32), ("root_early_stopped", ctypes.c_uint32),
         ("l2_fingerprint", ctypes.c_uint64), ("l1_fingerprint", ctypes.c_uint64),
         ("l0_fingerprint", ctypes.c_uint64), ("verification_ms", ctypes.c_double),
+        ("audited_stages", ctypes.c_uint32), ("reserved_audit", ctypes.c_uint32),
     ]
 
 
@@ -78,6 +79,7 @@ class FullTerConfig:
     # RootOutputPolicy (include/ter/full_ter.hpp:79-83); FirstWitness is the reference's default
     root_policy: int = _abi.ROOT_POLICY_FIRST_WITNESS
     telemetry: bool = False       # the reference's full telemetry: prefilter counts, fingerprints
+    audit: bool = False           # FullTerConfig::audit: stages checked against the scalar oracles
 
 
 @dataclass
@@ -118,6 +120,7 @@ def _stats_dict(s: AttemptStats) -> dict:
         "valid_roots": int(s.valid_roots), "root_pairs": int(s.root_pairs),
         "l2_ms": float(s.l2_ms), "l1_ms": float(s.l1_ms), "root_ms": float(s.root_ms),
         "total_ms": float(s.total_ms), "verification_ms": float(s.verification_ms),
+        "audited_stages": int(s.audited_stages),
     }
     for name in _STAT_INTS:
         d[name] = int(getattr(s, name))
@@ -144,7 +147,8 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     ain.n = instance.n
     ain.flags = ((_abi.ATTEMPT_CAPTURE_ONLY if config.capture_only else 0)
                  | (_abi.ATTEMPT_NO_GRAPH if config.no_graph else 0)
-                 | (_abi.ATTEMPT_TELEMETRY if config.telemetry else 0))
+                 | (_abi.ATTEMPT_TELEMETRY if config.telemetry else 0)
+                 | (_abi.ATTEMPT_AUDIT if config.audit else 0))
     ain.values_le = values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.target_le = target.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.seed = config.seed & (2**64 - 1)

@@ -178,3 +178,16 @@ def test_time_limit_cancels_inside_the_n108_root():
     assert p.returncode == 1
     assert "Cancelled" in p.stderr
     assert elapsed < 6.0, elapsed
+
+
+@pytest.mark.gpu
+def test_audit_flag_checks_the_stages(tmp_path):
+    """--audit (the reference's audit mode) runs: every stage of the n=36 attempts
+    is checked against the scalar oracles and the command succeeds with
+    audit=on in its metadata."""
+    import subprocess
+
+    proc = subprocess.run([str(CLI), "--n=36", "--attempt-limit=8", "--warmup=0", "--repeat=1", "--audit"],
+                          capture_output=True, text=True, timeout=600)
+    assert proc.returncode == 0, proc.stderr
+    assert "audit=on" in proc.stdout

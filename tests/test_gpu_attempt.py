@@ -92,6 +92,36 @@ def test_attempt_telemetry_matches_reference(golden, case):
         assert sum(a["level1"]) == row["middle"]["deduplicated"]
 
 
+@pytest.mark.parametrize("case", [i for i in range(16) if i % 2 == 1])
+def test_audit_mode_checks_every_stage_and_matches_reference(golden, case):
+    """TERGPU_ATTEMPT_AUDIT (the reference's FullTerConfig::audit): every stage
+    whose scalar oracle takes at most 10^6 pairs or triples is recomputed on the
+    host and compared with the device's output and provenance -- all 13 stages
+    at n=36 (nine L3 -> L2 merges, three L2 -> L1 merges, the root), the nine
+    L3 -> L2 merges at n=72.  No stage disagrees, and the audited run reports the
+    root as FullCanonicalOutput whatever policy was asked for, as the reference's
+    audit does: its counters and fingerprints equal the reference's
+    FullCanonicalOutput telemetry."""
+    from tergpu import _abi
+
+    g = golden["attempt_telemetry"][case]
+    assert g["policy"] == "canon"
+    _, res = _attempt(g["n"], g["seed"], 0, g["attempts"], kind=g["kind"],
+                      root_policy=_abi.ROOT_POLICY_FIRST_WITNESS, telemetry=True, audit=True,
+                      memory_limit_bytes=64 << 30)
+    final = g["final"]
+    assert res.status == final["status"], (res.status_name, _abi.last_error())
+    assert res.fingerprint == hexint(final["fingerprint"])
+    assert len(res.attempts) == len(g["rows"])
+    for a, row in zip(res.attempts, g["rows"]):
+        assert a["audited_stages"] == (13 if g["n"] == 36 else 9)
+        for stage, fields in STAGES.items():
+            for ref_key, dev_key in fields.items():
+                want = row[stage][ref_key]
+                want = hexint(want) if ref_key == "fingerprint" else want
+                assert a[dev_key] == want, (g["n"], g["seed"], row["attempt"], stage, ref_key)
+
+
 def test_n36_attempt_loop_stops_like_the_reference(golden):
     """The whole loop in one call: the reference's final status and attempt count."""
     from tergpu import _abi
