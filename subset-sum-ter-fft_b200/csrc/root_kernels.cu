@@ -1473,11 +1473,24 @@ __global__ void __launch_bounds__(256) k_family_arrange(uint64_t* __restrict__ r
     order[pos] = static_cast<uint16_t>(i);
   }
   __syncthreads();
+  // while every class still has entries, a slot takes exactly one entry of each
+  // class (lane k <- class k): the first m0 = min over classes of the class size
+  // slots are filled by all threads at once, exactly as the loop below would
+  __shared__ uint32_t m0s;
   if (threadIdx.x < 32u) {
-    uint32_t cur = cstart[lane];
-    uint32_t rem = cend[lane] - cstart[lane];
+    const uint32_t m = __reduce_min_sync(kFull, cend[lane] - cstart[lane]);
+    if (lane == 0u) m0s = m;
+  }
+  __syncthreads();
+  const uint32_t m0 = m0s;
+  for (uint32_t p = threadIdx.x; p < 32u * m0; p += blockDim.x) {
+    perm[p] = order[cstart[p & 31u] + (p >> 5)];
+  }
+  if (threadIdx.x < 32u) {
+    uint32_t cur = cstart[lane] + m0;
+    uint32_t rem = cend[lane] - cstart[lane] - m0;
     const uint32_t slots = (n + 31u) / 32u;
-    for (uint32_t j = 0; j < slots; ++j) {
+    for (uint32_t j = m0; j < slots; ++j) {
       // take <= sum of rem, and every lane with rem > 0 takes one, so at most
       // `take` lanes take one here and the loop below always finds a lane
       const uint32_t take = min(32u, n - 32u * j);
