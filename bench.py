@@ -464,16 +464,17 @@ def run_tergpu(args):
         print(json.dumps(result), flush=True)
 
 
-def ref_binary():
+def ref_binary(have=None, ref=None):
     """The reference harness for timing: the widest of its builds whose CPU flags
-    this host has -- -march=native (the CPU that built it), then x86-64-v4
-    (AVX-512), then the portable x86-64-v3."""
-    ref = ROOT / "oracle" / "_ref"
-    have = set()
-    for line in Path("/proc/cpuinfo").read_text().splitlines():
-        if line.startswith("flags"):
-            have = set(line.split(":", 1)[1].split())
-            break
+    this host has (`have`, default /proc/cpuinfo's) -- -march=native (the CPU
+    that built it), then x86-64-v4 (AVX-512), then the portable x86-64-v3."""
+    ref = Path(ref) if ref is not None else ROOT / "oracle" / "_ref"
+    if have is None:
+        have = set()
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                have = set(line.split(":", 1)[1].split())
+                break
     skipped = []
     for exe, flags, name in (("terref_native", "native_flags.txt", "native"),
                              ("terref_v4", "v4_flags.txt", "x86-64-v4")):
