@@ -184,10 +184,23 @@ __global__ void __launch_bounds__(256) k_scatter_priv(
   }
 }
 
-// One CTA of 1024 threads: padded exclusive scan of up to 65536 family counts.
+// The staged scatter's bucket table (u32): bucket cursors at [32 h] (one
+// 128-byte line each, so the tiles' reservations spread over L2 slices instead
+// of queueing on one), then bucket starts, bucket sizes and the tile prefix over
+// the buckets; k_scan fills it with the family offsets.
+constexpr uint32_t kStageBins = 128;
+constexpr uint32_t kStageCurStride = 32;
+constexpr uint32_t kStageTabStart = kStageBins * kStageCurStride, kStageTabSize = kStageTabStart + kStageBins,
+                   kStageTabTiles = kStageTabSize + kStageBins;
+
+// One CTA of 1024 threads: padded exclusive scan of up to 65536 family counts;
+// with a table, also the staged scatter's buckets of 2^lb families each (at
+// most kStageBins of them, each at least as wide as one thread's families).
 __global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t nfam, uint32_t* __restrict__ off,
-                       uint32_t* __restrict__ cursor) {
+                       uint32_t* __restrict__ cursor, uint32_t lb = 0, uint32_t* __restrict__ table = nullptr) {
   __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t bsum[kStageBins];
+  if (table != nullptr && threadIdx.x < kStageBins) bsum[threadIdx.x] = 0u;
   const uint32_t per = (nfam + blockDim.x - 1) / blockDim.x;
   const uint32_t begin = threadIdx.x * per;
   const uint32_t end = min(nfam, begin + per);
@@ -212,12 +225,35 @@ __global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t nfam, uint32_t
   }
   __syncthreads();
   uint32_t run = v - local + (warp > 0 ? warp_sums[warp - 1] : 0);
+  uint32_t plain = 0;
   for (uint32_t f = begin; f < end; ++f) {
     off[f] = run;
     cursor[f] = run;
     run += (cnt[f] + 1u) & ~1u;
+    plain += cnt[f];
   }
   if (threadIdx.x == blockDim.x - 1) off[nfam] = run;
+  if (table == nullptr) return;  // uniform across the block
+  if (begin < end && plain != 0u) atomicAdd(&bsum[begin >> lb], plain);
+  __syncthreads();  // off[] and the bucket sums complete
+  const uint32_t nb = nfam >> lb;
+  __shared__ uint32_t btiles[kStageBins];
+  if (threadIdx.x < nb) {
+    const uint32_t h = threadIdx.x;
+    table[h * kStageCurStride] = off[h << lb];
+    table[kStageTabStart + h] = off[h << lb];
+    table[kStageTabSize + h] = bsum[h];
+    btiles[h] = (bsum[h] + kStageTile - 1) / kStageTile;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (uint32_t h = 0; h < nb; ++h) {
+      table[kStageTabTiles + h] = t;
+      t += btiles[h];
+    }
+    table[kStageTabTiles + nb] = t;
+  }
 }
 
 __global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __restrict__ key_hi,
@@ -252,9 +288,7 @@ __global__ void k_scatter(const uint64_t* __restrict__ key_lo, const uint8_t* __
 // land in consecutive slots (about 64 entries per digit and tile).  Within a
 // family, entries keep no particular order (the sweep needs none).
 //
-// table (u32): bucket cursors at [32 h] (one 128-byte line each, so the tiles'
-// reservations spread over L2 slices instead of queueing on one), then bucket
-// starts, bucket sizes and the tile prefix over the buckets.
+// The bucket table comes from k_scan (launch_scan_staged).
 
 struct StageArgs {
   const uint64_t* key;      // pass reading the caller's lists: keys, high bytes, ids
@@ -275,33 +309,6 @@ struct StageArgs {
   uint32_t fb, lb;
 };
 
-constexpr uint32_t kStageBins = 128;
-constexpr uint32_t kStageCurStride = 32;
-constexpr uint32_t kStageTabStart = kStageBins * kStageCurStride, kStageTabSize = kStageTabStart + kStageBins,
-                   kStageTabTiles = kStageTabSize + kStageBins;
-
-__global__ void k_bucket_init(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
-                              uint32_t fb, uint32_t lb, uint32_t* __restrict__ table) {
-  __shared__ uint32_t tiles[kStageBins];
-  const uint32_t nb = 1u << (fb - lb), h = threadIdx.x;
-  if (h < nb) {
-    uint32_t s = 0;
-    for (uint32_t l = 0; l < (1u << lb); ++l) s += cnt[(h << lb) + l];
-    table[h * kStageCurStride] = off[h << lb];
-    table[kStageTabStart + h] = off[h << lb];
-    table[kStageTabSize + h] = s;
-    tiles[h] = (s + kStageTile - 1) / kStageTile;
-  }
-  __syncthreads();
-  if (h == 0) {
-    uint32_t run = 0;
-    for (uint32_t i = 0; i < nb; ++i) {
-      table[kStageTabTiles + i] = run;
-      run += tiles[i];
-    }
-    table[kStageTabTiles + nb] = run;
-  }
-}
 
 // FROM_INPUT: tiles of the caller's list (else: tiles of the temp buckets).
 // TO_FINAL: digit = low family digit, into the families (else: high digit,
@@ -1789,9 +1796,9 @@ bool staged_partition(const Count& n, uint32_t fb) {
 uint32_t staged_table_words(uint32_t) { return kStageTabTiles + kStageBins + 1; }
 
 uint32_t launch_scatter_staged(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, Count n,
-                               uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, const uint32_t* cnt,
-                               const uint32_t* off, uint32_t* cursor, const StageBuffers& tmp, uint64_t* res,
-                               uint8_t* hi, uint32_t* out_id, cudaStream_t st) {
+                               uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
+                               const StageBuffers& tmp, uint64_t* res, uint8_t* hi, uint32_t* out_id,
+                               cudaStream_t st) {
   if (n.cap == 0) return 0;
   StageArgs a{};
   a.key = key_lo;
@@ -1819,15 +1826,25 @@ uint32_t launch_scatter_staged(const uint64_t* key_lo, const uint8_t* key_hi, co
     k_stage_scatter<true, true><<<static_cast<int>(std::min(tiles, kResident)), kStageThreads, smem, st>>>(a);
     return 1;
   }
-  a.lb = fb / 2;
+  a.lb = staged_low_bits(fb);
   a.nb = 1u << (fb - a.lb);
-  k_bucket_init<<<1, kStageBins, 0, st>>>(cnt, off, fb, a.lb, tmp.table);
   allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<true, false>));
   allow_max_smem(reinterpret_cast<const void*>(k_stage_scatter<false, true>));
   k_stage_scatter<true, false><<<static_cast<int>(std::min(tiles, kResident)), kStageThreads, smem, st>>>(a);
   k_stage_scatter<false, true>
       <<<static_cast<int>(std::min(tiles + a.nb, kResident)), kStageThreads, smem, st>>>(a);
-  return 3;
+  return 2;
+}
+
+uint32_t staged_low_bits(uint32_t fb) { return fb <= 7 ? fb : fb / 2; }
+
+void launch_scan_staged(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor, uint32_t fb,
+                        uint32_t* table, cudaStream_t st) {
+  if (fb <= 7) {  // one staged pass: no buckets
+    k_scan<<<1, 1024, 0, st>>>(cnt, nfam, off, cursor);
+    return;
+  }
+  k_scan<<<1, 1024, 0, st>>>(cnt, nfam, off, cursor, staged_low_bits(fb), table);
 }
 
 void launch_max_family(const uint32_t* cnt, uint32_t nfam, unsigned long long* counters, int slot,

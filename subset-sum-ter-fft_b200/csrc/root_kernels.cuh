@@ -145,12 +145,17 @@ struct StageBuffers {
 };
 bool staged_partition(const Count& n, uint32_t fb);
 uint32_t staged_table_words(uint32_t fb);
-// The scatter of launch_scatter through the two staged passes (cursor and off
-// as the scan left them).  Returns the kernels launched.
+// Family digits of the second staged pass (all fb digits when one pass does).
+uint32_t staged_low_bits(uint32_t fb);
+// launch_scan that also fills the staged scatter's bucket table (tmp.table).
+void launch_scan_staged(const uint32_t* cnt, uint32_t nfam, uint32_t* off, uint32_t* cursor, uint32_t fb,
+                        uint32_t* table, cudaStream_t st);
+// The scatter of launch_scatter through the staged passes (cursor and the
+// bucket table as launch_scan_staged left them).  Returns the kernels launched.
 uint32_t launch_scatter_staged(const uint64_t* key_lo, const uint8_t* key_hi, const uint32_t* id, Count n,
-                               uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, const uint32_t* cnt,
-                               const uint32_t* off, uint32_t* cursor, const StageBuffers& tmp, uint64_t* res,
-                               uint8_t* hi, uint32_t* out_id, cudaStream_t st);
+                               uint32_t fb, uint64_t fast_mask, uint32_t hi_mask, uint32_t* cursor,
+                               const StageBuffers& tmp, uint64_t* res, uint8_t* hi, uint32_t* out_id,
+                               cudaStream_t st);
 size_t sweep_smem_bytes(uint32_t wb);
 // v1: A windows in registers, B broadcast (any family order).
 void launch_sweep(const SweepArgs& a, bool aligned, cudaStream_t st);

@@ -330,13 +330,13 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
   for (int l = 0; l < 3; ++l) {
     check(cudaMemsetAsync(b.cnt[l], 0, nfam * 4ull, st), "memset");
     launch_hist(j.key_lo[l], j.count[l], nfam - 1, b.cnt[l], st);
-    launch_scan(b.cnt[l], nfam, b.off[l], b.cur[l], st);
     const uint32_t hi_mask = hi_bits ? ((1u << hi_bits) - 1u) : 0u;
     if (b.stage.key != nullptr && staged_partition(j.count[l], tu.fb)) {
+      launch_scan_staged(b.cnt[l], nfam, b.off[l], b.cur[l], tu.fb, b.stage.table, st);
       *launches += launch_scatter_staged(j.key_lo[l], j.key_hi[l], j.id[l], j.count[l], tu.fb, fast_mask,
-                                         hi_mask, b.cnt[l], b.off[l], b.cur[l], b.stage, b.res[l], b.hi[l],
-                                         b.id[l], st);
+                                         hi_mask, b.cur[l], b.stage, b.res[l], b.hi[l], b.id[l], st);
     } else {
+      launch_scan(b.cnt[l], nfam, b.off[l], b.cur[l], st);
       launch_scatter(j.key_lo[l], j.key_hi[l], j.id[l], j.count[l], tu.fb, fast_mask, hi_mask, b.cur[l],
                      b.res[l], b.hi[l], b.id[l], st);
       *launches += j.count[l].cap != 0 ? 1 : 0;
