@@ -454,9 +454,15 @@ def run_tergpu(args):
     if rank == 0 and world == 1 and not args.no_batch:
         result["batch"] = batch_measure(args, False, 256, args.rate, args.serve_n)
         result["serve"] = batch_measure(args, True, 400, 200.0, "36,48,60,72,84,96")
-        result["serve"]["note"] = ("n = 108 requests (seconds of sweep per attempt, up to 64 "
-                                   "attempts) are measured apart: bench.py --serve "
-                                   "--serve-n 36,48,60,72,84,96,108")
+        result["serve"]["note"] = ("without n = 108: see serve_n108 for a mix with it")
+        # config 5 with n = 108 in the mix: 28 requests at 4/s over n = 36 ... 108; n = 108
+        # budgets capped at one attempt (one holds the device for ~7.7 s), the others 1-64
+        result["serve_n108"] = batch_measure(args, True, 28, 4.0, "36,48,60,72,84,96,108",
+                                             max_attempts_108=1)
+        result["serve_n108"]["note"] = ("n = 108 requests with a budget of 1 attempt (the config's "
+                                        "1-64 would make one such request minutes of whole-GPU "
+                                        "sweep); per-n latency, admission wait and service time "
+                                        "in config.by_n")
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -749,7 +755,8 @@ def solve_requests(args, serve: bool):
     return reqs
 
 
-def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -> dict:
+def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str,
+                  max_attempts_108: int | None = None) -> dict:
     """One batch (config 4) or served (config 5) measurement: the same seeded
     requests one at a time (one pipeline, in order) and through the
     continuous-batching engine; every result must be bit-identical between the
@@ -759,6 +766,8 @@ def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -
 
     a = argparse.Namespace(**vars(args))
     a.requests, a.rate, a.serve_n = requests, rate, serve_n
+    if max_attempts_108 is not None:
+        a.max_attempts_108 = max_attempts_108
     reqs = solve_requests(a, serve)
     # warm both paths: module load, and every slot's workspace with its captured
     # attempt graphs (the engine keeps its slots between calls, as a server would);
@@ -818,7 +827,7 @@ def batch_measure(args, serve: bool, requests: int, rate: float, serve_n: str) -
                    "found": len(found), "slots": args.slots, "seed": args.seed,
                    "n": sorted({r.instance.n for r in reqs}), "by_n": by_n,
                    "max_attempts": args.max_attempts or (64 if serve else 16),
-                   "max_attempts_n108": (getattr(args, "max_attempts_108", 0) or None)
+                   "max_attempts_n108": (getattr(a, "max_attempts_108", 0) or None)
                    if any(r.instance.n >= 108 for r in reqs) else None,
                    "arrival_rate_per_s": rate if serve else None,
                    "attempts_run": sum(len(r.attempts) for r in many.results),
