@@ -307,7 +307,11 @@ typedef struct {
   uint32_t attempt_first;
   uint32_t attempt_count;
   uint64_t memory_limit_bytes; /* 0: no ceiling */
-  const volatile int32_t *cancel; /* host flag, polled between stages; may be NULL */
+  const volatile int32_t *cancel; /* host flag, polled between stages and inside the root
+                                     and L2 -> L1 sweeps (mirrored into a device-visible word
+                                     every 200 us; each warp reads it every eighth work item),
+                                     so a running n = 108 sweep stops within milliseconds:
+                                     TERGPU_CANCELLED.  May be NULL */
   int32_t device;
   uint32_t root_policy;        /* TERGPU_ROOT_POLICY_* (the numerics of ter::RootOutputPolicy,
                                   include/ter/full_ter.hpp:79-83) */
@@ -396,6 +400,12 @@ typedef struct {
   uint64_t refused;             /* requests completed at admission by the preflight */
 } tergpu_batch_out;
 
+/* The slots run two streams each (TERGPU_ATTEMPT_BACKGROUND for n >= 108 on the lower-priority
+ * one).  CUDA maps streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware work queues (8 unless
+ * set), so with more streams than queues a short request's kernel can wait behind a long one
+ * queued earlier on another slot's stream.  Loading this library sets the variable to 32 when
+ * the caller has not set it; it takes effect only for a CUDA context created afterwards, so a
+ * caller that initializes CUDA first should set it itself. */
 int tergpu_attempt_batch(const tergpu_batch_in *in, tergpu_batch_out *out);
 
 /*
