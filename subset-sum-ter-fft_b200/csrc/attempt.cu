@@ -364,9 +364,9 @@ struct RootOutcome {
   std::vector<std::array<uint64_t, 2>> parents;
 };
 
-RootOutcome pick_root(uint32_t n, uint32_t Q, uint32_t policy, const uint32_t* trip, const uint8_t* flags,
-                      uint64_t count, const uint64_t* d_key_a, const uint64_t* d_key_b,
-                      uint8_t* const recs[3], uint32_t rb) {
+RootOutcome pick_root(Workspace& w, cudaStream_t st, uint32_t n, uint32_t Q, uint32_t policy,
+                      const uint32_t* trip, const uint8_t* flags, uint64_t count, const uint64_t* d_key_a,
+                      const uint64_t* d_key_b, uint8_t* const recs[3], uint32_t rb) {
   const uint32_t w64 = (n + 63) / 64;
   RootOutcome o;
   std::vector<uint64_t> mod;  // the visitor's modular candidates
@@ -383,8 +383,12 @@ RootOutcome pick_root(uint32_t n, uint32_t Q, uint32_t policy, const uint32_t* t
     std::array<uint64_t, 2> p{0, 0};
     for (int l = 0; l < 3; ++l) {
       uint32_t wds[4] = {0, 0, 0, 0};  // the record's pos words (w64 <= 2)
-      check(cudaMemcpy(wds, recs[l] + (uint64_t)trip[3 * i + l] * rb, w64 * 8, cudaMemcpyDeviceToHost),
+      // on the attempt's own stream: the legacy default stream is shared by every
+      // thread of the process (the batch engine's other slots included)
+      check(cudaMemcpyAsync(wds, recs[l] + (uint64_t)trip[3 * i + l] * rb, w64 * 8, cudaMemcpyDeviceToHost,
+                            st),
             "record download");
+      sync_stream(w, st, "record download");
       p[0] |= (uint64_t)wds[0] | ((uint64_t)wds[1] << 32);
       if (w64 > 1) p[1] |= (uint64_t)wds[2] | ((uint64_t)wds[3] << 32);
     }
@@ -401,8 +405,9 @@ RootOutcome pick_root(uint32_t n, uint32_t Q, uint32_t policy, const uint32_t* t
     for (size_t k = 0; k < mod.size(); ++k) {
       const uint64_t i = mod[k];
       uint64_t ka = 0, kb = 0;
-      check(cudaMemcpy(&ka, d_key_a + trip[3 * i], 8, cudaMemcpyDeviceToHost), "key download");
-      check(cudaMemcpy(&kb, d_key_b + trip[3 * i + 1], 8, cudaMemcpyDeviceToHost), "key download");
+      check(cudaMemcpyAsync(&ka, d_key_a + trip[3 * i], 8, cudaMemcpyDeviceToHost, st), "key download");
+      check(cudaMemcpyAsync(&kb, d_key_b + trip[3 * i + 1], 8, cudaMemcpyDeviceToHost, st), "key download");
+      sync_stream(w, st, "key download");
       const uint32_t bi = (uint32_t)((ka & pm) >> tb);
       keys[k] = VisitKey{bi + (uint32_t)((kb & pm) >> tb), bi, trip[3 * i], trip[3 * i + 1], trip[3 * i + 2]};
       if ((flags[i] & 4) != 0 && (first < 0 || keys[k].before(keys[first]))) first = (int64_t)k;
@@ -871,7 +876,7 @@ bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, uint32
   stat->root_pairs = c.l1[0] * c.l1[1];
   const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
   const uint32_t rb = 16 * w64 + 4 * w32;
-  *root = pick_root(n, n - r1, policy, g.h_triples, g.h_aflags, c.root_counters[kTriples], g.rk_lo[0],
+  *root = pick_root(w, st, n, n - r1, policy, g.h_triples, g.h_aflags, c.root_counters[kTriples], g.rk_lo[0],
                     g.rk_lo[1], g.recs, rb);
   return true;
 }
@@ -1263,7 +1268,8 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       check(cudaMemcpyAsync(hflags.data(), dflags, jr.triples, cudaMemcpyDeviceToHost, st), "d2h");
       sync_stream(w, st, "sync");
     }
-    root = pick_root(n, Q, policy, htrip.data(), hflags.data(), jr.triples, j.key_lo[0], j.key_lo[1], recs, rb);
+    root = pick_root(w, st, n, Q, policy, htrip.data(), hflags.data(), jr.triples, j.key_lo[0], j.key_lo[1], recs,
+                     rb);
     if (audit && cubic_fits(l1n[0], l1n[1], l1n[2])) {
       const TernaryOracle o = ternary_oracle(n, n, T & nmask, n / 2, host_entries(w, l1[0], l1n[0], st),
                                              host_entries(w, l1[1], l1n[1], st), host_entries(w, l1[2], l1n[2], st));

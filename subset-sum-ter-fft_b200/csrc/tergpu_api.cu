@@ -622,7 +622,8 @@ JoinResult run_join(Workspace& w, const JoinInput& in, uint64_t input_bytes) {
     if (in.cells != nullptr) {
       std::memcpy(hcells.data(), in.cells, 4096);
     } else {
-      check(cudaMemcpy(hcells.data(), d_cells, 4096, cudaMemcpyDeviceToHost), "cells download");
+      check(cudaMemcpyAsync(hcells.data(), d_cells, 4096, cudaMemcpyDeviceToHost, st), "cells download");
+      sync_stream(w, st, "cells download");
     }
   }
   // B sizes by t mod 64: the cell mask and the shard (shards | 64) see only that
