@@ -11,6 +11,7 @@
 //   residual and the high key byte.  No floating point anywhere.
 
 #include <algorithm>
+#include <cmath>
 #include "root_kernels.cuh"
 
 #include <cooperative_groups.h>
@@ -1438,21 +1439,24 @@ __global__ void __launch_bounds__(kSweep4Threads, 1) k_sweep4(const SweepArgs a)
 // from the classes with the most entries left (fewest repeats in the slot
 // first).  A permutation inside the family: the sweep is exact for any order,
 // the layout only decides bank conflicts.  Larger families stay as they are.
+// `cap` (at most kSortCap) sizes the shared-memory layout: a family of more
+// entries keeps its order (the sweep stays exact; only its probes may share
+// banks), a smaller cap leaves room for more CTAs per SM.
 __global__ void __launch_bounds__(256) k_family_arrange(uint64_t* __restrict__ res,
                                                         uint8_t* __restrict__ hi,
                                                         uint32_t* __restrict__ id,
                                                         const uint32_t* __restrict__ off,
-                                                        const uint32_t* __restrict__ cnt) {
+                                                        const uint32_t* __restrict__ cnt, uint32_t cap) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem);
-  uint32_t* ids = reinterpret_cast<uint32_t*>(keys + kSortCap);
-  uint16_t* order = reinterpret_cast<uint16_t*>(ids + kSortCap);  // entries grouped by class
-  uint16_t* perm = order + kSortCap;                               // position -> entry
-  uint8_t* his = reinterpret_cast<uint8_t*>(perm + kSortCap);
+  uint32_t* ids = reinterpret_cast<uint32_t*>(keys + cap);
+  uint16_t* order = reinterpret_cast<uint16_t*>(ids + cap);  // entries grouped by class
+  uint16_t* perm = order + cap;                               // position -> entry
+  uint8_t* his = reinterpret_cast<uint8_t*>(perm + cap);
   __shared__ uint32_t cend[32], cstart[32];
   const uint32_t f = blockIdx.x;
   const uint32_t n = cnt[f];
-  if (n < 2u || n > kSortCap) return;  // uniform across the block
+  if (n < 2u || n > cap) return;  // uniform across the block
   const uint32_t base = off[f];
   if (threadIdx.x < 32u) cend[threadIdx.x] = 0u;
   __syncthreads();
@@ -1924,10 +1928,14 @@ void launch_sweep3(const SweepArgs& a, cudaStream_t st) {
 }
 
 void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
-                           const uint32_t* cnt, uint32_t nfam, cudaStream_t st) {
-  const size_t smem = static_cast<size_t>(kSortCap) * (8 + 4 + 2 + 2 + 1);
+                           const uint32_t* cnt, uint32_t nfam, uint64_t mean_family, cudaStream_t st) {
+  // half the layout when the families' Poisson tail (mean + 6 sd) stays inside it:
+  // twice the CTAs per SM (the n = 108 root's ~1,700-entry B families)
+  const double tail = static_cast<double>(mean_family) + 6.0 * std::sqrt(static_cast<double>(mean_family)) + 32;
+  const uint32_t cap = tail <= kSortCap / 2 ? kSortCap / 2 : kSortCap;
+  const size_t smem = static_cast<size_t>(cap) * (8 + 4 + 2 + 2 + 1);
   allow_max_smem(reinterpret_cast<const void*>(k_family_arrange));
-  k_family_arrange<<<nfam, 256, smem, st>>>(res, hi, id, off, cnt);
+  k_family_arrange<<<nfam, 256, smem, st>>>(res, hi, id, off, cnt, cap);
 }
 
 void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,

@@ -190,7 +190,7 @@ void launch_arrange4(const uint64_t* res, const uint8_t* hi, const uint32_t* id,
 // Lays every B family (of at most kSortCap entries) out in lane slots of 32
 // entries with distinct residual classes mod 32 wherever the counts allow.
 void launch_family_arrange(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,
-                           const uint32_t* cnt, uint32_t nfam, cudaStream_t st);
+                           const uint32_t* cnt, uint32_t nfam, uint64_t mean_family, cudaStream_t st);
 // Sorts every family of one partitioned list (of at most kSortCap entries) by
 // the top `sb` bits of its sweep window, in place; larger families stay as they are.
 void launch_family_sort(uint64_t* res, uint8_t* hi, uint32_t* id, const uint32_t* off,

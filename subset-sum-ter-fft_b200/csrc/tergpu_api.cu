@@ -364,7 +364,7 @@ uint32_t enqueue_join(const JoinBuffers& b, const JoinWork& j, const Tuning& tu,
     x4view = ListView{b.res4, b.hi4, b.id4, b.off4, b.cnt4, b.win4};
   } else if (main_variant == 3 && j.count[1].cap != 0) {
     // B families in lane slots of distinct residual classes mod 32 (bank-free probes)
-    launch_family_arrange(b.res[1], b.hi[1], b.id[1], b.off[1], b.cnt[1], nfam, st);
+    launch_family_arrange(b.res[1], b.hi[1], b.id[1], b.off[1], b.cnt[1], nfam, j.count[1].cap >> tu.fb, st);
     *launches += 1;
   } else if (main_variant == 2 && j.count[1].cap != 0) {
     // B families sorted by the top filter-word bits of the full-width window
