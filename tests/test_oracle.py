@@ -78,3 +78,21 @@ def test_instance_generators(oracle_mod):
         if p[i]:
             acc += int(v[i][0])
     assert acc % (1 << 36) == int(t[0])
+
+
+def test_config3_goldens_cover_32_seeds(golden):
+    """Config 3's golden set, printed by the reference: 32 n=108 seeds (six
+    published, 26 fresh), each with its capture's three L1 checksums and frozen
+    ARWLF's 16-cell sample, and whole unplanted roots merged from cell slices
+    that cover all 4,096 cells."""
+    rows = golden["seed_roots"]
+    assert len(rows) == 32 and len({g["seed"] for g in rows}) == 32
+    assert sum(1 for g in rows if g["published"]) == 6
+    for g in rows:
+        assert len(g["checksums"]) == 3 and len(g["level1"]) == 3
+        assert g["arwlf16"]["projected_hits"] > 0
+    whole = [g for g in golden["whole_roots"] if "arwlf" in g]
+    assert whole
+    for g in whole:
+        assert g["arwlf"]["cells"] == 4096 and len(g["slice_rows"]) == g["slices"]
+        assert g["arwlf"]["pairs"] == g["level1"][0] * g["level1"][1]
