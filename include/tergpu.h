@@ -26,8 +26,9 @@ extern "C" {
  *    per-stage counters and output fingerprints, tergpu_attempt_out the run
  *    fingerprint and the level-3 time.
  * 4: tergpu_attempt_stats gained audited_stages (TERGPU_ATTEMPT_AUDIT).
+ * 5: tergpu_attempt_in gained planted_root (TERGPU_ATTEMPT_GUIDED).
  * Callers compiled against another version must not call in (the adapter checks). */
-#define TERGPU_ABI_VERSION 4
+#define TERGPU_ABI_VERSION 5
 
 enum tergpu_status {
   TERGPU_COMPLETED = 0,
@@ -292,6 +293,15 @@ typedef struct {
                                           TERGPU_INVARIANT_VIOLATION.  Runs stage by stage and
                                           reports the root as FullCanonicalOutput, as the
                                           reference's audit does */
+#define TERGPU_ATTEMPT_GUIDED 64u     /* the reference's GuidedPlanted targets
+                                          (TerTargetMode::GuidedPlanted, src/full_ter.cpp:
+                                          2281-2317, 2412-2428): planted_root, which must hold
+                                          n/4 ones in each half, is split into three level-1
+                                          and nine level-2 vectors, each half's ones dealt out
+                                          in order, and every attempt's targets are those
+                                          vectors' residues (masked to r1 / r2 bits) instead
+                                          of SplitMix64 draws; an unbalanced or missing
+                                          planted root is TERGPU_INVALID_CONFIGURATION */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return
@@ -315,6 +325,8 @@ typedef struct {
   int32_t device;
   uint32_t root_policy;        /* TERGPU_ROOT_POLICY_* (the numerics of ter::RootOutputPolicy,
                                   include/ter/full_ter.hpp:79-83) */
+  const uint8_t *planted_root; /* TERGPU_ATTEMPT_GUIDED: the instance's planted solution, n digits
+                                  of 0 or 1 (Instance::planted_root); NULL otherwise */
 } tergpu_attempt_in;
 
 /* tergpu_attempt_in.root_policy.  FirstWitness (the reference's default): the

@@ -13,7 +13,8 @@
 // A solve is one call of attempt_limit attempts on the reference's benchmark
 // instance (the planted support fixed to the first n/4 coordinates of each
 // half, bench/ter_full_bench.cpp:218-245).  --audit checks every stage whose
-// scalar oracle fits against it (TERGPU_ATTEMPT_AUDIT).  --fixture, --guided and
+// scalar oracle fits against it (TERGPU_ATTEMPT_AUDIT); --guided takes every
+// attempt's targets from the planted root (TERGPU_ATTEMPT_GUIDED).  --fixture and
 // --family=paper-rounded select reference paths the device does not implement;
 // they are refused with a message and exit status 2.
 #include "tergpu.h"
@@ -74,6 +75,7 @@ struct Options {
   bool preflight = false;
   bool require_found = false;
   bool audit = false;
+  bool guided = false;
   bool unsupported = false;
   std::string unsupported_what;
   uint32_t attempt_limit = 1;
@@ -130,7 +132,8 @@ int parse_options(int argc, char** argv, Options* o) {
     if (v == "--preflight") { o->preflight = true; continue; }
     if (v == "--require-found") { o->require_found = true; continue; }
     if (v == "--audit") { o->audit = true; continue; }
-    if (v == "--guided" || v == "--fixture") {
+    if (v == "--guided") { o->guided = true; continue; }
+    if (v == "--fixture") {
       o->unsupported = true;
       o->unsupported_what = std::string(v);
       continue;
@@ -257,6 +260,7 @@ struct Instance {
   uint32_t n = 0;
   std::vector<uint64_t> values;  // n * ceil(n/64) words
   std::vector<uint64_t> target;  // ceil(n/64) words
+  std::vector<uint8_t> planted;  // n digits: the planted root
 };
 
 Instance benchmark_instance(uint32_t n, uint64_t seed) {
@@ -278,9 +282,11 @@ Instance benchmark_instance(uint32_t n, uint64_t seed) {
     inst.values[i * w + w - 1] &= top_mask;
   }
   inst.target.assign(w, 0);
+  inst.planted.assign(n, 0);
   for (uint32_t half = 0; half < 2; ++half) {
     for (uint32_t off = 0; off < n / 4; ++off) {
       const uint32_t i = half * (n / 2) + off;
+      inst.planted[i] = 1;
       uint64_t carry = 0;
       for (uint32_t k = 0; k < w; ++k) {
         const uint64_t a = inst.target[k], b = inst.values[i * w + k];
@@ -351,7 +357,9 @@ Solve solve(const Options& o, const Instance& inst, uint64_t seed, uint64_t time
   in.memory_limit_bytes = o.memory_limit_bytes;
   in.cancel = &cancel;
   in.device = o.device;
-  in.flags = (telemetry ? TERGPU_ATTEMPT_TELEMETRY : 0u) | (o.audit ? TERGPU_ATTEMPT_AUDIT : 0u);
+  in.flags = (telemetry ? TERGPU_ATTEMPT_TELEMETRY : 0u) | (o.audit ? TERGPU_ATTEMPT_AUDIT : 0u) |
+             (o.guided ? TERGPU_ATTEMPT_GUIDED : 0u);
+  in.planted_root = o.guided ? inst.planted.data() : nullptr;
   // the reference's bench keeps FirstWitness (include/ter/full_ter.hpp:105)
   in.root_policy = TERGPU_ROOT_POLICY_FIRST_WITNESS;
   s.out.stats = s.stats.data();
@@ -388,7 +396,8 @@ void print_metadata(const Options& o, const std::string& command, uint64_t execu
             << " attempts_executed=" << executed << " warmup=" << o.warmup
             << " repeat=" << o.repeat << " time_limit_ms=" << o.time_limit_ms
             << " memory_limit_bytes=" << o.memory_limit_bytes << " seed=" << o.seed
-            << " execution_mode=FullTer target=Random audit=" << (o.audit ? "on" : "off")
+            << " execution_mode=FullTer target=" << (o.guided ? "GuidedPlanted" : "Random")
+            << " audit=" << (o.audit ? "on" : "off")
             << " family=FiniteSanity"
             << " command=\"" << command << "\"\n";
 }

@@ -101,6 +101,62 @@ Targets random_targets(uint64_t seed, uint32_t r1, uint32_t r2, u128 T) {
   return t;
 }
 
+// GuidedPlanted targets (TerTargetMode::GuidedPlanted): the planted root's
+// half-balanced decomposition (build_guided_tree, src/full_ter.cpp:2230-2317)
+// into three level-1 vectors -- in each half the root's ones, in coordinate
+// order, go n/12 to each child -- and nine level-2 vectors -- each level-1
+// vector's ones in each half go n/36 to each of its three children (FiniteSanity
+// shapes have no -1 digits, so the decomposition's other patterns are empty);
+// each target is its vector's residue masked to r1 or r2 bits (guided_targets,
+// src/full_ter.cpp:2412-2428).  False when the planted root is not binary with
+// n/4 ones in each half.
+bool guided_targets(const uint8_t* planted, uint32_t n, uint32_t r1, uint32_t r2, const uint64_t* values_le,
+                    Targets* t) {
+  if (planted == nullptr) return false;
+  const uint32_t w64 = (n + 63) / 64;
+  for (uint32_t half = 0; half < 2; ++half) {
+    uint32_t ones = 0;
+    for (uint32_t c = half * n / 2; c < (half + 1) * n / 2; ++c) {
+      if (planted[c] > 1) return false;
+      ones += planted[c];
+    }
+    if (ones != n / 4) return false;
+  }
+  // deal each half's set coordinates of `parent` out to three children, `per` each
+  auto split = [n](const std::vector<uint8_t>& parent, uint32_t per) {
+    std::array<std::vector<uint8_t>, 3> kids;
+    for (auto& k : kids) k.assign(n, 0);
+    for (uint32_t half = 0; half < 2; ++half) {
+      uint32_t seen = 0;
+      for (uint32_t c = half * n / 2; c < (half + 1) * n / 2; ++c) {
+        if (parent[c] == 0) continue;
+        kids[std::min<uint32_t>(seen / per, 2)][c] = 1;
+        ++seen;
+      }
+    }
+    return kids;
+  };
+  const u128 nm = mask128(n);
+  auto residue = [&](const std::vector<uint8_t>& v) {
+    u128 s = 0;
+    for (uint32_t c = 0; c < n; ++c) {
+      if (v[c] == 0) continue;
+      u128 w = values_le[c * w64];
+      if (w64 > 1) w |= (u128)values_le[c * w64 + 1] << 64;
+      s = (s + w) & nm;
+    }
+    return s;
+  };
+  const std::vector<uint8_t> root(planted, planted + n);
+  const auto l1 = split(root, n / 12);
+  for (int g = 0; g < 3; ++g) {
+    t->t1[g] = residue(l1[g]) & mask128(r1);
+    const auto l2 = split(l1[g], n / 36);
+    for (int k = 0; k < 3; ++k) t->t2[3 * g + k] = residue(l2[k]) & mask128(r2);
+  }
+  return true;
+}
+
 uint64_t binom_host(uint32_t m, uint32_t k) {
   if (k > m) return 0;
   uint64_t r = 1;
@@ -929,6 +985,13 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   u128 T = in->target_le[0];
   if (w64 > 1) T |= (u128)in->target_le[1] << 64;
   T &= nmask;
+  // GuidedPlanted: every attempt takes the planted root's targets
+  const bool guided = (in->flags & TERGPU_ATTEMPT_GUIDED) != 0;
+  Targets guided_tg{};
+  if (guided && !guided_targets(in->planted_root, n, r1, r2, in->values_le, &guided_tg)) {
+    t_error = "guided TER requires a planted binary root balanced across both halves";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
 
   Workspace& w = own != nullptr ? *own : workspace(in->device);
   std::lock_guard<std::mutex> lock(w.mu);
@@ -1019,7 +1082,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     tergpu_attempt_stats stat;
     std::memset(&stat, 0, sizeof stat);
     stat.attempt = attempt;
-    const Targets tg = random_targets(in->seed + attempt, r1, r2, T);
+    const Targets tg = guided ? guided_tg : random_targets(in->seed + attempt, r1, r2, T);
     RootOutcome root;
     bool graphed = false;
     if (plan != nullptr) {

@@ -37,7 +37,7 @@ STATUS_NAMES = {
 
 ROOT_COUNT_ONLY = 1
 ROOT_DEVICE_INPUTS = 2
-ABI_VERSION = 4  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
+ABI_VERSION = 5  # include/tergpu.h TERGPU_ABI_VERSION: the struct layouts below
 ROOT_SWEEP_V1 = 4
 ROOT_SWEEP_V2 = 8
 ROOT_AUTOTUNE = 16
@@ -53,6 +53,7 @@ ATTEMPT_PREFLIGHT = 2
 ATTEMPT_NO_GRAPH = 4
 ATTEMPT_TELEMETRY = 8
 ATTEMPT_AUDIT = 32
+ATTEMPT_GUIDED = 64
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _u32p = ctypes.POINTER(ctypes.c_uint32)

@@ -48,7 +48,7 @@ class AttemptIn(ctypes.Structure):
         ("seed", ctypes.c_uint64), ("attempt_first", ctypes.c_uint32),
         ("attempt_count", ctypes.c_uint32), ("memory_limit_bytes", ctypes.c_uint64),
         ("cancel", ctypes.POINTER(ctypes.c_int32)), ("device", ctypes.c_int32),
-        ("root_policy", ctypes.c_uint32),
+        ("root_policy", ctypes.c_uint32), ("planted_root", ctypes.POINTER(ctypes.c_uint8)),
     ]
 
 
@@ -80,6 +80,7 @@ class FullTerConfig:
     root_policy: int = _abi.ROOT_POLICY_FIRST_WITNESS
     telemetry: bool = False       # the reference's full telemetry: prefilter counts, fingerprints
     audit: bool = False           # FullTerConfig::audit: stages checked against the scalar oracles
+    guided: bool = False          # TerTargetMode::GuidedPlanted: targets from the planted root
 
 
 @dataclass
@@ -148,7 +149,11 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     ain.flags = ((_abi.ATTEMPT_CAPTURE_ONLY if config.capture_only else 0)
                  | (_abi.ATTEMPT_NO_GRAPH if config.no_graph else 0)
                  | (_abi.ATTEMPT_TELEMETRY if config.telemetry else 0)
-                 | (_abi.ATTEMPT_AUDIT if config.audit else 0))
+                 | (_abi.ATTEMPT_AUDIT if config.audit else 0)
+                 | (_abi.ATTEMPT_GUIDED if config.guided else 0))
+    planted = np.ascontiguousarray(instance.planted, dtype=np.uint8)
+    if config.guided:
+        ain.planted_root = planted.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
     ain.values_le = values.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.target_le = target.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     ain.seed = config.seed & (2**64 - 1)
@@ -161,7 +166,7 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     stats = (AttemptStats * max(1, config.attempt_limit))()
     out = AttemptOut()
     out.stats = ctypes.cast(stats, ctypes.POINTER(AttemptStats))
-    return ain, out, (values, target, stats)
+    return ain, out, (values, target, stats, planted)
 
 
 def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -> FullTerResult:
@@ -173,7 +178,7 @@ def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -
     lib = _abi.load()
     lib.tergpu_attempt_run.argtypes = [ctypes.POINTER(AttemptIn), ctypes.POINTER(AttemptOut)]
     lib.tergpu_attempt_run.restype = ctypes.c_int
-    ain, out, (_values, _target, stats) = make_request(instance, config, cancel)
+    ain, out, (_values, _target, stats, _planted) = make_request(instance, config, cancel)
     w64, w32 = (instance.n + 63) // 64, (instance.n + 31) // 32
     rb = 16 * w64 + 4 * w32
     bufs = []

@@ -3,11 +3,12 @@
 CPU: option handling and --preflight (no device work).  GPU: attempt-cost and
 time-to-found rows against the reference's attempts (golden fixtures),
 success-curve against the oracle, and the cooperative time limit."""
+import json
 import subprocess
 
 import pytest
 
-from conftest import ROOT
+from conftest import GOLDEN_DIR, ROOT
 
 CLI = ROOT / "subset-sum-ter-fft_b200" / "cli" / "tergpu_full_bench"
 ANCHOR_SEED = 19797034556212562  # ter_full_bench's default seed (0x46554c4c544552)
@@ -59,7 +60,7 @@ def test_preflight_refusals():
     (["--mode=success-curve", "--repeat=3"], 1, "--repeat does not apply"),
     (["--attempt-limit=0"], 1, "invalid --attempt-limit value"),
     (["--fixture"], 2, "does not implement"),
-    (["--guided"], 2, "does not implement"),
+    (["--fixture"], 2, "does not implement"),
     (["--family=paper-rounded"], 2, "does not implement"),
     (["--nonsense"], 1, "usage"),
 ])
@@ -101,14 +102,19 @@ SHARED_COLUMNS = (
 )
 
 
+_ROWS = len(json.loads((GOLDEN_DIR / "reference_golden.json").read_text())["full_bench_rows"])
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", range(5))
+@pytest.mark.parametrize("case", range(_ROWS))
 def test_row_matches_reference_ter_full_bench(golden, case):
     """The device row against the reference's own ter_full_bench row (built from
     bench/ter_full_bench.cpp): the same header, and every count column plus the
     telemetry fingerprint equal.  The n=72 0x7201 run is Found at attempt 21
     under FirstWitness, so its root counters stop at the reference's first
-    witness in its tiled visit order."""
+    witness in its tiled visit order.  The --guided rows take every attempt's
+    targets from the planted root (TerTargetMode::GuidedPlanted) and are Found at
+    attempt 0."""
     g = golden["full_bench_rows"][case]
     ref = csv_rows(g["header"] + "\n" + g["row"])[0]
     p = run(*g["args"], "--memory-limit-mib=65536", timeout=1200)
