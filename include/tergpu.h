@@ -26,7 +26,8 @@ extern "C" {
  *    per-stage counters and output fingerprints, tergpu_attempt_out the run
  *    fingerprint and the level-3 time.
  * 4: tergpu_attempt_stats gained audited_stages (TERGPU_ATTEMPT_AUDIT).
- * 5: tergpu_attempt_in gained planted_root (TERGPU_ATTEMPT_GUIDED).
+ * 5: tergpu_attempt_in gained planted_root (TERGPU_ATTEMPT_GUIDED) and fixture_level3_limit
+ *    (TERGPU_ATTEMPT_FIXTURE).
  * Callers compiled against another version must not call in (the adapter checks). */
 #define TERGPU_ABI_VERSION 5
 
@@ -302,6 +303,15 @@ typedef struct {
                                           vectors' residues (masked to r1 / r2 bits) instead
                                           of SplitMix64 draws; an unbalanced or missing
                                           planted root is TERGPU_INVALID_CONFIGURATION */
+#define TERGPU_ATTEMPT_FIXTURE 128u   /* the reference's FixtureTer execution
+                                          (TerExecutionMode::FixtureTer, src/full_ter.cpp:
+                                          2785-2845, 2319-2362): each level-3 half is its first
+                                          min(C(n/2, n/36), fixture_level3_limit) k-subsets in
+                                          enumeration order; with TERGPU_ATTEMPT_GUIDED the
+                                          halves of the nine guided level-2 vectors come first
+                                          and the first subsets fill up to the limit, in
+                                          canonical order (a limit below the guided halves is
+                                          TERGPU_RESOURCE_LIMIT).  Runs stage by stage */
 #define TERGPU_ATTEMPT_PREFLIGHT 2u    /* derive r1, r2, the level-3 size and the predicted
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return
@@ -327,6 +337,7 @@ typedef struct {
                                   include/ter/full_ter.hpp:79-83) */
   const uint8_t *planted_root; /* TERGPU_ATTEMPT_GUIDED: the instance's planted solution, n digits
                                   of 0 or 1 (Instance::planted_root); NULL otherwise */
+  uint64_t fixture_level3_limit; /* TERGPU_ATTEMPT_FIXTURE: level-3 entries per half (> 0) */
 } tergpu_attempt_in;
 
 /* tergpu_attempt_in.root_policy.  FirstWitness (the reference's default): the

@@ -14,9 +14,10 @@
 // instance (the planted support fixed to the first n/4 coordinates of each
 // half, bench/ter_full_bench.cpp:218-245).  --audit checks every stage whose
 // scalar oracle fits against it (TERGPU_ATTEMPT_AUDIT); --guided takes every
-// attempt's targets from the planted root (TERGPU_ATTEMPT_GUIDED).  --fixture and
-// --family=paper-rounded select reference paths the device does not implement;
-// they are refused with a message and exit status 2.
+// attempt's targets from the planted root (TERGPU_ATTEMPT_GUIDED); --fixture and
+// --fixture-limit=<n> keep the first n level-3 subsets of each half
+// (TERGPU_ATTEMPT_FIXTURE).  --family=paper-rounded selects a reference path the
+// device does not implement; it is refused with a message and exit status 2.
 #include "tergpu.h"
 
 #include <algorithm>
@@ -76,6 +77,8 @@ struct Options {
   bool require_found = false;
   bool audit = false;
   bool guided = false;
+  bool fixture = false;
+  uint64_t fixture_limit = 64;  // the reference's kDefaultFixtureLevel3Limit
   bool unsupported = false;
   std::string unsupported_what;
   uint32_t attempt_limit = 1;
@@ -133,14 +136,13 @@ int parse_options(int argc, char** argv, Options* o) {
     if (v == "--require-found") { o->require_found = true; continue; }
     if (v == "--audit") { o->audit = true; continue; }
     if (v == "--guided") { o->guided = true; continue; }
-    if (v == "--fixture") {
-      o->unsupported = true;
-      o->unsupported_what = std::string(v);
-      continue;
-    }
+    if (v == "--fixture") { o->fixture = true; continue; }
     if (has_prefix("--fixture-limit=")) {
-      o->unsupported = true;
-      o->unsupported_what = "--fixture-limit";
+      if (!value_of("--fixture-limit=", &x) || x == 0) {
+        std::cerr << "invalid --fixture-limit value\n";
+        return 1;
+      }
+      o->fixture_limit = x;
       continue;
     }
     if (has_prefix("--family=")) {
@@ -358,8 +360,9 @@ Solve solve(const Options& o, const Instance& inst, uint64_t seed, uint64_t time
   in.cancel = &cancel;
   in.device = o.device;
   in.flags = (telemetry ? TERGPU_ATTEMPT_TELEMETRY : 0u) | (o.audit ? TERGPU_ATTEMPT_AUDIT : 0u) |
-             (o.guided ? TERGPU_ATTEMPT_GUIDED : 0u);
+             (o.guided ? TERGPU_ATTEMPT_GUIDED : 0u) | (o.fixture ? TERGPU_ATTEMPT_FIXTURE : 0u);
   in.planted_root = o.guided ? inst.planted.data() : nullptr;
+  in.fixture_level3_limit = o.fixture ? o.fixture_limit : 0;
   // the reference's bench keeps FirstWitness (include/ter/full_ter.hpp:105)
   in.root_policy = TERGPU_ROOT_POLICY_FIRST_WITNESS;
   s.out.stats = s.stats.data();
@@ -396,7 +399,8 @@ void print_metadata(const Options& o, const std::string& command, uint64_t execu
             << " attempts_executed=" << executed << " warmup=" << o.warmup
             << " repeat=" << o.repeat << " time_limit_ms=" << o.time_limit_ms
             << " memory_limit_bytes=" << o.memory_limit_bytes << " seed=" << o.seed
-            << " execution_mode=FullTer target=" << (o.guided ? "GuidedPlanted" : "Random")
+            << " execution_mode=" << (o.fixture ? "FixtureTer" : "FullTer")
+            << " target=" << (o.guided ? "GuidedPlanted" : "Random")
             << " audit=" << (o.audit ? "on" : "off")
             << " family=FiniteSanity"
             << " command=\"" << command << "\"\n";
@@ -405,7 +409,8 @@ void print_metadata(const Options& o, const std::string& command, uint64_t execu
 int run_preflight(const Options& o) {
   tergpu_attempt_in in{};
   in.n = o.n;
-  in.flags = TERGPU_ATTEMPT_PREFLIGHT;
+  in.flags = TERGPU_ATTEMPT_PREFLIGHT | (o.fixture ? TERGPU_ATTEMPT_FIXTURE : 0u);
+  in.fixture_level3_limit = o.fixture ? o.fixture_limit : 0;
   in.memory_limit_bytes = o.memory_limit_bytes;
   in.device = o.device;
   tergpu_attempt_out out{};
@@ -435,7 +440,7 @@ int run_preflight(const Options& o) {
             << '\n';
   std::cout << "  predicted_device_bytes=" << out.device_bytes << '\n';
   std::cout << "  memory_limit_bytes=" << o.memory_limit_bytes << '\n';
-  std::cout << "  execution_mode=FullTer\n";
+  std::cout << "  execution_mode=" << (o.fixture ? "FixtureTer" : "FullTer") << '\n';
   std::cout << "  pair_materializing_fallback=no\n";
   if (st == TERGPU_RESOURCE_LIMIT) {
     std::cout << "  VERDICT: ResourceLimit (predicted device bytes exceed the ceiling)\n";

@@ -111,7 +111,7 @@ Targets random_targets(uint64_t seed, uint32_t r1, uint32_t r2, u128 T) {
 // src/full_ter.cpp:2412-2428).  False when the planted root is not binary with
 // n/4 ones in each half.
 bool guided_targets(const uint8_t* planted, uint32_t n, uint32_t r1, uint32_t r2, const uint64_t* values_le,
-                    Targets* t) {
+                    Targets* t, std::vector<std::vector<uint8_t>>* level2 = nullptr) {
   if (planted == nullptr) return false;
   const uint32_t w64 = (n + 63) / 64;
   for (uint32_t half = 0; half < 2; ++half) {
@@ -152,7 +152,10 @@ bool guided_targets(const uint8_t* planted, uint32_t n, uint32_t r1, uint32_t r2
   for (int g = 0; g < 3; ++g) {
     t->t1[g] = residue(l1[g]) & mask128(r1);
     const auto l2 = split(l1[g], n / 36);
-    for (int k = 0; k < 3; ++k) t->t2[3 * g + k] = residue(l2[k]) & mask128(r2);
+    for (int k = 0; k < 3; ++k) {
+      t->t2[3 * g + k] = residue(l2[k]) & mask128(r2);
+      if (level2 != nullptr) level2->push_back(l2[k]);
+    }
   }
   return true;
 }
@@ -964,7 +967,14 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   }
   const uint32_t w64 = (n + 63) / 64, w32 = (n + 31) / 32;
   const u128 nmask = mask128(n);
-  const uint64_t l3 = binom_host(n / 2, n / 36);
+  // FixtureTer: each level-3 half is its first fixture_level3_limit subsets
+  const bool fixture = (in->flags & TERGPU_ATTEMPT_FIXTURE) != 0;
+  if (fixture && in->fixture_level3_limit == 0) {
+    t_error = "level-3 generation configuration is invalid";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
+  const uint64_t l3 = fixture ? std::min<uint64_t>(binom_host(n / 2, n / 36), in->fixture_level3_limit)
+                              : binom_host(n / 2, n / 36);
   out->level3_size = l3;
 
   // Preflight against the ceiling, from the expected level sizes (2x margin).
@@ -988,7 +998,8 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   // GuidedPlanted: every attempt takes the planted root's targets
   const bool guided = (in->flags & TERGPU_ATTEMPT_GUIDED) != 0;
   Targets guided_tg{};
-  if (guided && !guided_targets(in->planted_root, n, r1, r2, in->values_le, &guided_tg)) {
+  std::vector<std::vector<uint8_t>> guided_l2;
+  if (guided && !guided_targets(in->planted_root, n, r1, r2, in->values_le, &guided_tg, &guided_l2)) {
     t_error = "guided TER requires a planted binary root balanced across both halves";
     return TERGPU_INVALID_CONFIGURATION;
   }
@@ -1040,7 +1051,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   }
   const auto t_l3 = std::chrono::steady_clock::now();
   GraphPlan* plan = nullptr;
-  if (!exporting && !telemetry && !audit && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
+  if (!exporting && !telemetry && !audit && !fixture && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {
     plan = graph_plan(w, n, r1, r2, l3, st);
     held.plan = plan;
     if (plan != nullptr) graph_level3(*plan, weights, st);
@@ -1058,6 +1069,54 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     right = entry_slot(w, S_L3 + 4, l3);
     launch_enumerate_half(d_weights, n, 0, l3, left, st);
     launch_enumerate_half(d_weights, n, 1, l3, right, st);
+    if (fixture && guided) {
+      // the guided level-2 vectors' halves first, then the first subsets up to
+      // the limit (include_guided_halves, src/full_ter.cpp:2319-2362)
+      for (int side = 0; side < 2; ++side) {
+        const EntryArrays& dst = side == 0 ? left : right;
+        const std::vector<HostEntry> original = host_entries(w, dst, l3, st);
+        std::vector<HostEntry> keep;
+        for (const auto& leaf : guided_l2) {
+          HostEntry e{0, 0, 0};
+          for (uint32_t c = side * n / 2; c < (side + 1) * n / 2; ++c) {
+            if (leaf[c] == 0) continue;
+            if (c < 64) e.p0 |= 1ull << c; else e.p1 |= 1ull << (c - 64);
+            u128 wgt = weights[2 * c];
+            wgt |= (u128)weights[2 * c + 1] << 64;
+            e.res = (e.res + wgt) & nmask;
+          }
+          keep.push_back(e);
+        }
+        keep = canonical_entries(std::move(keep));
+        if (keep.size() > in->fixture_level3_limit) {
+          t_error = "fixture limit is too small for guided level-3 halves";
+          throw Failure{TERGPU_RESOURCE_LIMIT};
+        }
+        for (const HostEntry& cand : original) {
+          if (keep.size() >= in->fixture_level3_limit) break;
+          if (!std::binary_search(keep.begin(), keep.end(), cand)) {
+            keep.push_back(cand);
+            std::sort(keep.begin(), keep.end());
+          }
+        }
+        if (keep.size() != l3) {
+          t_error = "guided fixture halves disagree in size";
+          throw Failure{TERGPU_INVARIANT_VIOLATION};
+        }
+        std::vector<uint64_t> a(l3), b(l3), c(l3), d(l3);
+        for (uint64_t i = 0; i < l3; ++i) {
+          a[i] = keep[i].p0;
+          b[i] = keep[i].p1;
+          c[i] = (uint64_t)keep[i].res;
+          d[i] = (uint64_t)(keep[i].res >> 64);
+        }
+        check(cudaMemcpyAsync(dst.pos0, a.data(), l3 * 8, cudaMemcpyHostToDevice, st), "fixture upload");
+        check(cudaMemcpyAsync(dst.pos1, b.data(), l3 * 8, cudaMemcpyHostToDevice, st), "fixture upload");
+        check(cudaMemcpyAsync(dst.res_lo, c.data(), l3 * 8, cudaMemcpyHostToDevice, st), "fixture upload");
+        check(cudaMemcpyAsync(dst.res_hi, d.data(), l3 * 8, cudaMemcpyHostToDevice, st), "fixture upload");
+        sync_stream(w, st, "fixture upload");
+      }
+    }
     const uint32_t nbk = 1u << r2;
     uint32_t* bcnt = ensure<uint32_t>(w, S_BCNT, (nbk + 16) * 4ull);
     boff = ensure<uint32_t>(w, S_BOFF, (nbk + 16) * 4ull);

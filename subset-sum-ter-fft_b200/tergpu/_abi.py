@@ -54,6 +54,7 @@ ATTEMPT_NO_GRAPH = 4
 ATTEMPT_TELEMETRY = 8
 ATTEMPT_AUDIT = 32
 ATTEMPT_GUIDED = 64
+ATTEMPT_FIXTURE = 128
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _u32p = ctypes.POINTER(ctypes.c_uint32)

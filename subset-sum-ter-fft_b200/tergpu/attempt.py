@@ -49,6 +49,7 @@ class AttemptIn(ctypes.Structure):
         ("attempt_count", ctypes.c_uint32), ("memory_limit_bytes", ctypes.c_uint64),
         ("cancel", ctypes.POINTER(ctypes.c_int32)), ("device", ctypes.c_int32),
         ("root_policy", ctypes.c_uint32), ("planted_root", ctypes.POINTER(ctypes.c_uint8)),
+        ("fixture_level3_limit", ctypes.c_uint64),
     ]
 
 
@@ -81,6 +82,7 @@ class FullTerConfig:
     telemetry: bool = False       # the reference's full telemetry: prefilter counts, fingerprints
     audit: bool = False           # FullTerConfig::audit: stages checked against the scalar oracles
     guided: bool = False          # TerTargetMode::GuidedPlanted: targets from the planted root
+    fixture_limit: int = 0        # > 0: TerExecutionMode::FixtureTer with this level-3 limit
 
 
 @dataclass
@@ -150,7 +152,9 @@ def make_request(instance, config: FullTerConfig, cancel=None):
                  | (_abi.ATTEMPT_NO_GRAPH if config.no_graph else 0)
                  | (_abi.ATTEMPT_TELEMETRY if config.telemetry else 0)
                  | (_abi.ATTEMPT_AUDIT if config.audit else 0)
-                 | (_abi.ATTEMPT_GUIDED if config.guided else 0))
+                 | (_abi.ATTEMPT_GUIDED if config.guided else 0)
+                 | (_abi.ATTEMPT_FIXTURE if config.fixture_limit else 0))
+    ain.fixture_level3_limit = config.fixture_limit
     planted = np.ascontiguousarray(instance.planted, dtype=np.uint8)
     if config.guided:
         ain.planted_root = planted.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))

@@ -302,14 +302,19 @@ def full_bench_rows(tmp: Path):
     """The reference's own ter_full_bench (bench/ter_full_bench.cpp, built from its
     sources into oracle/_ref/ter_full_bench): its CSV header and row for the
     device command line to reproduce, with random and with guided (planted-root)
-    targets."""
+    targets, complete (FullTer) and truncated (FixtureTer) level-3 lists."""
     import subprocess
 
     binary = HERE.parent.parent / "oracle" / "_ref" / "ter_full_bench"
     out = []
     for n, seed, limit, extra in ((36, ANCHOR_SEED, 8, []), (36, 0x1001, 8, []), (36, 0x2A, 8, []),
                                   (72, ANCHOR_SEED, 1, []), (72, 0x7201, 22, []),
-                                  (36, ANCHOR_SEED, 2, ["--guided"]), (72, ANCHOR_SEED, 1, ["--guided"])):
+                                  (36, ANCHOR_SEED, 2, ["--guided"]), (72, ANCHOR_SEED, 1, ["--guided"]),
+                                  (36, ANCHOR_SEED, 2, ["--fixture"]),
+                                  (72, ANCHOR_SEED, 2, ["--fixture", "--fixture-limit=200"]),
+                                  (72, ANCHOR_SEED, 2, ["--fixture", "--fixture-limit=100", "--guided"]),
+                                  (108, 0x1001, 2, ["--fixture", "--fixture-limit=1500"]),
+                                  (108, 0x1001, 2, ["--fixture", "--fixture-limit=600", "--guided"])):
         args = [f"--n={n}", f"--seed={seed}", f"--attempt-limit={limit}", "--warmup=0", "--repeat=1", *extra]
         proc = subprocess.run([str(binary), *args], capture_output=True, text=True, timeout=1800)
         if proc.returncode != 0:
