@@ -59,8 +59,7 @@ def test_preflight_refusals():
     (["--mode=bogus"], 1, "invalid --mode value"),
     (["--mode=success-curve", "--repeat=3"], 1, "--repeat does not apply"),
     (["--attempt-limit=0"], 1, "invalid --attempt-limit value"),
-    (["--fixture"], 2, "does not implement"),
-    (["--fixture"], 2, "does not implement"),
+    (["--fixture-limit=0"], 1, "invalid --fixture-limit value"),
     (["--family=paper-rounded"], 2, "does not implement"),
     (["--nonsense"], 1, "usage"),
 ])
