@@ -1494,7 +1494,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     f.mix(in->seed);
     f.mix(n);
     f.mix(n);  // modulus bits: the full TER modulus is 2^n
-    f.mix(0);  // TerExecutionMode::FullTer
+    f.mix(fixture ? 1 : 0);  // TerExecutionMode: FullTer 0, FixtureTer 1 (include/ter/types.hpp:25-28)
     f.mix(0);  // ShapeFamily::FiniteSanity
     f.mix(r1);
     f.mix(r2);
