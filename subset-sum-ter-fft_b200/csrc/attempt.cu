@@ -926,7 +926,7 @@ bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, uint32
   stat->l3_survivors = c.bounds[9];
   stat->l2_modular = c.l2_triples[0] + c.l2_triples[1] + c.l2_triples[2];
   for (int grp = 0; grp < 3; ++grp) {
-    stat->l2_pairs += c.kept9[3 * grp] * c.kept9[3 * grp + 1];
+    if (c.kept9[3 * grp + 2] != 0) stat->l2_pairs += c.kept9[3 * grp] * c.kept9[3 * grp + 1];
     stat->l2_structural_rejects += c.l1rej[grp][0];
     stat->l2_distribution_rejects += c.l1rej[grp][1];
     stat->l2_survivors += c.ncand[grp];
@@ -1262,7 +1262,9 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
       unsigned long long lc[4] = {0, 0, 0, 0};  // kept, (unused), structural, distribution rejects
       download(w, lc, acc + 4, 4, st);
       const unsigned long long ncand = lc[0];
-      stat.l2_pairs += l2n[3 * g] * l2n[3 * g + 1];
+      // the reference's ternary merge counts nothing when a list is empty
+      // (src/full_ter.cpp:1153-1156)
+      if (l2n[3 * g + 2] != 0) stat.l2_pairs += l2n[3 * g] * l2n[3 * g + 1];
       stat.l2_structural_rejects += lc[2];
       stat.l2_distribution_rejects += lc[3];
       stat.l2_survivors += ncand;
@@ -1453,6 +1455,18 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     if (telemetry) {
       stat.root_full_quotient_rejects = stat.root_low_prefilter - stat.root_modular;
       stat.l0_fingerprint = l0_fingerprint(n, parents, T);
+    }
+    if (stat.level1_sizes[0] == 0 || stat.level1_sizes[1] == 0 || stat.level1_sizes[2] == 0) {
+      // the reference's tiled root returns before it records anything when a
+      // level-1 list is empty (src/full_ter.cpp:1644-1647): its stage telemetry
+      // keeps its defaults, FullCanonicalOutput among them
+      stat.root_pairs = 0;
+      stat.root_quotient_bits = 0;
+      stat.root_prefilter_bits = 0;
+      stat.root_low_prefilter = 0;
+      stat.root_full_quotient_rejects = 0;
+      stat.root_policy = TERGPU_ROOT_POLICY_FULL_CANONICAL;
+      stat.root_early_stopped = 0;
     }
     stat.level0_size = parents.size();
     stat.status = parents.empty() ? TERGPU_NO_WITNESS_THIS_ATTEMPT : TERGPU_FOUND;
