@@ -52,6 +52,7 @@ ATTEMPT_CAPTURE_ONLY = 1
 ATTEMPT_PREFLIGHT = 2
 ATTEMPT_NO_GRAPH = 4
 ATTEMPT_TELEMETRY = 8
+ATTEMPT_BACKGROUND = 16
 ATTEMPT_AUDIT = 32
 ATTEMPT_GUIDED = 64
 ATTEMPT_FIXTURE = 128

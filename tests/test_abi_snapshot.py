@@ -23,6 +23,22 @@ def test_library_exports_every_declared_symbol():
     assert lib.tergpu_abi_version() == int(version)
 
 
+def test_python_constants_mirror_every_header_value():
+    """Every flag, limit and status value of include/tergpu.h has a constant of
+    the same name (less the TERGPU_ prefix) and value in tergpu._abi."""
+    from tergpu import _abi
+
+    header = (ROOT / "include" / "tergpu.h").read_text()
+    values = {m.group(1): int(m.group(2))
+              for m in re.finditer(r"^#define TERGPU_(\w+) (\d+)u?\b", header, flags=re.M)}
+    enum = re.search(r"enum tergpu_status \{(.*?)\};", header, flags=re.S).group(1)
+    values.update((m.group(1), int(m.group(2)))
+                  for m in re.finditer(r"TERGPU_(\w+) = (\d+)", enum))
+    assert len(values) > 30 and "ATTEMPT_FIXTURE" in values and "INVALID_INPUT" in values
+    for name, value in values.items():
+        assert getattr(_abi, name, None) == value, name
+
+
 def test_ctypes_structs_match_the_c_layout(tmp_path):
     """Every ctypes mirror has the C struct's size and field offsets (a C probe
     compiled against include/tergpu.h prints them)."""
