@@ -96,3 +96,28 @@ def test_config3_goldens_cover_32_seeds(golden):
     for g in whole:
         assert g["arwlf"]["cells"] == 4096 and len(g["slice_rows"]) == g["slices"]
         assert g["arwlf"]["pairs"] == g["level1"][0] * g["level1"][1]
+
+
+def test_wide_quotient_truncation_fixture(oracle_mod):
+    """The reference's Q = 69 known answer (tests/full_ter_tests.cpp:805-838):
+    the two A entries agree on the low 64 quotient bits, so a truncated window
+    cannot separate them; the full 69-bit join keeps only the arithmetic root,
+    whose residue sum equals the root target and whose parent has the root shape."""
+    from conftest import wide_quotient_capture
+    from tergpu import snapshot
+
+    snap = wide_quotient_capture()
+    Q, lo, hi, tau = snapshot.root_keys(snap)
+    assert Q == 69 and tau == 0
+    assert lo[0].tolist() == [0, 0] and hi[0].tolist() == [0, 1]
+    assert oracle_mod.projected_count(32, lo) == 2
+    digest, trip = oracle_mod.root_join(Q, lo, hi, capacity=16)
+    assert digest["triples"] == 1 and trip.tolist() == [[0, 0, 0]]
+    mod = 1 << snap.n
+    target = snapshot.words_to_int(snap.root_target)
+    for a, accepted in ((0, True), (1, False)):
+        total = sum(snapshot.words_to_int(snap.residues(l)[i]) for l, i in ((0, a), (1, 0), (2, 0)))
+        assert (total % mod == target) is accepted
+    pos = [snap.masks(l)[0][0] for l in range(3)]
+    parent = [int(pos[0][k]) | int(pos[1][k]) | int(pos[2][k]) for k in range(snap.words64)]
+    assert sum(bin(w).count("1") for w in parent) == snap.n // 2
