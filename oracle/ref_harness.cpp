@@ -5,10 +5,12 @@
 // against it, and so bench.py can time the reference's CPU backends on the same
 // host.  Every line of output is one JSON object.
 //
-//   terref solve N SEED ATTEMPTS KIND POLICY AUDIT
+//   terref solve N SEED ATTEMPTS KIND POLICY AUDIT [CONFIG_SEED [MODES]]
 //       solve_full_ter (src/full_ter.cpp:3867) on authentic_instance (KIND=auth)
 //       or build_instance(n, 10, seed) (KIND=build); per-attempt level sizes,
-//       root accounting and the witness.
+//       root accounting and the witness.  CONFIG_SEED (default SEED, "-" keeps
+//       it) seeds the targets; MODES "guided", "fixture=<limit>" or both
+//       (comma-separated) select GuidedPlanted targets and FixtureTer level 3.
 //   terref capture N SEED ATTEMPT KIND OUT
 //       root_snapshot::capture_to_file (ter2_root/frozen/ter_root_snapshot.cpp:124).
 //   terref snaproot SNAP BACKEND CELLS PROJ
@@ -114,7 +116,19 @@ int cmd_solve(int argc, char** argv) {
   const std::string policy = argv[6];
   const bool audit = std::string(argv[7]) == "1";
   const ter::Instance instance = make_instance(n, seed, kind);
-  ter::FullTerConfig config = rg::authentic_config(seed);
+  // optional: the config seed when it differs from the instance seed ("-" keeps
+  // it), and the modes "guided", "fixture=<limit>" or "guided,fixture=<limit>"
+  const std::uint64_t config_seed =
+      argc > 8 && std::string(argv[8]) != "-" ? std::strtoull(argv[8], nullptr, 0) : seed;
+  ter::FullTerConfig config = rg::authentic_config(config_seed);
+  const std::string modes = argc > 9 ? argv[9] : "";
+  if (modes.find("guided") != std::string::npos) {
+    config.target_mode = ter::TerTargetMode::GuidedPlanted;
+  }
+  if (const auto at = modes.find("fixture="); at != std::string::npos) {
+    config.execution_mode = ter::TerExecutionMode::FixtureTer;
+    config.fixture_level3_limit = std::strtoull(modes.c_str() + at + 8, nullptr, 0);
+  }
   config.attempt_limit = attempts;
   config.audit = audit;
   config.root_output_policy = policy == "canon" ? ter::RootOutputPolicy::FullCanonicalOutput

@@ -298,6 +298,21 @@ def attempt_telemetry(tmp: Path):
     return out
 
 
+def guided_replay(tmp: Path):
+    """The reference's guided pipeline test (tests/full_ter_tests.cpp:236-330):
+    its balanced n=36 instance (seed 0x544552F, the benchmark instance) solved
+    with config seed 91 and GuidedPlanted targets, audited, under FullTer and
+    under FixtureTer with level-3 limit 9; plus the FullTer run without the
+    audit under FirstWitness.  Every stage's telemetry and the run fingerprint."""
+    out = []
+    for modes, policy, audit in (("guided", "first", 1), ("guided,fixture=9", "first", 1),
+                                 ("guided", "first", 0)):
+        rows = O.ref_run("solve", 36, 0x544552F, 1, "auth", policy, audit, 91, modes)
+        out.append({"n": 36, "seed": 0x544552F, "config_seed": 91, "modes": modes, "policy": policy,
+                    "audit": audit, "rows": rows[:-1], "final": rows[-1]})
+    return out
+
+
 def full_bench_rows(tmp: Path):
     """The reference's own ter_full_bench (bench/ter_full_bench.cpp, built from its
     sources into oracle/_ref/ter_full_bench): its CSV header and row for the
@@ -359,6 +374,7 @@ SECTIONS = {
     "seed_roots": seed_roots,
     "whole_roots": whole_roots,
     "attempt_telemetry": attempt_telemetry,
+    "guided_replay": guided_replay,
     "full_bench_rows": full_bench_rows,
     "published_runs": published_runs,
 }

@@ -122,6 +122,44 @@ def test_audit_mode_checks_every_stage_and_matches_reference(golden, case):
                 assert a[dev_key] == want, (g["n"], g["seed"], row["attempt"], stage, ref_key)
 
 
+@pytest.mark.parametrize("case", range(3))
+def test_guided_pipeline_and_replay_match_reference(golden, case):
+    """The reference's guided pipeline test (tests/full_ter_tests.cpp:236-330) on
+    the device: its balanced n=36 instance (seed 0x544552F) with config seed 91
+    and GuidedPlanted targets, audited (the reference's default) under FullTer
+    and under FixtureTer with level-3 limit 9, and without the audit under
+    FirstWitness.  Found with the reference's witness, every stage counter, stage
+    fingerprint and run fingerprint equal to the reference's; a second identical
+    call replays the witness and the fingerprint exactly."""
+    from tergpu import _abi, attempt, instance
+
+    g = golden["guided_replay"][case]
+    inst = instance.benchmark_instance(g["n"], g["seed"])
+    fixture = int(g["modes"].split("fixture=")[1]) if "fixture=" in g["modes"] else 0
+    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=1, guided=True,
+                                fixture_limit=fixture, audit=bool(g["audit"]), telemetry=True,
+                                memory_limit_bytes=64 << 20)
+    first = attempt.solve_full_ter(inst, cfg)
+    final = g["final"]
+    assert first.status == final["status"] == _abi.FOUND, (first.status_name, _abi.last_error())
+    assert "".join(str(int(d)) for d in first.witness) == final["witness"]
+    assert instance.verify_witness(inst, first.witness)
+    assert first.fingerprint == hexint(final["fingerprint"]), g["modes"]
+    assert first.level3_size == final["l3"][0]
+    (a,), (row,) = first.attempts, g["rows"]
+    assert a["attempt_seed"] == row["seed"] and a["status"] == row["status"]
+    assert a["level2"] == row["level2"] and a["level1"] == row["level1"] and a["level0"] == row["level0"]
+    for stage, fields in STAGES.items():
+        for ref_key, dev_key in fields.items():
+            want = row[stage][ref_key]
+            want = hexint(want) if ref_key == "fingerprint" else want
+            assert a[dev_key] == want, (g["modes"], g["audit"], stage, ref_key, a[dev_key], want)
+    assert a["audited_stages"] == (13 if g["audit"] else 0)
+    second = attempt.solve_full_ter(inst, cfg)
+    assert second.status == first.status and second.fingerprint == first.fingerprint
+    assert np.array_equal(second.witness, first.witness)
+
+
 def test_n36_attempt_loop_stops_like_the_reference(golden):
     """The whole loop in one call: the reference's final status and attempt count."""
     from tergpu import _abi

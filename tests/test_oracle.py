@@ -121,3 +121,29 @@ def test_wide_quotient_truncation_fixture(oracle_mod):
     pos = [snap.masks(l)[0][0] for l in range(3)]
     parent = [int(pos[0][k]) | int(pos[1][k]) | int(pos[2][k]) for k in range(snap.words64)]
     assert sum(bin(w).count("1") for w in parent) == snap.n // 2
+
+
+def test_witness_verification_fails_closed(golden):
+    """verify_full_ter_witness's refusals as the reference's guided test checks
+    them (tests/full_ter_tests.cpp:331-350), on the witness the reference found
+    for its balanced n=36 instance (seed 0x544552F, the benchmark instance): a
+    -1 digit, one selected item dropped, and the target's lowest bit flipped are
+    each refused; the witness itself is the planted support."""
+    import dataclasses
+
+    from tergpu import instance
+
+    g = golden["guided_replay"][0]
+    inst = instance.benchmark_instance(g["n"], g["seed"])
+    witness = [int(c) for c in g["final"]["witness"]]
+    assert witness == inst.planted.tolist()
+    assert instance.verify_witness(inst, witness)
+    negative = list(witness)
+    negative[0] = -1
+    assert not instance.verify_witness(inst, negative)
+    light = list(witness)
+    light[light.index(1)] = 0
+    assert not instance.verify_witness(inst, light)
+    target = inst.target_le.copy()
+    target[0] ^= 1
+    assert not instance.verify_witness(dataclasses.replace(inst, target_le=target), witness)
