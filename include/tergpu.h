@@ -346,8 +346,11 @@ typedef struct {
  * the prefilter buckets, bucket i of A, then A's and B's EntryIds, then C's
  * EntryId descending); that triple's parent is the witness and the root's
  * counters stop there.  FullCanonicalOutput: every valid parent, sorted and
- * deduplicated; the witness is the first of them.  CountOnly: valid roots are
- * counted, none is retained (no witness). */
+ * deduplicated; the witness is the first of them.  CountOnly is refused with
+ * TERGPU_INVALID_CONFIGURATION before any work, as solve_full_ter refuses it (a
+ * SAT result must keep a verifiable witness; src/full_ter.cpp:2945-2957): the
+ * root reports count without retaining (report_full_ter_root /
+ * count_full_ter_root over tergpu_root_run_records). */
 #define TERGPU_ROOT_POLICY_FIRST_WITNESS 0u
 #define TERGPU_ROOT_POLICY_COUNT_ONLY 1u
 #define TERGPU_ROOT_POLICY_FULL_CANONICAL 2u

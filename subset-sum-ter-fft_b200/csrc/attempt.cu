@@ -951,6 +951,13 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     t_error = "full TER on the device requires n in {36, 72, 108}";
     return TERGPU_INVALID_CONFIGURATION;
   }
+  // solve_full_ter refuses CountOnly, since a SAT result must keep a verifiable
+  // witness (src/full_ter.cpp:2945-2957); the root reports count instead
+  if (in->root_policy != TERGPU_ROOT_POLICY_FIRST_WITNESS &&
+      in->root_policy != TERGPU_ROOT_POLICY_FULL_CANONICAL) {
+    t_error = "root_policy must be FirstWitness (0) or FullCanonicalOutput (2); solve_full_ter refuses CountOnly";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
   const bool preflight = (in->flags & TERGPU_ATTEMPT_PREFLIGHT) != 0;
   if (!preflight &&
       (in->values_le == nullptr || in->target_le == nullptr || in->attempt_count == 0)) {
@@ -1045,10 +1052,6 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   // root then reports FullCanonicalOutput, as the reference's audit does)
   const bool audit = (in->flags & TERGPU_ATTEMPT_AUDIT) != 0;
   const uint32_t policy = audit ? TERGPU_ROOT_POLICY_FULL_CANONICAL : in->root_policy;
-  if (in->root_policy > TERGPU_ROOT_POLICY_FULL_CANONICAL) {
-    t_error = "root_policy must be FirstWitness (0), CountOnly (1) or FullCanonicalOutput (2)";
-    return TERGPU_INVALID_CONFIGURATION;
-  }
   const auto t_l3 = std::chrono::steady_clock::now();
   GraphPlan* plan = nullptr;
   if (!exporting && !telemetry && !audit && !fixture && (in->flags & TERGPU_ATTEMPT_NO_GRAPH) == 0) {

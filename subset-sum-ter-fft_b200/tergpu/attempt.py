@@ -173,6 +173,24 @@ def make_request(instance, config: FullTerConfig, cancel=None):
     return ain, out, (values, target, stats, planted)
 
 
+def preflight(instance, config: FullTerConfig | None = None) -> FullTerResult:
+    """The checks and prediction solve_full_ter makes before any device work, as
+    ter_full_bench --preflight reports them (bench/ter_full_bench.cpp:594-680):
+    r1, r2, the level-3 size per half and the predicted device bytes with status
+    Completed, or the refusal the call would return (InvalidConfiguration,
+    ResourceLimit against memory_limit_bytes).  Touches no device."""
+    config = config or FullTerConfig()
+    lib = _abi.load()
+    lib.tergpu_attempt_run.argtypes = [ctypes.POINTER(AttemptIn), ctypes.POINTER(AttemptOut)]
+    lib.tergpu_attempt_run.restype = ctypes.c_int
+    ain, out, (_values, _target, stats, _planted) = make_request(instance, config)
+    ain.flags |= _abi.ATTEMPT_PREFLIGHT
+    st = lib.tergpu_attempt_run(ctypes.byref(ain), ctypes.byref(out))
+    if st not in (_abi.COMPLETED, _abi.RESOURCE_LIMIT, _abi.INVALID_CONFIGURATION):
+        raise TergpuError(st, _abi.last_error())
+    return _result(st, out, stats, instance.n)
+
+
 def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -> FullTerResult:
     """Runs attempts [attempt_first, attempt_first + attempt_limit) on the device.
 
