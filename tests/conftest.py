@@ -37,29 +37,48 @@ def hexint(v):
     return int(v, 16) if isinstance(v, str) else int(v)
 
 
-def wide_quotient_capture():
-    """The reference's Q = 69 truncation fixture (wide_quotient_root_capture,
-    tests/full_ter_tests.cpp:769-803) as a capture: n = 108, r1 = 39; list A
-    holds the root parent (ones on coordinates 54..107) twice, with residues 0
-    and 2^103; lists B and C hold the zero vector; every target is 0.  Both A
-    entries have quotient 0 on the low 64 bits; 2^103 >> 39 = 2^64 sets bit 64
-    of the second one's quotient, just outside a 64-bit window."""
+def capture_from_records(n, r1, r2, lists):
+    """A snapshot.Snapshot of a hand-built root capture: `lists` holds, per L1
+    list, (ones, residue) pairs -- the coordinates whose digit is 1 and the
+    residue as an integer mod 2^n; every child and root target is 0."""
     import numpy as np
     from tergpu import snapshot
 
-    n, w64, w32 = 108, 2, 4
+    w64, w32 = (n + 63) // 64, (n + 31) // 32
 
-    def record(ones, residue_words):
+    def record(ones, residue):
         pos = [0] * w64
         for i in ones:
             pos[i // 64] |= 1 << (i % 64)
         masks = np.array(pos + [0] * w64, dtype="<u8").view(np.uint8)
-        return np.concatenate([masks, np.array(residue_words, dtype="<u4").view(np.uint8)])
+        words = [(residue >> (32 * k)) & 0xFFFFFFFF for k in range(w32)]
+        return np.concatenate([masks, np.array(words, dtype="<u4").view(np.uint8)])
 
-    parent = range(n // 2, n)
-    a = np.concatenate([record(parent, [0, 0, 0, 0]), record(parent, [0, 0, 0, 1 << 7])])
-    zero = record([], [0, 0, 0, 0])
-    return snapshot.Snapshot(n=n, r1=39, r2=12, attempt=0, seed=0, attempt_seed=0,
-                             records=[a, zero.copy(), zero.copy()],
+    records = [np.concatenate([record(o, r) for o, r in entries]) if entries else np.zeros(0, np.uint8)
+               for entries in lists]
+    return snapshot.Snapshot(n=n, r1=r1, r2=r2, attempt=0, seed=0, attempt_seed=0, records=records,
                              child_targets=[np.zeros(w32, dtype=np.uint32) for _ in range(3)],
                              root_target=np.zeros(w32, dtype=np.uint32))
+
+
+def wide_quotient_capture():
+    """The reference's Q = 69 truncation fixture (wide_quotient_root_capture,
+    tests/full_ter_tests.cpp:769-803): n = 108, r1 = 39; list A holds the root
+    parent (ones on coordinates 54..107) twice, with residues 0 and 2^103; lists
+    B and C hold the zero vector; every target is 0.  Both A entries have
+    quotient 0 on the low 64 bits; 2^103 >> 39 = 2^64 sets bit 64 of the second
+    one's quotient, just outside a 64-bit window."""
+    parent = range(54, 108)
+    return capture_from_records(108, 39, 12, [[(parent, 0), (parent, 1 << 103)], [((), 0)], [((), 0)]])
+
+
+def early_root_capture():
+    """The reference's deterministic root-report fixture (early_root_capture,
+    tests/full_ter_tests.cpp:423-453): n = 36, r1 = 12; list A holds the parents
+    with ones on 18..35 and on 0..17, alternating, four entries; lists B and C
+    hold four zero vectors each; residues and targets are 0.  Every one of the
+    4 x 4 x 4 triples is an exact root, with two distinct parents."""
+    first, second = range(18, 36), range(0, 18)
+    zeros = [((), 0)] * 4
+    return capture_from_records(36, 12, 3, [[(first, 0), (second, 0), (first, 0), (second, 0)],
+                                            zeros, zeros])

@@ -80,3 +80,20 @@ def test_wide_quotient_root_uses_the_full_key():
         assert got.parents[0].tolist() == [0] * 54 + [1] * 54
     count = report.count_full_ter_root(snap)
     assert count.status == 0 and count.valid_root_count == 1
+
+
+def test_early_root_fixture_report_stops_and_counts():
+    """The reference's deterministic root-report fixture
+    (tests/full_ter_tests.cpp:423-485): FullCanonicalOutput counts the 64
+    pre-dedup roots and retains the 2 distinct parents, FirstWitness counts and
+    retains one, CountOnly counts 64."""
+    from conftest import early_root_capture
+    from tergpu import report
+
+    snap = early_root_capture()
+    canon = report.report_full_ter_root(snap, report.RootOutputPolicy.FULL_CANONICAL_OUTPUT)
+    assert canon.status == 0 and canon.valid_root_count == 64 and canon.retained_root_count == 2
+    first = report.report_full_ter_root(snap, report.RootOutputPolicy.FIRST_WITNESS)
+    assert first.status == 0 and first.valid_root_count == 1 and first.retained_root_count == 1
+    count = report.count_full_ter_root(snap)
+    assert count.status == 0 and count.valid_root_count == 64

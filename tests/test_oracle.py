@@ -147,3 +147,21 @@ def test_witness_verification_fails_closed(golden):
     target = inst.target_le.copy()
     target[0] ^= 1
     assert not instance.verify_witness(dataclasses.replace(inst, target_le=target), witness)
+
+
+def test_early_root_fixture_multiplicity(oracle_mod):
+    """The reference's deterministic root-report fixture
+    (tests/full_ter_tests.cpp:423-485): every one of the 4 x 4 x 4 triples is an
+    exact root (all keys 0 at Q = 24), 64 pre-dedup roots with two distinct
+    parents, each of them the root shape."""
+    from conftest import early_root_capture
+    from tergpu import snapshot
+
+    snap = early_root_capture()
+    Q, lo, hi, tau = snapshot.root_keys(snap)
+    assert Q == 24 and tau == 0 and all(not v.any() for v in lo)
+    digest, trip = oracle_mod.root_join(Q, lo, hi, capacity=128)
+    assert digest["triples"] == 64 and len(trip) == 64
+    pos = [snap.masks(l)[0][:, 0] for l in range(3)]
+    parents = {int(pos[0][a]) | int(pos[1][b]) | int(pos[2][c]) for a, b, c in trip.tolist()}
+    assert len(parents) == 2 and all(bin(p).count("1") == 18 for p in parents)
