@@ -298,17 +298,36 @@ def attempt_telemetry(tmp: Path):
     return out
 
 
+# (n, instance seed, config seed, modes, policy, audit): the solves of the
+# reference's guided tests in tests/full_ter_tests.cpp, at its default root
+# prefilter (the device has no prefilter or tile-width knob)
+GUIDED_CASES = [
+    # test_guided_pipeline_and_replay (:236-350): FullTer and FixtureTer 9, audited
+    (36, 0x544552F, 91, "guided", "first", 1),
+    (36, 0x544552F, 91, "guided,fixture=9", "first", 1),
+    (36, 0x544552F, 91, "guided", "first", 0),
+    # test_phase5_root_output_policies (:352-421): audited, FirstWitness, and the
+    # deterministic no-root run under random targets
+    (36, 0x5048415345355445, 0x5048415345355345, "guided,fixture=9", "first", 1),
+    (36, 0x5048415345355445, 0x5048415345355345, "guided,fixture=9", "first", 0),
+    (36, 0x5048415345355445, 0x4E4F524F4F543535, "fixture=9", "first", 0),
+    # test_authentic_l2_capture_tiled_merge_matches_exact_authorities (:497-527)
+    (36, 0x54494C4544434150, 0x4C324C31, "guided", "first", 1),
+    # test_m2_root_uses_complete_47_bit_quotients (:562-595): the n=72 root reads
+    # quotient bits above 63
+    (72, 0x4d32524f4f543732, 0x373242495453, "guided,fixture=9", "first", 1),
+]
+
+
 def guided_replay(tmp: Path):
-    """The reference's guided pipeline test (tests/full_ter_tests.cpp:236-330):
-    its balanced n=36 instance (seed 0x544552F, the benchmark instance) solved
-    with config seed 91 and GuidedPlanted targets, audited, under FullTer and
-    under FixtureTer with level-3 limit 9; plus the FullTer run without the
-    audit under FirstWitness.  Every stage's telemetry and the run fingerprint."""
+    """The solves of the reference's guided tests (GUIDED_CASES) on their
+    balanced instances (the benchmark instance): every stage's telemetry, the
+    run fingerprint, the status and the witness, from the reference's own
+    solve_full_ter."""
     out = []
-    for modes, policy, audit in (("guided", "first", 1), ("guided,fixture=9", "first", 1),
-                                 ("guided", "first", 0)):
-        rows = O.ref_run("solve", 36, 0x544552F, 1, "auth", policy, audit, 91, modes)
-        out.append({"n": 36, "seed": 0x544552F, "config_seed": 91, "modes": modes, "policy": policy,
+    for n, seed, config_seed, modes, policy, audit in GUIDED_CASES:
+        rows = O.ref_run("solve", n, seed, 1, "auth", policy, audit, config_seed, modes)
+        out.append({"n": n, "seed": seed, "config_seed": config_seed, "modes": modes, "policy": policy,
                     "audit": audit, "rows": rows[:-1], "final": rows[-1]})
     return out
 

@@ -122,29 +122,37 @@ def test_audit_mode_checks_every_stage_and_matches_reference(golden, case):
                 assert a[dev_key] == want, (g["n"], g["seed"], row["attempt"], stage, ref_key)
 
 
-@pytest.mark.parametrize("case", range(3))
-def test_guided_pipeline_and_replay_match_reference(golden, case):
-    """The reference's guided pipeline test (tests/full_ter_tests.cpp:236-330) on
-    the device: its balanced n=36 instance (seed 0x544552F) with config seed 91
-    and GuidedPlanted targets, audited (the reference's default) under FullTer
-    and under FixtureTer with level-3 limit 9, and without the audit under
-    FirstWitness.  Found with the reference's witness, every stage counter, stage
-    fingerprint and run fingerprint equal to the reference's; a second identical
-    call replays the witness and the fingerprint exactly."""
+GUIDED_CASES = 8  # golden guided_replay: the solves of the reference's guided tests
+
+
+@pytest.mark.parametrize("case", range(GUIDED_CASES))
+def test_guided_tests_match_reference(golden, case):
+    """The solves of the reference's guided tests in tests/full_ter_tests.cpp
+    (guided pipeline and replay, root output policies with their no-root run,
+    the authentic L2 capture, the n=72 root over 47-bit quotients) on the
+    device: their balanced instances with their config seeds, GuidedPlanted or
+    random targets, FullTer or FixtureTer at level-3 limit 9, audited or under
+    FirstWitness.  The reference's status and witness, every stage counter,
+    stage fingerprint and the run fingerprint; a second identical call replays
+    them exactly."""
     from tergpu import _abi, attempt, instance
 
+    assert len(golden["guided_replay"]) == GUIDED_CASES
     g = golden["guided_replay"][case]
     inst = instance.benchmark_instance(g["n"], g["seed"])
     fixture = int(g["modes"].split("fixture=")[1]) if "fixture=" in g["modes"] else 0
-    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=1, guided=True,
+    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=1, guided="guided" in g["modes"],
                                 fixture_limit=fixture, audit=bool(g["audit"]), telemetry=True,
-                                memory_limit_bytes=64 << 20)
+                                memory_limit_bytes=128 << 20)
     first = attempt.solve_full_ter(inst, cfg)
     final = g["final"]
-    assert first.status == final["status"] == _abi.FOUND, (first.status_name, _abi.last_error())
-    assert "".join(str(int(d)) for d in first.witness) == final["witness"]
-    assert instance.verify_witness(inst, first.witness)
-    assert first.fingerprint == hexint(final["fingerprint"]), g["modes"]
+    assert first.status == final["status"], (g["modes"], first.status_name, _abi.last_error())
+    if first.status == _abi.FOUND:
+        assert "".join(str(int(d)) for d in first.witness) == final["witness"]
+        assert instance.verify_witness(inst, first.witness)
+    else:
+        assert first.witness is None
+    assert first.fingerprint == hexint(final["fingerprint"]), (g["seed"], g["modes"], g["audit"])
     assert first.level3_size == final["l3"][0]
     (a,), (row,) = first.attempts, g["rows"]
     assert a["attempt_seed"] == row["seed"] and a["status"] == row["status"]
@@ -153,11 +161,13 @@ def test_guided_pipeline_and_replay_match_reference(golden, case):
         for ref_key, dev_key in fields.items():
             want = row[stage][ref_key]
             want = hexint(want) if ref_key == "fingerprint" else want
-            assert a[dev_key] == want, (g["modes"], g["audit"], stage, ref_key, a[dev_key], want)
-    assert a["audited_stages"] == (13 if g["audit"] else 0)
+            assert a[dev_key] == want, (g["seed"], g["modes"], g["audit"], stage, ref_key, a[dev_key], want)
+    # the nine L3 -> L2 merges always fit the audit's cap at these level-3 sizes
+    assert a["audited_stages"] >= 9 if g["audit"] else a["audited_stages"] == 0
     second = attempt.solve_full_ter(inst, cfg)
     assert second.status == first.status and second.fingerprint == first.fingerprint
-    assert np.array_equal(second.witness, first.witness)
+    if first.status == _abi.FOUND:
+        assert np.array_equal(second.witness, first.witness)
 
 
 def test_n36_attempt_loop_stops_like_the_reference(golden):

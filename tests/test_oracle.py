@@ -165,3 +165,31 @@ def test_early_root_fixture_multiplicity(oracle_mod):
     pos = [snap.masks(l)[0][:, 0] for l in range(3)]
     parents = {int(pos[0][a]) | int(pos[1][b]) | int(pos[2][c]) for a, b, c in trip.tolist()}
     assert len(parents) == 2 and all(bin(p).count("1") == 18 for p in parents)
+
+
+def test_guided_goldens_hold_the_reference_tests_assertions(golden):
+    """The golden guided_replay rows, printed by the reference's solve_full_ter,
+    satisfy what the reference's own tests assert of those solves
+    (tests/full_ter_tests.cpp:249-330, 372-421, 578-595): the guided solves are
+    Found with the planted root as witness; audited roots report
+    FullCanonicalOutput without an early stop; FirstWitness stops early with one
+    retained root; the random-target run exhausts its budget with an empty root."""
+    from tergpu import instance
+
+    rows = golden["guided_replay"]
+    assert len(rows) == 8
+    for g in rows:
+        final, root = g["final"], g["rows"][0]["root"]
+        if "guided" in g["modes"]:
+            assert final["status"] == 1
+            inst = instance.benchmark_instance(g["n"], g["seed"])
+            assert [int(c) for c in final["witness"]] == inst.planted.tolist()
+            assert g["rows"][0]["level0"] == 1
+            if g["audit"]:
+                assert root["policy"] == 2 and root["early_stopped"] == 0
+            else:
+                assert root["policy"] == 0 and root["early_stopped"] == 1 and root["valid_roots"] == 1
+        else:
+            assert final["status"] == 3 and g["rows"][0]["level0"] == 0 and root["early_stopped"] == 0
+    n72 = [g for g in rows if g["n"] == 72]
+    assert n72 and n72[0]["rows"][0]["root"]["quotient_bits"] == 47
