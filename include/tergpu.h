@@ -221,11 +221,16 @@ int tergpu_root_run_records(const tergpu_root_records_in *in, tergpu_root_record
  * src/full_ter.cpp:2879-2908) and returned as the witness.
  *
  * Statuses: TERGPU_FOUND, TERGPU_ATTEMPT_LIMIT_REACHED (budget spent, never UNSAT),
- * TERGPU_CANCELLED (*cancel != 0 before an attempt or stage),
- * TERGPU_RESOURCE_LIMIT (the predicted device bytes exceed memory_limit_bytes,
- * refused before any allocation), TERGPU_INVALID_CONFIGURATION (36 does not
- * divide n, or n > 108), TERGPU_INVARIANT_VIOLATION (a witness that fails
- * verification).
+ * TERGPU_CANCELLED (*cancel != 0 when the call starts -- returned before level 3
+ * and any device work, with the run fingerprint of no attempts under
+ * TERGPU_ATTEMPT_TELEMETRY, as the reference's pre-cancelled solve -- or before
+ * an attempt or stage, or inside a sweep), TERGPU_RESOURCE_LIMIT (the predicted
+ * device bytes exceed memory_limit_bytes, refused before any allocation),
+ * TERGPU_INVALID_CONFIGURATION (36 does not divide n or n > 108, attempt_count
+ * 0, root_policy CountOnly or unknown, flag bits outside TERGPU_ATTEMPT_*, an
+ * unbalanced planted root under TERGPU_ATTEMPT_GUIDED, fixture limit 0; all
+ * before any device work), TERGPU_INVARIANT_VIOLATION (a witness that fails
+ * verification, or an audited stage that disagrees with its scalar oracle).
  */
 typedef struct {
   uint32_t attempt;

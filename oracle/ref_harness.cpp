@@ -9,8 +9,9 @@
 //       solve_full_ter (src/full_ter.cpp:3867) on authentic_instance (KIND=auth)
 //       or build_instance(n, 10, seed) (KIND=build); per-attempt level sizes,
 //       root accounting and the witness.  CONFIG_SEED (default SEED, "-" keeps
-//       it) seeds the targets; MODES "guided", "fixture=<limit>" or both
-//       (comma-separated) select GuidedPlanted targets and FixtureTer level 3.
+//       it) seeds the targets; MODES "guided", "fixture=<limit>" and
+//       "cancelled" (comma-separated) select GuidedPlanted targets, FixtureTer
+//       level 3 and a cancellation flag already set when the solve starts.
 //   terref capture N SEED ATTEMPT KIND OUT
 //       root_snapshot::capture_to_file (ter2_root/frozen/ter_root_snapshot.cpp:124).
 //   terref snaproot SNAP BACKEND CELLS PROJ
@@ -52,6 +53,7 @@
 #include "ter/limitations.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -133,6 +135,8 @@ int cmd_solve(int argc, char** argv) {
   config.audit = audit;
   config.root_output_policy = policy == "canon" ? ter::RootOutputPolicy::FullCanonicalOutput
                                                 : ter::RootOutputPolicy::FirstWitness;
+  std::atomic_bool cancelled{true};
+  if (modes.find("cancelled") != std::string::npos) { config.cancellation = &cancelled; }
   const auto start = Clock::now();
   const ter::FullTerResult result = ter::solve_full_ter(instance, config);
   const double ms = std::chrono::duration<double, std::milli>(Clock::now() - start).count();

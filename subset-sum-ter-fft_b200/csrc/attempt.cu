@@ -940,6 +940,47 @@ bool graph_attempt(GraphPlan& g, Workspace& w, const Targets& tg, u128 T, uint32
   return true;
 }
 
+// FullTerTelemetry::fingerprint (src/full_ter.cpp:2532-2577): the witness's
+// digits when one was found, the run's fields, then every attempt's.  l3 is 0
+// for a run that stopped before level 3 (the reference leaves its physical
+// level-3 sizes unset there).
+uint64_t run_fingerprint(const uint8_t* witness, uint32_t n, uint64_t seed, bool fixture, uint32_t r1,
+                         uint32_t r2, uint64_t l3, const std::vector<tergpu_attempt_stats>& run) {
+  Fnv64 f;
+  if (witness != nullptr)
+    for (uint32_t i = 0; i < n; ++i) f.mix((uint64_t)witness[i] + 1u);
+  f.mix(seed);
+  f.mix(n);
+  f.mix(n);  // modulus bits: the full TER modulus is 2^n
+  f.mix(fixture ? 1 : 0);  // TerExecutionMode: FullTer 0, FixtureTer 1 (include/ter/types.hpp:25-28)
+  f.mix(0);  // ShapeFamily::FiniteSanity
+  f.mix(r1);
+  f.mix(r2);
+  f.mix(l3);
+  f.mix(l3);
+  f.mix(run.size());
+  for (const auto& a : run) {
+    f.mix(a.attempt_seed);
+    f.mix(a.attempt);
+    f.mix((uint64_t)a.status);
+    for (int i = 0; i < 9; ++i) f.mix(a.level2_sizes[i]);
+    for (int i = 0; i < 3; ++i) f.mix(a.level1_sizes[i]);
+    f.mix(a.level0_size);
+    f.mix(a.l3_modular);
+    f.mix(a.l2_modular);
+    f.mix(a.root_modular);
+    f.mix(a.root_quotient_bits);
+    f.mix(a.root_prefilter_bits);
+    f.mix(a.root_low_prefilter);
+    f.mix(a.root_full_quotient_rejects);
+    f.mix(0);  // pair_records: the root materializes no pair records
+    f.mix(a.l2_fingerprint);
+    f.mix(a.l1_fingerprint);
+    f.mix(a.l0_fingerprint);
+  }
+  return f.h;
+}
+
 }  // namespace
 
 // One attempt range on `own` (a private workspace of the batch engine) or, when
@@ -959,10 +1000,22 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     return TERGPU_INVALID_CONFIGURATION;
   }
   const bool preflight = (in->flags & TERGPU_ATTEMPT_PREFLIGHT) != 0;
-  if (!preflight &&
-      (in->values_le == nullptr || in->target_le == nullptr || in->attempt_count == 0)) {
-    t_error = "instance or attempt range missing";
+  constexpr uint32_t kKnownFlags = TERGPU_ATTEMPT_CAPTURE_ONLY | TERGPU_ATTEMPT_PREFLIGHT | TERGPU_ATTEMPT_NO_GRAPH |
+                                   TERGPU_ATTEMPT_TELEMETRY | TERGPU_ATTEMPT_BACKGROUND | TERGPU_ATTEMPT_AUDIT |
+                                   TERGPU_ATTEMPT_GUIDED | TERGPU_ATTEMPT_FIXTURE;
+  if ((in->flags & ~kKnownFlags) != 0) {
+    t_error = "unknown attempt flags";
+    return TERGPU_INVALID_CONFIGURATION;
+  }
+  if (!preflight && (in->values_le == nullptr || in->target_le == nullptr)) {
+    t_error = "instance missing";
     return TERGPU_INVALID_INPUT;
+  }
+  // an empty attempt budget is a configuration the reference refuses
+  // (runtime_limit_supported, src/full_ter.cpp:2945-2957)
+  if (!preflight && in->attempt_count == 0) {
+    t_error = "full TER solver configuration or instance is invalid";
+    return TERGPU_INVALID_CONFIGURATION;
   }
   const uint32_t r1 = floor_log2_multinomial3(n / 2, n / 6) / 2;
   const uint32_t r2 = floor_log2_multinomial3(n / 6, n / 18) / 2;
@@ -983,6 +1036,16 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   const uint64_t l3 = fixture ? std::min<uint64_t>(binom_host(n / 2, n / 36), in->fixture_level3_limit)
                               : binom_host(n / 2, n / 36);
   out->level3_size = l3;
+  // a call cancelled before it starts returns before level 3, as the
+  // reference's does (src/full_ter.cpp:2979-2985), with the run fingerprint of
+  // no attempts and no level-3 lists
+  if (!preflight && in->cancel != nullptr && *in->cancel != 0) {
+    t_error = "full TER execution was cancelled";
+    if ((in->flags & TERGPU_ATTEMPT_TELEMETRY) != 0)
+      out->fingerprint = run_fingerprint(nullptr, n, in->seed, fixture, r1, r2, 0, {});
+    out->total_ms = ms_since(t_call);
+    return TERGPU_CANCELLED;
+  }
 
   // Preflight against the ceiling, from the expected level sizes (2x margin).
   const double l2_est = (double)l3 * l3 / std::ldexp(1.0, r2) * 1.3 + 64;
@@ -1503,42 +1566,8 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     run.push_back(stat);
     if (status == TERGPU_FOUND) break;
   }
-  if (telemetry) {
-    // FullTerTelemetry::fingerprint (src/full_ter.cpp:2532-2577)
-    Fnv64 f;
-    if (status == TERGPU_FOUND)
-      for (uint32_t i = 0; i < n; ++i) f.mix((uint64_t)out->witness[i] + 1u);
-    f.mix(in->seed);
-    f.mix(n);
-    f.mix(n);  // modulus bits: the full TER modulus is 2^n
-    f.mix(fixture ? 1 : 0);  // TerExecutionMode: FullTer 0, FixtureTer 1 (include/ter/types.hpp:25-28)
-    f.mix(0);  // ShapeFamily::FiniteSanity
-    f.mix(r1);
-    f.mix(r2);
-    f.mix(l3);
-    f.mix(l3);
-    f.mix(run.size());
-    for (const auto& a : run) {
-      f.mix(a.attempt_seed);
-      f.mix(a.attempt);
-      f.mix((uint64_t)a.status);
-      for (int i = 0; i < 9; ++i) f.mix(a.level2_sizes[i]);
-      for (int i = 0; i < 3; ++i) f.mix(a.level1_sizes[i]);
-      f.mix(a.level0_size);
-      f.mix(a.l3_modular);
-      f.mix(a.l2_modular);
-      f.mix(a.root_modular);
-      f.mix(a.root_quotient_bits);
-      f.mix(a.root_prefilter_bits);
-      f.mix(a.root_low_prefilter);
-      f.mix(a.root_full_quotient_rejects);
-      f.mix(0);  // pair_records: the root materializes no pair records
-      f.mix(a.l2_fingerprint);
-      f.mix(a.l1_fingerprint);
-      f.mix(a.l0_fingerprint);
-    }
-    out->fingerprint = f.h;
-  }
+  if (telemetry) out->fingerprint = run_fingerprint(status == TERGPU_FOUND ? out->witness : nullptr, n, in->seed,
+                                                    fixture, r1, r2, l3, run);
   out->status = status;
   out->total_ms = ms_since(t_call);
   return status;

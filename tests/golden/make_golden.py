@@ -332,6 +332,21 @@ def guided_replay(tmp: Path):
     return out
 
 
+def failure_semantics(tmp: Path):
+    """The solves of the reference's failure-semantics test
+    (tests/full_ter_tests.cpp:597-668): its balanced n=36 instance (seed 17),
+    config seed 3, FixtureTer with level-3 limit 1, random targets, two
+    attempts, the default (audited) config; the same run with its cancellation
+    flag set before the call; and an empty attempt budget."""
+    out = []
+    for name, attempts, modes in (("run", 2, "fixture=1"), ("pre_cancelled", 2, "fixture=1,cancelled"),
+                                  ("no_attempts", 0, "fixture=1")):
+        rows = O.ref_run("solve", 36, 17, attempts, "auth", "first", 1, 3, modes)
+        out.append({"name": name, "n": 36, "seed": 17, "config_seed": 3, "attempts": attempts,
+                    "fixture_limit": 1, "audit": 1, "rows": rows[:-1], "final": rows[-1]})
+    return out
+
+
 def full_bench_rows(tmp: Path):
     """The reference's own ter_full_bench (bench/ter_full_bench.cpp, built from its
     sources into oracle/_ref/ter_full_bench): its CSV header and row for the
@@ -394,6 +409,7 @@ SECTIONS = {
     "whole_roots": whole_roots,
     "attempt_telemetry": attempt_telemetry,
     "guided_replay": guided_replay,
+    "failure_semantics": failure_semantics,
     "full_bench_rows": full_bench_rows,
     "published_runs": published_runs,
 }

@@ -66,3 +66,59 @@ def test_solve_refusals_before_device_work():
     res = attempt.solve_full_ter(bad, attempt.FullTerConfig(seed=91, guided=True))
     assert res.status == _abi.INVALID_CONFIGURATION
     assert _abi.last_error() == "guided TER requires a planted binary root balanced across both halves"
+
+
+def _failure_case(golden, name):
+    from tergpu import attempt, instance
+
+    g = next(c for c in golden["failure_semantics"] if c["name"] == name)
+    inst = instance.benchmark_instance(g["n"], g["seed"])
+    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=g["attempts"],
+                                fixture_limit=g["fixture_limit"], audit=bool(g["audit"]), telemetry=True)
+    return g, inst, cfg
+
+
+def test_pre_cancelled_solve_matches_reference(golden):
+    """A solve whose cancellation flag is set before the call returns Cancelled
+    before level 3, with the reference's run fingerprint (no attempts, no
+    level-3 lists): the reference's failure-semantics test
+    (tests/full_ter_tests.cpp:636-645), with no device work."""
+    import ctypes
+
+    from conftest import hexint
+    from tergpu import _abi, attempt
+
+    g, inst, cfg = _failure_case(golden, "pre_cancelled")
+    assert g["final"]["status"] == _abi.CANCELLED and g["final"]["l3"] == [0, 0]
+    res = attempt.solve_full_ter(inst, cfg, cancel=ctypes.c_int32(1))
+    assert res.status == _abi.CANCELLED and res.attempts == []
+    assert res.fingerprint == hexint(g["final"]["fingerprint"])
+    assert _abi.last_error() == g["final"]["message"]
+
+
+def test_empty_budget_and_tiny_ceiling_fail_closed(golden):
+    """An empty attempt budget is InvalidConfiguration, as the reference's
+    (tests/full_ter_tests.cpp:647-652), and a 1-byte memory ceiling is
+    ResourceLimit (:630-633); neither touches the device."""
+    from tergpu import _abi, attempt
+
+    g, inst, cfg = _failure_case(golden, "no_attempts")
+    assert g["final"]["status"] == _abi.INVALID_CONFIGURATION
+    assert attempt.solve_full_ter(inst, cfg).status == _abi.INVALID_CONFIGURATION
+    _, inst, cfg = _failure_case(golden, "run")
+    tight = attempt.FullTerConfig(**{**cfg.__dict__, "memory_limit_bytes": 1})
+    assert attempt.solve_full_ter(inst, tight).status == _abi.RESOURCE_LIMIT
+
+
+def test_unknown_flags_are_refused():
+    """Flag bits outside the ABI's set fail closed (the reference refuses
+    out-of-range execution-mode values: tests/full_ter_tests.cpp:654-658)."""
+    import ctypes
+
+    from tergpu import _abi, attempt, instance
+
+    lib = _abi.load()
+    ain, out, keep = attempt.make_request(instance.benchmark_instance(36, 17), attempt.FullTerConfig())
+    ain.flags |= 1 << 12
+    lib.tergpu_attempt_run.argtypes = [ctypes.POINTER(attempt.AttemptIn), ctypes.POINTER(attempt.AttemptOut)]
+    assert lib.tergpu_attempt_run(ctypes.byref(ain), ctypes.byref(out)) == _abi.INVALID_CONFIGURATION

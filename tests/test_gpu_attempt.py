@@ -170,6 +170,35 @@ def test_guided_tests_match_reference(golden, case):
         assert np.array_equal(second.witness, first.witness)
 
 
+def test_failure_semantics_run_matches_reference(golden):
+    """The reference's failure-semantics run (tests/full_ter_tests.cpp:597-628):
+    balanced n=36 instance (seed 17), config seed 3, FixtureTer with one level-3
+    subset per half, random targets, two audited attempts.  Both attempts have
+    empty level-1 lists and the budget is exhausted; every attempt's seed, stage
+    counters and fingerprints and the run fingerprint equal the reference's, and
+    a second call replays them."""
+    from tergpu import _abi, attempt, instance
+
+    g = next(c for c in golden["failure_semantics"] if c["name"] == "run")
+    inst = instance.benchmark_instance(g["n"], g["seed"])
+    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=g["attempts"],
+                                fixture_limit=g["fixture_limit"], audit=bool(g["audit"]), telemetry=True,
+                                memory_limit_bytes=16 << 20)
+    res = attempt.solve_full_ter(inst, cfg)
+    assert res.status == g["final"]["status"] == _abi.ATTEMPT_LIMIT_REACHED, _abi.last_error()
+    assert res.fingerprint == hexint(g["final"]["fingerprint"])
+    assert [a["attempt_seed"] for a in res.attempts] == [r["seed"] for r in g["rows"]] == [3, 4]
+    for a, row in zip(res.attempts, g["rows"]):
+        assert a["status"] == row["status"] and a["level2"] == row["level2"] and a["level1"] == row["level1"]
+        for stage, fields in STAGES.items():
+            for ref_key, dev_key in fields.items():
+                want = row[stage][ref_key]
+                want = hexint(want) if ref_key == "fingerprint" else want
+                assert a[dev_key] == want, (row["attempt"], stage, ref_key, a[dev_key], want)
+    again = attempt.solve_full_ter(inst, cfg)
+    assert again.status == res.status and again.fingerprint == res.fingerprint
+
+
 def test_n36_attempt_loop_stops_like_the_reference(golden):
     """The whole loop in one call: the reference's final status and attempt count."""
     from tergpu import _abi
