@@ -129,10 +129,20 @@ def test_snapshot_damage_is_rejected(tmp_path, golden):
         p.write_bytes(bytes(bad))
         with pytest.raises(snapshot.SnapshotError):
             snapshot.load(p)
-    p = tmp_path / "trunc.snap"
-    p.write_bytes(bytes(raw[:-5]))
-    with pytest.raises(snapshot.SnapshotError):
-        snapshot.load(p)
+    # the reference's own damage cases (ter2_root/tests/ter_root_snapshot_tests.cpp:205-220):
+    # a record cut short by two records, a tampered header field, a trailing byte
+    off_n = snapshot.HEADER_DTYPE.fields["n"][1]
+    tampered = bytearray(raw)
+    tampered[off_n] ^= 0x01
+    for name, data in (("trunc", raw[:-5]), ("trunc48", raw[:-48]), ("header", tampered),
+                       ("trailing", raw + b"\0")):
+        p = tmp_path / f"{name}.snap"
+        p.write_bytes(bytes(data))
+        with pytest.raises(snapshot.SnapshotError):
+            snapshot.load(p)
+    p = tmp_path / "original.snap"
+    p.write_bytes(bytes(raw))
+    assert snapshot.load(p).entries == golden["n36_snapshot"]["level1"]
 
 
 def test_host_key_derivation_matches_oracle_attempt(oracle_mod, golden):
