@@ -33,6 +33,24 @@ def n72_anchor_attempt(oracle_mod):
     return oracle_mod.attempt(72, 19797034556212562, 0, export_l1=True)
 
 
+# reference FullTerStageTelemetry field -> device stats field, per stage
+STAGES = {
+    "binary": {"pairs": "l3_pairs", "modular": "l3_modular", "structural": "l3_structural_rejects",
+               "distribution": "l3_distribution_rejects", "survivors": "l3_survivors",
+               "fingerprint": "l2_fingerprint"},
+    "middle": {"pairs": "l2_pairs", "modular": "l2_modular", "structural": "l2_structural_rejects",
+               "distribution": "l2_distribution_rejects", "survivors": "l2_survivors",
+               "fingerprint": "l1_fingerprint"},
+    "root": {"pairs": "root_pairs", "modular": "root_modular",
+             "structural": "root_structural_rejects", "distribution": "root_distribution_rejects",
+             "survivors": "valid_roots", "deduplicated": "level0", "quotient_bits": "root_quotient_bits",
+             "prefilter_bits": "root_prefilter_bits", "low_prefilter": "root_low_prefilter",
+             "full_quotient_rejects": "root_full_quotient_rejects", "valid_roots": "valid_roots",
+             "policy": "root_policy", "early_stopped": "root_early_stopped",
+             "fingerprint": "l0_fingerprint"},
+}
+
+
 def hexint(v):
     return int(v, 16) if isinstance(v, str) else int(v)
 

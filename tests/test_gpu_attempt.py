@@ -5,7 +5,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_DIR, hexint
+from conftest import GOLDEN_DIR, STAGES, hexint
 
 pytestmark = pytest.mark.gpu
 
@@ -38,24 +38,6 @@ def test_n36_attempts_match_reference(golden, case):
             assert res.status == _abi.FOUND and instance.verify_witness(inst, res.witness)
         else:
             assert res.status == _abi.ATTEMPT_LIMIT_REACHED
-
-
-STAGES = {
-    # reference FullTerStageTelemetry field -> device stats field, per stage
-    "binary": {"pairs": "l3_pairs", "modular": "l3_modular", "structural": "l3_structural_rejects",
-               "distribution": "l3_distribution_rejects", "survivors": "l3_survivors",
-               "fingerprint": "l2_fingerprint"},
-    "middle": {"pairs": "l2_pairs", "modular": "l2_modular", "structural": "l2_structural_rejects",
-               "distribution": "l2_distribution_rejects", "survivors": "l2_survivors",
-               "fingerprint": "l1_fingerprint"},
-    "root": {"pairs": "root_pairs", "modular": "root_modular",
-             "structural": "root_structural_rejects", "distribution": "root_distribution_rejects",
-             "survivors": "valid_roots", "deduplicated": "level0", "quotient_bits": "root_quotient_bits",
-             "prefilter_bits": "root_prefilter_bits", "low_prefilter": "root_low_prefilter",
-             "full_quotient_rejects": "root_full_quotient_rejects", "valid_roots": "valid_roots",
-             "policy": "root_policy", "early_stopped": "root_early_stopped",
-             "fingerprint": "l0_fingerprint"},
-}
 
 
 @pytest.mark.parametrize("case", range(16))
@@ -120,83 +102,6 @@ def test_audit_mode_checks_every_stage_and_matches_reference(golden, case):
                 want = row[stage][ref_key]
                 want = hexint(want) if ref_key == "fingerprint" else want
                 assert a[dev_key] == want, (g["n"], g["seed"], row["attempt"], stage, ref_key)
-
-
-GUIDED_CASES = 8  # golden guided_replay: the solves of the reference's guided tests
-
-
-@pytest.mark.parametrize("case", range(GUIDED_CASES))
-def test_guided_tests_match_reference(golden, case):
-    """The solves of the reference's guided tests in tests/full_ter_tests.cpp
-    (guided pipeline and replay, root output policies with their no-root run,
-    the authentic L2 capture, the n=72 root over 47-bit quotients) on the
-    device: their balanced instances with their config seeds, GuidedPlanted or
-    random targets, FullTer or FixtureTer at level-3 limit 9, audited or under
-    FirstWitness.  The reference's status and witness, every stage counter,
-    stage fingerprint and the run fingerprint; a second identical call replays
-    them exactly."""
-    from tergpu import _abi, attempt, instance
-
-    assert len(golden["guided_replay"]) == GUIDED_CASES
-    g = golden["guided_replay"][case]
-    inst = instance.benchmark_instance(g["n"], g["seed"])
-    fixture = int(g["modes"].split("fixture=")[1]) if "fixture=" in g["modes"] else 0
-    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=1, guided="guided" in g["modes"],
-                                fixture_limit=fixture, audit=bool(g["audit"]), telemetry=True,
-                                memory_limit_bytes=128 << 20)
-    first = attempt.solve_full_ter(inst, cfg)
-    final = g["final"]
-    assert first.status == final["status"], (g["modes"], first.status_name, _abi.last_error())
-    if first.status == _abi.FOUND:
-        assert "".join(str(int(d)) for d in first.witness) == final["witness"]
-        assert instance.verify_witness(inst, first.witness)
-    else:
-        assert first.witness is None
-    assert first.fingerprint == hexint(final["fingerprint"]), (g["seed"], g["modes"], g["audit"])
-    assert first.level3_size == final["l3"][0]
-    (a,), (row,) = first.attempts, g["rows"]
-    assert a["attempt_seed"] == row["seed"] and a["status"] == row["status"]
-    assert a["level2"] == row["level2"] and a["level1"] == row["level1"] and a["level0"] == row["level0"]
-    for stage, fields in STAGES.items():
-        for ref_key, dev_key in fields.items():
-            want = row[stage][ref_key]
-            want = hexint(want) if ref_key == "fingerprint" else want
-            assert a[dev_key] == want, (g["seed"], g["modes"], g["audit"], stage, ref_key, a[dev_key], want)
-    # the nine L3 -> L2 merges always fit the audit's cap at these level-3 sizes
-    assert a["audited_stages"] >= 9 if g["audit"] else a["audited_stages"] == 0
-    second = attempt.solve_full_ter(inst, cfg)
-    assert second.status == first.status and second.fingerprint == first.fingerprint
-    if first.status == _abi.FOUND:
-        assert np.array_equal(second.witness, first.witness)
-
-
-def test_failure_semantics_run_matches_reference(golden):
-    """The reference's failure-semantics run (tests/full_ter_tests.cpp:597-628):
-    balanced n=36 instance (seed 17), config seed 3, FixtureTer with one level-3
-    subset per half, random targets, two audited attempts.  Both attempts have
-    empty level-1 lists and the budget is exhausted; every attempt's seed, stage
-    counters and fingerprints and the run fingerprint equal the reference's, and
-    a second call replays them."""
-    from tergpu import _abi, attempt, instance
-
-    g = next(c for c in golden["failure_semantics"] if c["name"] == "run")
-    inst = instance.benchmark_instance(g["n"], g["seed"])
-    cfg = attempt.FullTerConfig(seed=g["config_seed"], attempt_limit=g["attempts"],
-                                fixture_limit=g["fixture_limit"], audit=bool(g["audit"]), telemetry=True,
-                                memory_limit_bytes=16 << 20)
-    res = attempt.solve_full_ter(inst, cfg)
-    assert res.status == g["final"]["status"] == _abi.ATTEMPT_LIMIT_REACHED, _abi.last_error()
-    assert res.fingerprint == hexint(g["final"]["fingerprint"])
-    assert [a["attempt_seed"] for a in res.attempts] == [r["seed"] for r in g["rows"]] == [3, 4]
-    for a, row in zip(res.attempts, g["rows"]):
-        assert a["status"] == row["status"] and a["level2"] == row["level2"] and a["level1"] == row["level1"]
-        for stage, fields in STAGES.items():
-            for ref_key, dev_key in fields.items():
-                want = row[stage][ref_key]
-                want = hexint(want) if ref_key == "fingerprint" else want
-                assert a[dev_key] == want, (row["attempt"], stage, ref_key, a[dev_key], want)
-    again = attempt.solve_full_ter(inst, cfg)
-    assert again.status == res.status and again.fingerprint == res.fingerprint
 
 
 def test_n36_attempt_loop_stops_like_the_reference(golden):

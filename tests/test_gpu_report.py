@@ -59,41 +59,3 @@ def test_root_report_resource_limit():
                                       Config(memory_limit_bytes=1024))
     assert got.status == 7 and got.valid_root_count == 0  # ResourceLimit, nothing counted
 
-
-def test_wide_quotient_root_uses_the_full_key():
-    """The reference's Q = 69 truncation fixture (tests/full_ter_tests.cpp:805-838):
-    both pairs agree on the low quotient window, the device's full 69-bit key
-    keeps one; exactly one valid root under every policy and in the count."""
-    from conftest import wide_quotient_capture
-    from tergpu import report
-    from tergpu.root import Config, run_gpu_root_records
-
-    snap = wide_quotient_capture()
-    res = run_gpu_root_records(snap, Config(projected_bits=32))
-    assert res.tau == 0 and res.telemetry.logical_pairs == 2
-    assert res.telemetry.projected_hits == 2
-    assert res.triples.tolist() == [[0, 0, 0]]
-    assert res.residue_exact == 1 and res.valid_roots == 1
-    for policy in (report.RootOutputPolicy.FULL_CANONICAL_OUTPUT, report.RootOutputPolicy.FIRST_WITNESS):
-        got = report.report_full_ter_root(snap, policy)
-        assert got.status == 0 and got.valid_root_count == 1 and got.retained_root_count == 1
-        assert got.parents[0].tolist() == [0] * 54 + [1] * 54
-    count = report.count_full_ter_root(snap)
-    assert count.status == 0 and count.valid_root_count == 1
-
-
-def test_early_root_fixture_report_stops_and_counts():
-    """The reference's deterministic root-report fixture
-    (tests/full_ter_tests.cpp:423-485): FullCanonicalOutput counts the 64
-    pre-dedup roots and retains the 2 distinct parents, FirstWitness counts and
-    retains one, CountOnly counts 64."""
-    from conftest import early_root_capture
-    from tergpu import report
-
-    snap = early_root_capture()
-    canon = report.report_full_ter_root(snap, report.RootOutputPolicy.FULL_CANONICAL_OUTPUT)
-    assert canon.status == 0 and canon.valid_root_count == 64 and canon.retained_root_count == 2
-    first = report.report_full_ter_root(snap, report.RootOutputPolicy.FIRST_WITNESS)
-    assert first.status == 0 and first.valid_root_count == 1 and first.retained_root_count == 1
-    count = report.count_full_ter_root(snap)
-    assert count.status == 0 and count.valid_root_count == 64
