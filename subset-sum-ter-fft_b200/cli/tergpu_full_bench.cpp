@@ -406,6 +406,32 @@ void print_metadata(const Options& o, const std::string& command, uint64_t execu
             << " command=\"" << command << "\"\n";
 }
 
+// The FiniteSanity representation count m! / (k! k! (m - 2k)!) as C(m, k) *
+// C(m - k, k), exact in 128 bits for n <= 108 (R1 < 2^80): the reference's
+// FullTerParameters::representation1 (m = n/2, k = n/6) and representation2
+// (m = n/6, k = n/18), printed by its preflight (bench/ter_full_bench.cpp:624-627).
+unsigned __int128 representation_count(uint32_t m, uint32_t k) {
+  unsigned __int128 a = 1, b = 1;
+  for (uint32_t i = 1; i <= k; ++i) a = a * (m - k + i) / i;      // C(m, k), exact at every step
+  for (uint32_t i = 1; i <= k; ++i) b = b * (m - 2 * k + i) / i;  // C(m - k, k)
+  return a * b;
+}
+
+std::string decimal(unsigned __int128 v) {
+  std::string digits;
+  do {
+    digits.insert(digits.begin(), static_cast<char>('0' + static_cast<int>(v % 10)));
+    v /= 10;
+  } while (v != 0);
+  return digits;
+}
+
+uint32_t floor_log2(unsigned __int128 v) {
+  uint32_t bits = 0;
+  while (v >>= 1) ++bits;
+  return bits;
+}
+
 int run_preflight(const Options& o) {
   tergpu_attempt_in in{};
   in.n = o.n;
@@ -426,6 +452,10 @@ int run_preflight(const Options& o) {
   const uint32_t root_q = o.n - out.r1, middle_q = out.r1 - out.r2;
   std::cout << "  r1=" << out.r1 << " r2=" << out.r2 << " root_Q=" << root_q
             << " l2_to_l1_Q=" << middle_q << '\n';
+  const unsigned __int128 rep1 = representation_count(o.n / 2, o.n / 6);
+  const unsigned __int128 rep2 = representation_count(o.n / 6, o.n / 18);
+  std::cout << "  representation1=" << decimal(rep1) << " floor_log2=" << floor_log2(rep1) << '\n';
+  std::cout << "  representation2=" << decimal(rep2) << " floor_log2=" << floor_log2(rep2) << '\n';
   std::cout << "  level3_per_half=" << out.level3_size << '\n';
   std::cout << "  l2_to_l1_backend=device ternary join on the projected quotient (streaming, "
                "no pair index)\n";

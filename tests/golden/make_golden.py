@@ -373,6 +373,21 @@ def full_bench_rows(tmp: Path):
     return out
 
 
+def preflight_text(tmp: Path):
+    """The reference's own ter_full_bench --preflight output (geometry,
+    representation counts, decisions) at n = 36, 72, 108 and a large ceiling,
+    and FixtureTer at n = 72."""
+    import subprocess
+
+    binary = HERE.parent.parent / "oracle" / "_ref" / "ter_full_bench"
+    out = []
+    for args in (["--n=36"], ["--n=72"], ["--n=108"], ["--n=72", "--fixture"]):
+        args = ["--preflight", *args, "--memory-limit-mib=1000000"]
+        proc = subprocess.run([str(binary), *args], capture_output=True, text=True, timeout=600)
+        out.append({"args": args, "rc": proc.returncode, "lines": proc.stdout.splitlines()})
+    return out
+
+
 REFERENCE = Path(os.environ.get("TER_REFERENCE_DIR", "/root/reference"))
 
 
@@ -411,6 +426,7 @@ SECTIONS = {
     "guided_replay": guided_replay,
     "failure_semantics": failure_semantics,
     "full_bench_rows": full_bench_rows,
+    "preflight_text": preflight_text,
     "published_runs": published_runs,
 }
 

@@ -48,6 +48,24 @@ def test_preflight_geometry(n, r1, r2, q):
     assert "VERDICT: bounded exact path on both merge stages" in p.stdout
 
 
+@pytest.mark.parametrize("case", range(4))
+def test_preflight_prints_the_reference_lines(case):
+    """Every line of the reference's own ter_full_bench --preflight (golden
+    preflight_text) appears in the device preflight, with the same exit code:
+    geometry, the exact representation counts R1 and R2, the decisions, the
+    ceiling and the mode.  The backend lines name the device's own join, and at
+    Q > 64 its full-key root decision, so those are left out of the
+    comparison."""
+    g = json.loads((GOLDEN_DIR / "reference_golden.json").read_text())["preflight_text"][case]
+    p = run(*g["args"])
+    assert p.returncode == g["rc"], p.stderr
+    got = set(p.stdout.splitlines())
+    device_worded = ("  l2_to_l1_backend=", "  root_backend=", "  root_decision=low-64")
+    for line in g["lines"]:
+        if not line.startswith(device_worded):
+            assert line in got, line
+
+
 def test_preflight_refusals():
     p = run("--preflight", "--n=48")
     assert p.returncode == 1 and "InvalidConfiguration" in p.stdout
