@@ -193,3 +193,21 @@ def test_guided_goldens_hold_the_reference_tests_assertions(golden):
             assert final["status"] == 3 and g["rows"][0]["level0"] == 0 and root["early_stopped"] == 0
     n72 = [g for g in rows if g["n"] == 72]
     assert n72 and n72[0]["rows"][0]["root"]["quotient_bits"] == 47
+
+
+def test_product_instances_equal_the_oracle_generator(oracle_mod):
+    """tergpu.instance, which builds every device request, gives the same
+    weights, target and planted support as the oracle's restatement of the
+    reference's generators (build_instance, src/instance.cpp:61-120, and the
+    benchmark instance with the planted support on the first n/4 coordinates
+    of each half, bench/ter_full_bench.cpp:218-245)."""
+    from tergpu import instance
+
+    for n in (36, 72, 108):
+        for seed in (1, 0x1001, ANCHOR_SEED, 0x544552F):
+            for kind, make in (("auth", instance.benchmark_instance), ("build", instance.build_instance)):
+                values, target, planted = oracle_mod.build_instance(n, seed, kind)
+                inst = make(n, seed)
+                assert np.array_equal(inst.values_le.reshape(values.shape), values), (n, seed, kind)
+                assert np.array_equal(inst.target_le, target), (n, seed, kind)
+                assert np.array_equal(inst.planted, planted), (n, seed, kind)
