@@ -211,3 +211,19 @@ def test_product_instances_equal_the_oracle_generator(oracle_mod):
                 assert np.array_equal(inst.values_le.reshape(values.shape), values), (n, seed, kind)
                 assert np.array_equal(inst.target_le, target), (n, seed, kind)
                 assert np.array_equal(inst.planted, planted), (n, seed, kind)
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_product_digest_equals_reference_brute_force(oracle_mod, golden, case):
+    """tergpu.workload.digest (the RootSink multiset hashes every GPU root test
+    compares, ter2_root/frozen/ter_root_queue_kernels.cpp:165-175) over the
+    oracle's triples of the six synthetic roots equals the reference's
+    brute-force digest."""
+    from tergpu import workload
+
+    g = golden["synthetic_roots"][case]
+    lo, hi = oracle_mod.synthetic_root(g["bits"], g["seed"], g["size"], g["pool"])
+    _, trip = oracle_mod.root_join(g["bits"], lo, hi, capacity=1 << 16)
+    got = workload.digest(trip)
+    for k in ("triples", "triple_sum", "triple_xor", "triple_sum2"):
+        assert got[k] == hexint(g["brute"][k]), k
