@@ -352,14 +352,56 @@ def whole_root(snap, root: str, run_id: str, out_dir, device: int = 0, load_ms: 
     return (0 if exact else 4), row
 
 
+# The reference's workload loader refuses roots below its 25-bit projection
+# (ter2_root/frozen/ter_root_generalization_workload.cpp:604-609).
+PROJECTION_BITS = 25
+
+
+def _attempt_row(snapshot_label: str, status: str, message: str, n: int = 0, seed: int = 0, attempt: int = 0,
+                 attempt_seed: int = 0, load_ms: float = 0.0, root_ms: float = 0.0, rebuild_ms: float = 0.0,
+                 verify_ms: float = 0.0, residue_exact: int = 0, structural_triples: int = 0,
+                 parents=(), planted_found: bool = False, device_name: str = "", device_root_ms: float = 0.0) -> dict:
+    """One attempts.jsonl row with the fields, in the order, that
+    ter_arwlf_solve_attempt writes (ter2_root/campaign/ter_arwlf_solve_attempt_main.cpp:161-177),
+    plus the device's name and root time."""
+    rss, peak = _memory_mib()
+    return {
+        "snapshot": snapshot_label, "status": status, "message": message, "n": n, "seed": seed,
+        "attempt": attempt, "attempt_seed": attempt_seed, "backend": "gpu",
+        "dispatch_ran": "", "load_ms": round(load_ms, 1), "keys_ms": 0.0, "root_ms": round(root_ms, 1),
+        "rebuild_ms": round(rebuild_ms, 1), "verify_ms": round(verify_ms, 3),
+        "residue_exact": int(residue_exact), "structural_triples": int(structural_triples),
+        "unique_parents": len(parents), "planted_found": planted_found,
+        "parents": sorted(parents) if status == "Found" else [],
+        "pin": "none", "pinned_cpu": -1, "cpu_start": -1, "cpu_end": -1,
+        "working_set_mib": rss, "peak_working_set_mib": peak, "build": "Release",
+        "git_commit": _git_commit(), "git_dirty_at_configure": -1, "utc": _utc(),
+        "device": device_name, "device_root_ms": round(float(device_root_ms), 3),
+    }
+
+
+def _append(out_path, row: dict) -> dict:
+    with open(out_path, "a") as f:
+        f.write(json.dumps(row, separators=(",", ":")) + "\n")
+    return row
+
+
 def solve_attempt(snap, snapshot_label: str, out_path, device: int = 0, load_ms: float = 0.0) -> dict:
-    """One attempt's root stage on the device, appended to `out_path`."""
+    """One attempt's root stage on the device, appended to `out_path`.  A root
+    whose quotient is below the reference's 25-bit projection (n = 36) is
+    recorded NotApplicable without device work, as the reference's
+    solve_attempt records it (ter2_root/campaign/ter_arwlf_solve.cpp:53-58)."""
     from . import instance as inst_mod
 
+    n = snap.n
+    if n - snap.r1 < PROJECTION_BITS:
+        return _append(out_path, _attempt_row(
+            snapshot_label, "NotApplicable",
+            f"quotient width Q={n - snap.r1} is below the 25-bit projection", n=n, seed=snap.seed,
+            load_ms=load_ms))
     t0 = time.perf_counter()
     res = run_gpu_root_records(snap, Config(device=device))
     root_ms = (time.perf_counter() - t0) * 1000.0
-    n = snap.n
     exact = res.triples[(res.flags & 1) == 1] if len(res.triples) else res.triples
     accepted = res.triples[(res.flags & 5) == 5] if len(res.triples) else res.triples
     t0 = time.perf_counter()
@@ -385,23 +427,12 @@ def solve_attempt(snap, snapshot_label: str, out_path, device: int = 0, load_ms:
         else:
             status = "Found"
     verify_ms = (time.perf_counter() - t0) * 1000.0
-    rss, peak = _memory_mib()
-    row = {
-        "snapshot": snapshot_label, "status": status, "message": message, "n": n, "seed": snap.seed,
-        "attempt": snap.attempt, "attempt_seed": snap.attempt_seed, "backend": "gpu",
-        "dispatch_ran": "", "load_ms": round(load_ms, 1), "keys_ms": 0.0, "root_ms": round(root_ms, 1),
-        "rebuild_ms": round(rebuild_ms, 1), "verify_ms": round(verify_ms, 3),
-        "residue_exact": int(len(exact)), "structural_triples": int(len(accepted)),
-        "unique_parents": len(parents), "planted_found": planted_found,
-        "parents": sorted(parents) if status == "Found" else [],
-        "pin": "none", "pinned_cpu": -1, "cpu_start": -1, "cpu_end": -1,
-        "working_set_mib": rss, "peak_working_set_mib": peak, "build": "Release",
-        "git_commit": _git_commit(), "git_dirty_at_configure": -1, "utc": _utc(),
-        "device": _device_name(device), "device_root_ms": round(float(res.telemetry.total_ms), 3),
-    }
-    with open(out_path, "a") as f:
-        f.write(json.dumps(row, separators=(",", ":")) + "\n")
-    return row
+    return _append(out_path, _attempt_row(
+        snapshot_label, status, message, n=n, seed=snap.seed, attempt=snap.attempt,
+        attempt_seed=snap.attempt_seed, load_ms=load_ms, root_ms=root_ms, rebuild_ms=rebuild_ms,
+        verify_ms=verify_ms, residue_exact=len(exact), structural_triples=len(accepted), parents=parents,
+        planted_found=planted_found, device_name=_device_name(device),
+        device_root_ms=res.telemetry.total_ms))
 
 
 def _load(args) -> tuple[object, str, float]:
@@ -439,6 +470,10 @@ def main(argv=None) -> int:
         snap, label, load_ms = _load(args)
     except (OSError, snapmod.SnapshotError, RuntimeError) as e:
         print(f"# snapshot: {e}")
+        if args.cmd == "solve-attempt":
+            # recorded, as the reference records an unreadable or damaged snapshot
+            # (ter_arwlf_solve.cpp:59-60; exit code 3)
+            _append(args.out, _attempt_row(args.snapshot or f"n{args.n}", "InvalidConfiguration", str(e)))
         return 3
     if args.cmd == "whole-root":
         if '"' in args.run:

@@ -6,6 +6,8 @@ import json
 
 import numpy as np
 
+from conftest import GOLDEN_DIR
+
 ANCHOR_SEED = 19797034556212562
 
 
@@ -91,8 +93,34 @@ def test_cli_usage_errors(tmp_path):
     r = subprocess.run([sys.executable, "-m", "tergpu.runs", "whole-root", f"--out-dir={tmp_path}",
                         "--run=x"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 2 and not (tmp_path / "runs.jsonl").exists()
-    # an unreadable snapshot: load failure, exit 3
+    # an unreadable snapshot: recorded InvalidConfiguration, exit 3, as the reference's
     r = subprocess.run([sys.executable, "-m", "tergpu.runs", "solve-attempt",
                         f"--snapshot={tmp_path / 'missing.snap'}", f"--out={tmp_path / 'a.jsonl'}"],
                        env=env, capture_output=True, text=True, timeout=120)
-    assert r.returncode == 3 and not (tmp_path / "a.jsonl").exists()
+    assert r.returncode == 3
+    rows = (tmp_path / "a.jsonl").read_text().splitlines()
+    assert len(rows) == 1 and json.loads(rows[0])["status"] == "InvalidConfiguration"
+
+
+def test_solve_attempt_refusals_are_recorded(tmp_path, golden):
+    """ter_arwlf_solve_attempt's refusals (ter2_root/tests/ter_arwlf_solve_tests.cpp:66-97),
+    recorded without device work: the n=36 root (Q = 24, below the 25-bit
+    projection) is NotApplicable with no parents and exit 0; a missing and a
+    damaged snapshot are InvalidConfiguration rows with no parents and exit 3."""
+    from tergpu import runs
+
+    out = tmp_path / "attempts.jsonl"
+    snap = GOLDEN_DIR / golden["n36_snapshot"]["path"]
+    assert runs.main(["solve-attempt", f"--snapshot={snap}", f"--out={out}"]) == 0
+    assert runs.main(["solve-attempt", f"--snapshot={tmp_path / 'missing.snap'}", f"--out={out}"]) == 3
+    damaged = tmp_path / "damaged.snap"
+    raw = bytearray(snap.read_bytes())
+    raw[-3] ^= 0x10
+    damaged.write_bytes(bytes(raw))
+    assert runs.main(["solve-attempt", f"--snapshot={damaged}", f"--out={out}"]) == 3
+    rows = [json.loads(line) for line in out.read_text().splitlines()]
+    assert [r["status"] for r in rows] == ["NotApplicable", "InvalidConfiguration", "InvalidConfiguration"]
+    assert rows[0]["message"] == "quotient width Q=24 is below the 25-bit projection"
+    assert rows[0]["n"] == 36 and rows[0]["root_ms"] == 0.0
+    for r in rows:
+        assert r["parents"] == [] and r["unique_parents"] == 0 and r["backend"] == "gpu"
