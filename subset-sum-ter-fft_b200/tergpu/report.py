@@ -18,7 +18,9 @@ n/2).  The policies then read as the reference defines them:
 
 Statuses follow the reference: Completed with the counts, ResourceLimit when
 the device refuses the declared ceiling, InvalidConfiguration for a capture
-that is not a FiniteSanity root the device runs.
+that is not a FiniteSanity root the device runs or that breaks the capture
+invariants the reference checks (targets and residues below 2^n, residues
+congruent to their child target modulo 2^r1), before any device work.
 """
 from __future__ import annotations
 
@@ -71,6 +73,32 @@ def _digits(words: tuple[int, ...], n: int) -> np.ndarray:
     return np.array([(words[i // 64] >> (i % 64)) & 1 for i in range(n)], dtype=np.uint8)
 
 
+def _capture_refusal(snap) -> str | None:
+    """The capture checks report_full_ter_root makes before its root
+    (src/full_ter.cpp:3772-3803), with the reference's messages: every target
+    below 2^n, and every residue below 2^n and congruent to its list's child
+    target modulo 2^r1.  None when the capture passes."""
+    from .snapshot import words_to_int
+
+    n, r1 = snap.n, snap.r1
+    targets = [words_to_int(t) for t in snap.child_targets]
+    if any(t >> n for t in targets):
+        return "root count child target exceeds the captured modulus"
+    if words_to_int(snap.root_target) >> n:
+        return "root count target exceeds the captured modulus"
+    top_bits = n - 32 * (snap.words32 - 1)  # bits of the top residue word below 2^n
+    low_mask = np.uint64((1 << r1) - 1)
+    for l in range(3):
+        res = snap.residues(l)
+        if len(res) == 0:
+            continue
+        low = res[:, 0].astype(np.uint64) | (res[:, 1].astype(np.uint64) << np.uint64(32))
+        above = top_bits < 32 and bool((res[:, -1] >> np.uint32(top_bits)).any())
+        if above or bool(((low & low_mask) != (np.uint64(targets[l] & (2**64 - 1)) & low_mask)).any()):
+            return "root report capture violates the child target invariant"
+    return None
+
+
 def report_full_ter_root(snap, policy: RootOutputPolicy = RootOutputPolicy.FIRST_WITNESS,
                          config: Config | None = None) -> FullTerRootReportResult:
     """report_full_ter_root on a captured root (see the module docstring)."""
@@ -78,6 +106,9 @@ def report_full_ter_root(snap, policy: RootOutputPolicy = RootOutputPolicy.FIRST
     config = config or Config()
     if snap.n == 0 or snap.n % 36 != 0 or snap.r1 >= snap.n:
         return FullTerRootReportResult(message="root report requires a completed FiniteSanity capture")
+    refusal = _capture_refusal(snap)
+    if refusal is not None:
+        return FullTerRootReportResult(status=_abi.INVALID_CONFIGURATION, message=refusal)
     try:
         res = run_gpu_root_records(snap, Config(memory_limit_bytes=config.memory_limit_bytes,
                                                 device=config.device,

@@ -164,3 +164,38 @@ def test_host_key_derivation_matches_oracle_attempt(oracle_mod, golden):
     d, _ = oracle_mod.root_join(Q, lo, [h.astype(np.uint64) for h in hi])
     row = golden["n36_attempts"][0]["attempts"][0]
     assert d["triples"] == row["root_modular"]
+
+
+def test_root_report_refuses_captures_that_break_the_invariants(golden):
+    """report_full_ter_root's capture checks (src/full_ter.cpp:3772-3803), with
+    the reference's messages and before any device work: a residue not
+    congruent to its child target modulo 2^r1, a residue at or above 2^n, and a
+    child or root target at or above 2^n are InvalidConfiguration."""
+    import copy
+
+    from tergpu import _abi, report, snapshot
+
+    base = snapshot.load(GOLDEN_DIR / golden["n36_snapshot"]["path"])
+    assert report._capture_refusal(base) is None
+    invariant = "root report capture violates the child target invariant"
+    cases = []
+    low = copy.deepcopy(base)
+    low.records[1].reshape(-1, low.record_bytes)[3, 16 * low.words64] ^= 1  # residue bit 0
+    cases.append((low, invariant))
+    high = copy.deepcopy(base)
+    high.records[2].reshape(-1, high.record_bytes)[0, 16 * high.words64 + 4] ^= 0x10  # residue bit 36
+    cases.append((high, invariant))
+    child = copy.deepcopy(base)
+    child.child_targets[0] = child.child_targets[0].copy()
+    child.child_targets[0][1] |= 1 << 4  # bit 36
+    cases.append((child, "root count child target exceeds the captured modulus"))
+    root = copy.deepcopy(base)
+    root.root_target = root.root_target.copy()
+    root.root_target[1] |= 1 << 5
+    cases.append((root, "root count target exceeds the captured modulus"))
+    for snap, message in cases:
+        for policy in report.RootOutputPolicy:
+            got = report.report_full_ter_root(snap, policy)
+            assert got.status == _abi.INVALID_CONFIGURATION and got.message == message
+        counted = report.count_full_ter_root(snap)
+        assert counted.status == _abi.INVALID_CONFIGURATION and counted.message == message
