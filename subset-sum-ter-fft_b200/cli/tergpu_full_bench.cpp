@@ -445,7 +445,9 @@ int run_preflight(const Options& o) {
   if (st == TERGPU_INVALID_CONFIGURATION) {
     std::cout << "  shape_status=InvalidConfiguration\n";
     std::cout << "  message=" << tergpu_last_error() << '\n';
-    std::cout << "  VERDICT: dimension is not a constructible exact TER shape on the device path\n";
+    // the reference's verdict where no path can construct the shape (36 does not divide n)
+    std::cout << "  VERDICT: dimension is not a constructible exact TER shape"
+              << (o.n != 0 && o.n % 36 == 0 ? " on the device path" : "") << '\n';
     return EXIT_FAILURE;
   }
   std::cout << "  shape_status=Completed\n";

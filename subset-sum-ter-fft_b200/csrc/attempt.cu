@@ -228,7 +228,7 @@ uint64_t canonicalize(Workspace& w, const EntryArrays& raw, uint64_t count, cons
 
 void cancelled_check(const tergpu_attempt_in* in) {
   if (in->cancel != nullptr && *in->cancel != 0) {
-    t_error = "cancelled";
+    t_error = "full TER execution was cancelled";
     throw Failure{TERGPU_CANCELLED};
   }
 }
@@ -989,7 +989,9 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
   const auto t_call = std::chrono::steady_clock::now();
   const uint32_t n = in->n;
   if (n == 0 || n % 36 != 0 || n > 108) {
-    t_error = "full TER on the device requires n in {36, 72, 108}";
+    // the reference's message where it refuses the shape too (src/full_ter.cpp:2589)
+    t_error = n == 0 || n % 36 != 0 ? "full TER requires n divisible by 36 and 0 < modulus_bits <= n"
+                                    : "full TER on the device requires n in {36, 72, 108}";
     return TERGPU_INVALID_CONFIGURATION;
   }
   // solve_full_ter refuses CountOnly, since a SAT result must keep a verifiable
@@ -1566,6 +1568,7 @@ int attempt_body(const tergpu_attempt_in* in, tergpu_attempt_out* out, Workspace
     run.push_back(stat);
     if (status == TERGPU_FOUND) break;
   }
+  if (status == TERGPU_ATTEMPT_LIMIT_REACHED) t_error = "deterministic TER attempts exhausted without proving UNSAT";
   if (telemetry) out->fingerprint = run_fingerprint(status == TERGPU_FOUND ? out->witness : nullptr, n, in->seed,
                                                     fixture, r1, r2, l3, run);
   out->status = status;

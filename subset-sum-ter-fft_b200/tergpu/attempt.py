@@ -2,9 +2,13 @@
 
 `solve_full_ter(instance, config)` mirrors the reference's entry point
 (include/ter/full_ter.hpp:255-256, src/full_ter.cpp:2933-3521) for the
-FiniteSanity shape with random targets: attempt a uses SplitMix64(seed + a);
-the result carries the status, the verified witness and per-attempt telemetry
-(level sizes and candidate counts).  `instance` comes from tergpu.instance.
+FiniteSanity shape: random targets (attempt a draws from SplitMix64(seed + a))
+or the planted root's guided targets, complete (FullTer) or truncated
+(FixtureTer) level 3.  The result carries the status, the reference's message
+for it, the verified witness and per-attempt telemetry (level sizes, stage
+counters, fingerprints).  `preflight(instance, config)` makes the same call's
+checks and prediction without device work.  `instance` comes from
+tergpu.instance.
 """
 from __future__ import annotations
 
@@ -98,6 +102,7 @@ class FullTerResult:
     total_ms: float = 0.0
     device_bytes: int = 0        # the preflight's predicted bytes
     device_bytes_held: int = 0   # bytes the workspace held at the end of the call
+    message: str = ""            # FullTerResult::message: why the call ended short of Found
     fingerprint: int = 0         # FullTerTelemetry::fingerprint (telemetry runs)
     level3_ms: float = 0.0
 
@@ -188,7 +193,9 @@ def preflight(instance, config: FullTerConfig | None = None) -> FullTerResult:
     st = lib.tergpu_attempt_run(ctypes.byref(ain), ctypes.byref(out))
     if st not in (_abi.COMPLETED, _abi.RESOURCE_LIMIT, _abi.INVALID_CONFIGURATION):
         raise TergpuError(st, _abi.last_error())
-    return _result(st, out, stats, instance.n)
+    res = _result(st, out, stats, instance.n)
+    res.message = _abi.last_error() if st != _abi.COMPLETED else ""
+    return res
 
 
 def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -> FullTerResult:
@@ -215,6 +222,7 @@ def solve_full_ter(instance, config: FullTerConfig | None = None, cancel=None) -
                   _abi.INVALID_CONFIGURATION):
         raise TergpuError(st, _abi.last_error())
     res = _result(st, out, stats, instance.n)
+    res.message = _abi.last_error() if st != _abi.FOUND else ""
     if bufs and out.attempts_run > 0:
         from .snapshot import Snapshot
 

@@ -376,12 +376,12 @@ def full_bench_rows(tmp: Path):
 def preflight_text(tmp: Path):
     """The reference's own ter_full_bench --preflight output (geometry,
     representation counts, decisions) at n = 36, 72, 108 and a large ceiling,
-    and FixtureTer at n = 72."""
+    FixtureTer at n = 72, and the refused n = 48."""
     import subprocess
 
     binary = HERE.parent.parent / "oracle" / "_ref" / "ter_full_bench"
     out = []
-    for args in (["--n=36"], ["--n=72"], ["--n=108"], ["--n=72", "--fixture"]):
+    for args in (["--n=36"], ["--n=72"], ["--n=108"], ["--n=72", "--fixture"], ["--n=48"]):
         args = ["--preflight", *args, "--memory-limit-mib=1000000"]
         proc = subprocess.run([str(binary), *args], capture_output=True, text=True, timeout=600)
         out.append({"args": args, "rc": proc.returncode, "lines": proc.stdout.splitlines()})

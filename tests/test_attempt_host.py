@@ -56,7 +56,9 @@ def test_solve_refusals_before_device_work():
     from tergpu import _abi, attempt, instance
 
     for n in (48, 60, 84, 96):
-        assert attempt.solve_full_ter(instance.benchmark_instance(n, 1)).status == _abi.INVALID_CONFIGURATION
+        res = attempt.solve_full_ter(instance.benchmark_instance(n, 1))
+        assert res.status == _abi.INVALID_CONFIGURATION
+        assert res.message == "full TER requires n divisible by 36 and 0 < modulus_bits <= n"
     tight = attempt.FullTerConfig(memory_limit_bytes=1 << 20)
     assert attempt.solve_full_ter(instance.benchmark_instance(108, 1), tight).status == _abi.RESOURCE_LIMIT
     inst = instance.benchmark_instance(36, 0x544552F)
@@ -93,7 +95,7 @@ def test_pre_cancelled_solve_matches_reference(golden):
     res = attempt.solve_full_ter(inst, cfg, cancel=ctypes.c_int32(1))
     assert res.status == _abi.CANCELLED and res.attempts == []
     assert res.fingerprint == hexint(g["final"]["fingerprint"])
-    assert _abi.last_error() == g["final"]["message"]
+    assert res.message == _abi.last_error() == g["final"]["message"]
 
 
 def test_empty_budget_and_tiny_ceiling_fail_closed(golden):
@@ -104,7 +106,8 @@ def test_empty_budget_and_tiny_ceiling_fail_closed(golden):
 
     g, inst, cfg = _failure_case(golden, "no_attempts")
     assert g["final"]["status"] == _abi.INVALID_CONFIGURATION
-    assert attempt.solve_full_ter(inst, cfg).status == _abi.INVALID_CONFIGURATION
+    res = attempt.solve_full_ter(inst, cfg)
+    assert res.status == _abi.INVALID_CONFIGURATION and res.message == g["final"]["message"]
     _, inst, cfg = _failure_case(golden, "run")
     tight = attempt.FullTerConfig(**{**cfg.__dict__, "memory_limit_bytes": 1})
     assert attempt.solve_full_ter(inst, tight).status == _abi.RESOURCE_LIMIT

@@ -48,7 +48,7 @@ def test_preflight_geometry(n, r1, r2, q):
     assert "VERDICT: bounded exact path on both merge stages" in p.stdout
 
 
-@pytest.mark.parametrize("case", range(4))
+@pytest.mark.parametrize("case", range(5))
 def test_preflight_prints_the_reference_lines(case):
     """Every line of the reference's own ter_full_bench --preflight (golden
     preflight_text) appears in the device preflight, with the same exit code:
