@@ -66,6 +66,8 @@ def lib():
         L = ctypes.CDLL(str(LIB_PATH))
         L.orc_mix64.restype = ctypes.c_uint64
         L.orc_mix64.argtypes = [ctypes.c_uint64]
+        L.orc_add_packed_word.restype = ctypes.c_int
+        L.orc_add_packed_word.argtypes = [ctypes.c_uint64] * 6 + [ctypes.POINTER(ctypes.c_uint64)] * 2
         L.orc_build_instance.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
                                          ctypes.c_int, _u64p, _u64p, _u8p]
         L.orc_params.argtypes = [ctypes.c_uint32, _u32p, _u32p]
@@ -100,6 +102,13 @@ def _p32(a: np.ndarray):
 
 def _p8(a):
     return None if a is None else a.ctypes.data_as(_u8p)
+
+
+def add_packed_word(ap: int, an: int, bp: int, bn: int, cp: int, cn: int):
+    """(valid, positive mask, negative mask) of one word of a + b + c."""
+    pos, neg = ctypes.c_uint64(), ctypes.c_uint64()
+    ok = lib().orc_add_packed_word(ap, an, bp, bn, cp, cn, ctypes.byref(pos), ctypes.byref(neg))
+    return bool(ok), int(pos.value), int(neg.value)
 
 
 def mix64(v: int) -> int:

@@ -239,6 +239,20 @@ static int add_three(const entry_t *a, const entry_t *b, const entry_t *c, uint3
   return 1;
 }
 
+/* One 64-digit word of the packed ternary add (add_packed_word,
+ * src/packed.cpp:15-38): 0 when a digit of a + b + c leaves {-1, 0, 1}, else 1
+ * with the sum's positive and negative masks. */
+int orc_add_packed_word(uint64_t ap, uint64_t an, uint64_t bp, uint64_t bn, uint64_t cp, uint64_t cn,
+                        uint64_t *pos, uint64_t *neg) {
+  entry_t a = {{ap, 0}, {an, 0}, 0}, b = {{bp, 0}, {bn, 0}, 0}, c = {{cp, 0}, {cn, 0}, 0};
+  uint64_t out_pos[2], out_neg[2];
+  uint32_t np, nn;
+  const int ok = add_three(&a, &b, &c, 64, out_pos, out_neg, &np, &nn);
+  *pos = ok ? out_pos[0] : 0;
+  *neg = ok ? out_neg[0] : 0;
+  return ok;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Attempt pipeline                                                           */
 /* ------------------------------------------------------------------------- */

@@ -227,3 +227,33 @@ def test_product_digest_equals_reference_brute_force(oracle_mod, golden, case):
     got = workload.digest(trip)
     for k in ("triples", "triple_sum", "triple_xor", "triple_sum2"):
         assert got[k] == hexint(g["brute"][k]), k
+
+
+def test_packed_add_matches_every_ternary_truth_table_row(oracle_mod):
+    """The oracle's packed ternary add (add_packed_word, src/packed.cpp:15-38)
+    on the reference's own truth-table test (tests/packed_tests.cpp:85-113):
+    valid exactly when a + b + c stays in {-1, 0, 1}, and then its sign; and
+    on seeded words of 64 independent digits against the scalar digit sums."""
+    for a in (-1, 0, 1):
+        for b in (-1, 0, 1):
+            for c in (-1, 0, 1):
+                ok, pos, neg = oracle_mod.add_packed_word(int(a == 1), int(a == -1), int(b == 1),
+                                                          int(b == -1), int(c == 1), int(c == -1))
+                total = a + b + c
+                assert ok == (-1 <= total <= 1), (a, b, c)
+                if ok:
+                    assert (pos & 1, neg & 1) == (int(total == 1), int(total == -1)), (a, b, c)
+    rng = np.random.default_rng(0x5041434B)
+    for _ in range(200):
+        digits = rng.integers(-1, 2, size=(3, 64))
+        # keep the sums in range most of the time, so both outcomes occur
+        if rng.random() < 0.7:
+            digits[2] = np.clip(-(digits[0] + digits[1]) + rng.integers(-1, 2, size=64), -1, 1)
+        masks = [(int(sum(1 << i for i in range(64) if d[i] == 1)),
+                  int(sum(1 << i for i in range(64) if d[i] == -1))) for d in digits]
+        ok, pos, neg = oracle_mod.add_packed_word(*masks[0], *masks[1], *masks[2])
+        total = digits.sum(axis=0)
+        assert ok == bool(np.all(np.abs(total) <= 1))
+        if ok:
+            assert pos == sum(1 << i for i in range(64) if total[i] == 1)
+            assert neg == sum(1 << i for i in range(64) if total[i] == -1)
