@@ -100,3 +100,29 @@ def early_root_capture():
     zeros = [((), 0)] * 4
     return capture_from_records(36, 12, 3, [[(first, 0), (second, 0), (first, 0), (second, 0)],
                                             zeros, zeros])
+
+
+def boundary_roots():
+    """The tiled reporter's boundary cases (tests/tiled_q3report_tests.cpp:157-231),
+    scaled from modulus 64 to 2^Q at
+    the device's key widths: singleton lists whose pair sums land on 0, M - 1,
+    M and 2M - 2 (M = 2^Q), and duplicated keys that keep their multiplicity.
+    Yields (Q, lo[3], hi[3], expected triples) with list 2 holding
+    d = tau - q_c, the expected count from exact integer arithmetic."""
+    import numpy as np
+
+    def lists(Q, a, b, c, tau):
+        M = 1 << Q
+        keys = [list(a), list(b), [(tau - v) % M for v in c]]
+        lo = [np.array([k & (2**64 - 1) for k in ks], dtype=np.uint64) for ks in keys]
+        hi = [np.array([k >> 64 for k in ks], dtype=np.uint8) for ks in keys]
+        want = sum(1 for x in keys[0] for y in keys[1] for z in keys[2] if (x + y - z) % M == 0)
+        return lo, hi, want
+
+    for Q in (24, 47, 64, 69, 72):
+        M = 1 << Q
+        for a, b, c, tau in ((0, 0, 0, 0), (0, 0, 1, 0), (M - 1, 0, 1, 0), (M - 1, 1, 0, 0),
+                             (M - 1, M - 1, 2, 0), (M - 1, M - 1, 1, M - 1), (M // 2, M // 2, 0, 0),
+                             (M // 2, M // 2 - 1, 1, 0)):
+            yield (Q,) + lists(Q, [a], [b], [c], tau)
+        yield (Q,) + lists(Q, [7] * 3, [9] * 2, [M - 16] * 4, 0)

@@ -257,3 +257,18 @@ def test_packed_add_matches_every_ternary_truth_table_row(oracle_mod):
         if ok:
             assert pos == sum(1 << i for i in range(64) if total[i] == 1)
             assert neg == sum(1 << i for i in range(64) if total[i] == -1)
+
+
+def test_boundary_roots_are_exact(oracle_mod):
+    """The reporter's boundary cases at every device key width: the oracle's
+    full-Q join finds exactly the triples exact integer arithmetic finds, and
+    the reference's own expectations hold (the (0, 0, 1) singleton is the one
+    miss; the duplicated keys give 3 x 2 x 4 = 24 triples)."""
+    from conftest import boundary_roots
+
+    wants = []
+    for Q, lo, hi, want in boundary_roots():
+        digest, _ = oracle_mod.root_join(Q, lo, [h.astype(np.uint64) for h in hi], capacity=64)
+        assert digest["triples"] == want, (Q, [int(v[0]) for v in lo])
+        wants.append(want)
+    assert wants == [1, 0, 1, 1, 1, 1, 1, 1, 24] * 5

@@ -125,3 +125,16 @@ def test_early_root_fixture_report_stops_and_counts():
     assert first.status == 0 and first.valid_root_count == 1 and first.retained_root_count == 1
     count = report.count_full_ter_root(snap)
     assert count.status == 0 and count.valid_root_count == 64
+
+
+def test_boundary_roots_on_the_device():
+    """The reporter's boundary cases (tests/tiled_q3report_tests.cpp:157-231),
+    scaled to the device's key widths 24, 47, 64, 69 and 72: pair sums at 0,
+    M - 1, M and 2M - 2 of M = 2^Q, and duplicated keys keeping multiplicity;
+    every count equals exact integer arithmetic."""
+    import tergpu
+    from conftest import boundary_roots
+
+    for Q, lo, hi, want in boundary_roots():
+        res = tergpu.run_gpu_root(tergpu.RootKeys(quotient_bits=Q, lo=lo, hi=hi))
+        assert len(res.triples) == want, (Q, [int(v[0]) for v in lo], len(res.triples), want)
