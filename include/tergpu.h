@@ -321,7 +321,10 @@ typedef struct {
                                           device bytes (out->device_bytes), check them
                                           against memory_limit_bytes and return
                                           TERGPU_COMPLETED without device work; the
-                                          instance may be NULL (ter_full_bench --preflight) */
+                                          instance may be NULL (ter_full_bench --preflight).
+                                          The shape, policy, flag and fixture-limit
+                                          refusals are the call's own; the budget, cancel
+                                          flag and guided root are not checked */
 
 typedef struct {
   uint32_t n;                  /* 36, 72 or 108 */
