@@ -1,5 +1,5 @@
 """bench.py's host logic (CPU only): which reference build times the CPU legs,
-and the served request mix's bounded n=108 budgets."""
+and the served request mix: bounded n=108 budgets, the same requests at any rate."""
 import argparse
 import importlib.util
 
@@ -45,3 +45,19 @@ def test_served_n108_budgets_are_bounded_and_seeded():
     again = bench.solve_requests(args, True)
     assert [(r.instance.n, r.config.seed, r.config.attempt_limit) for r in again] == \
         [(r.instance.n, r.config.seed, r.config.attempt_limit) for r in reqs]
+
+
+def test_saturated_serve_stream_has_the_same_requests():
+    """serve_saturated re-times the serve stream: the same seeded requests (n,
+    seed, budget), only the arrival gaps shrink with the rate."""
+    bench = _bench()
+
+    def stream(rate):
+        args = argparse.Namespace(seed=0x1001, requests=400, rate=rate, serve_n="36,48,60,72,84,96",
+                                  max_attempts=0)
+        return bench.solve_requests(args, True)
+
+    slow, fast = stream(200.0), stream(5000.0)
+    assert [(r.instance.n, r.config.seed, r.config.attempt_limit) for r in slow] == \
+        [(r.instance.n, r.config.seed, r.config.attempt_limit) for r in fast]
+    assert abs(fast[-1].arrival_ms * 25 - slow[-1].arrival_ms) < 1e-6 * slow[-1].arrival_ms
