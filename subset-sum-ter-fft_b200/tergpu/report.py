@@ -100,12 +100,22 @@ def _capture_refusal(snap) -> str | None:
 
 
 def report_full_ter_root(snap, policy: RootOutputPolicy = RootOutputPolicy.FIRST_WITNESS,
-                         config: Config | None = None) -> FullTerRootReportResult:
-    """report_full_ter_root on a captured root (see the module docstring)."""
-    policy = RootOutputPolicy(policy)
+                         config: Config | None = None, cancel=None) -> FullTerRootReportResult:
+    """report_full_ter_root on a captured root (see the module docstring).
+    `cancel` (a ctypes.c_int32 or None) is the reference's config.cancellation:
+    set before the call, the report returns Cancelled without device work.  An
+    unknown policy or a capture that is not a FiniteSanity root is refused
+    with the reference's message (src/full_ter.cpp:3727-3743)."""
     config = config or Config()
-    if snap.n == 0 or snap.n % 36 != 0 or snap.r1 >= snap.n:
-        return FullTerRootReportResult(message="root report requires a completed FiniteSanity capture")
+    try:
+        policy = RootOutputPolicy(policy)
+    except ValueError:
+        policy = None
+    if policy is None or snap.n == 0 or snap.n % 36 != 0 or snap.r1 >= snap.n:
+        return FullTerRootReportResult(
+            message="root report requires a completed native root capture and valid tiled limits")
+    if cancel is not None and cancel.value != 0:
+        return FullTerRootReportResult(status=_abi.CANCELLED, message="root report was cancelled")
     refusal = _capture_refusal(snap)
     if refusal is not None:
         return FullTerRootReportResult(status=_abi.INVALID_CONFIGURATION, message=refusal)
@@ -139,8 +149,8 @@ def report_full_ter_root(snap, policy: RootOutputPolicy = RootOutputPolicy.FIRST
     return out
 
 
-def count_full_ter_root(snap, config: Config | None = None) -> FullTerRootCountResult:
+def count_full_ter_root(snap, config: Config | None = None, cancel=None) -> FullTerRootCountResult:
     """count_full_ter_root: the CountOnly projection of the report."""
-    r = report_full_ter_root(snap, RootOutputPolicy.COUNT_ONLY, config)
+    r = report_full_ter_root(snap, RootOutputPolicy.COUNT_ONLY, config, cancel)
     return FullTerRootCountResult(status=r.status, valid_root_count=r.valid_root_count,
                                   telemetry=r.telemetry, message=r.message)

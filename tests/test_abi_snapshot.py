@@ -199,3 +199,22 @@ def test_root_report_refuses_captures_that_break_the_invariants(golden):
             assert got.status == _abi.INVALID_CONFIGURATION and got.message == message
         counted = report.count_full_ter_root(snap)
         assert counted.status == _abi.INVALID_CONFIGURATION and counted.message == message
+
+
+def test_root_report_refuses_bad_policy_and_honours_a_set_cancel_flag(golden):
+    """report_full_ter_root's first checks (src/full_ter.cpp:3727-3743), before
+    any device work: a policy outside the enum is InvalidConfiguration with the
+    reference's message, and a cancellation flag already set returns Cancelled
+    from the report and the count."""
+    from tergpu import _abi, report, snapshot
+
+    snap = snapshot.load(GOLDEN_DIR / golden["n36_snapshot"]["path"])
+    bad = report.report_full_ter_root(snap, 7)
+    assert bad.status == _abi.INVALID_CONFIGURATION
+    assert bad.message == "root report requires a completed native root capture and valid tiled limits"
+    flag = ctypes.c_int32(1)
+    for policy in report.RootOutputPolicy:
+        got = report.report_full_ter_root(snap, policy, cancel=flag)
+        assert got.status == _abi.CANCELLED and got.message == "root report was cancelled"
+    counted = report.count_full_ter_root(snap, cancel=flag)
+    assert counted.status == _abi.CANCELLED and counted.valid_root_count == 0
