@@ -306,6 +306,11 @@ def whole_root(snap, root: str, run_id: str, out_dir, device: int = 0, load_ms: 
                 print(f"# run {run_id} already complete")
                 return 0, None
     Q = snap.n - snap.r1
+    if Q < PROJECTION_BITS:
+        # the reference's runner stops at its workload loader with exit 3 and no row
+        # (ter2_root/campaign/ter_arwlf_whole_root_main.cpp:234-240)
+        print(f"# snapshot {root} : NotApplicable (quotient width Q={Q} is below the 25-bit projection)")
+        return 3, None
     cell = anchor_cell()
     t0 = time.perf_counter()
     planted = plant_positive(snap, cell) if plant else None

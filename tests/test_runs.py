@@ -124,3 +124,14 @@ def test_solve_attempt_refusals_are_recorded(tmp_path, golden):
     assert rows[0]["n"] == 36 and rows[0]["root_ms"] == 0.0
     for r in rows:
         assert r["parents"] == [] and r["unique_parents"] == 0 and r["backend"] == "gpu"
+
+
+def test_whole_root_below_the_projection_is_refused(tmp_path, golden):
+    """The whole-root runner on the n=36 root (Q = 24): the reference's loader
+    refuses it, so the run exits 3 and records no row
+    (ter2_root/campaign/ter_arwlf_whole_root_main.cpp:234-240), with no device work."""
+    from tergpu import runs
+
+    snap = GOLDEN_DIR / golden["n36_snapshot"]["path"]
+    code = runs.main(["whole-root", f"--snapshot={snap}", f"--out-dir={tmp_path}", "--run=n36"])
+    assert code == 3 and not (tmp_path / "runs.jsonl").exists()
